@@ -1,0 +1,146 @@
+/*
+ * v2rdm_gpu.h -- C ABI of the B200 boundary-point SDP solver for the
+ * active-space hot path of v2RDM-CASSCF.
+ *
+ * The plugin's solver object (v2RDMSolver, v2rdm_solver.h:79-575) keeps the
+ * BPSDP state in Psi4 vectors and runs the outer loop of compute_energy
+ * (v2rdm_solver.cc:1778-1908) on the host.  These entry points replace that
+ * loop and the functions it calls:
+ *
+ *   v2g_create                 common_init's layout part (v2rdm_solver.cc:487-1285)
+ *                              and BuildBasis (basis.cc:439-757)
+ *   v2g_set_hamiltonian        GetIntegrals/RepackIntegrals/FrozenCoreEnergy
+ *                              (tei.cc:55-313) for DF/CD three-index integrals
+ *   v2g_guess_random           Guess, TPDM_GUESS=RANDOM (v2rdm_solver.cc:2479-2490)
+ *   v2g_set_state/get_state    the x, y, z, mu members; checkpoint restart
+ *                              (checkpoint.cc:56-121)
+ *   v2g_apply_A / v2g_apply_AT bpsdp_Au / bpsdp_ATu (v2rdm_solver.cc:3020-3158)
+ *   v2g_solve                  the outer loop (v2rdm_solver.cc:1778-1908) with
+ *                              CGSolver::solve (cg_solver.cc:125-177) and
+ *                              Update_xz (v2rdm_solver.cc:3216-3289)
+ *   v2g_solve_batch            many such solves in one lock-step GPU run
+ *
+ * Conventions: every function returns V2G_OK (0) or a negative status; no
+ * C++ exception crosses this boundary.  v2g_last_error() gives the message of
+ * the last failure on the calling thread.  All arrays are host memory in the
+ * reference's layout (x, z: dimx; y, b: nconstraints), except the *_device
+ * entry points, which take device pointers on the handle's stream.  A handle
+ * is used by one host thread at a time.
+ */
+#ifndef V2RDM_GPU_H
+#define V2RDM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define V2G_OK 0
+#define V2G_ERR_ARG -1          /* invalid argument or option value */
+#define V2G_ERR_CUDA -2         /* CUDA runtime failure */
+#define V2G_ERR_NOT_CONVERGED -3 /* MAXITER reached ("v2RDM did not converge.") */
+#define V2G_ERR_NONFINITE -4    /* NaN or Inf appeared in the iteration */
+#define V2G_ERR_UNSUPPORTED -5  /* option combination not built */
+#define V2G_ERR_NO_DEVICE -6    /* no CUDA device visible */
+
+typedef struct v2g_handle v2g_handle;
+
+/* Options on the hot path, same names and defaults as the plugin
+ * (plugin.cc:66-124); fill with v2g_default_options(). */
+typedef struct v2g_options {
+    const char* positivity;     /* "D", "DQ", "DG", "DQG", "DQGT1", "DQGT2", "DQGT1T2" */
+    int constrain_spin;         /* CONSTRAIN_SPIN (1) */
+    int constrain_sz;           /* CONSTRAIN_SZ (1) */
+    double r_convergence;       /* R_CONVERGENCE (1e-4) */
+    double e_convergence;       /* E_CONVERGENCE (1e-4) */
+    double cg_convergence;      /* CG_CONVERGENCE (1e-9) */
+    int maxiter;                /* MAXITER (10000) */
+    int cg_maxiter;             /* CG_MAXITER (10000) */
+    double tau_parameter;       /* TAU_PARAMETER (1.0) */
+    int mu_update_frequency;    /* MU_UPDATE_FREQUENCY (500) */
+    int device;                 /* CUDA device ordinal (0) */
+    int record_trace;           /* keep the per-iteration line of v2rdm_solver.cc:1881 (0) */
+} v2g_options;
+
+typedef struct v2g_result {
+    double e_total;      /* c.x + enuc + efzc ("v2RDM total energy") */
+    double e_primal;     /* c.x + enuc + efzc at the last iteration */
+    double e_dual;       /* b.y + enuc + efzc */
+    double ep;           /* ||A x - b|| */
+    double ed;           /* ||A^T y - c + z|| */
+    double mu;
+    double efzc, enuc;
+    long oiter;          /* outer (macro) iterations */
+    long iiter;          /* total CG (micro) iterations */
+    int status;          /* V2G_OK, V2G_ERR_NOT_CONVERGED, V2G_ERR_NONFINITE */
+    double t_cg;         /* device seconds in the CG phase (iiter_time_) */
+    double t_xz;         /* device seconds in Update_xz (oiter_time_) */
+    double t_total;      /* device seconds for the whole solve */
+} v2g_result;
+
+void v2g_default_options(v2g_options* opt);
+const char* v2g_last_error(void);
+
+/* Active-space problem.  Orbital counts per irrep in Pitzer order, like the
+ * plugin's frzcpi/rstcpi/active/rstvpi/frzvpi; nalpha/nbeta are total electron
+ * counts of the reference wavefunction (the active counts are nalpha minus
+ * the doubly occupied core).  multiplicity = 2S+1. */
+int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int* rstcpi, const int* amopi,
+               const int* rstvpi, const int* frzvpi, int nalpha, int nbeta, int multiplicity, v2g_handle** out);
+void v2g_destroy(v2g_handle* h);
+
+/* Sizes: dimx_, nconstraints_, and the PSD blocks (dimensions_). */
+long v2g_dimx(const v2g_handle* h);
+long v2g_nconstraints(const v2g_handle* h);
+int v2g_nblocks(const v2g_handle* h);
+int v2g_block_dims(const v2g_handle* h, int* dims);
+
+/* Integrals: oei packed per irrep as lower triangles over the orbitals that
+ * are not frozen virtuals (oei_full_sym_), and three-index integrals
+ * qmo[Q * ntri + INDEX(p,q)], ntri = nmo'(nmo'+1)/2 (Qmo_, tei.cc:321). */
+int v2g_set_hamiltonian(v2g_handle* h, const double* oei_packed, const double* qmo, int nq, double enuc);
+int v2g_get_c(const v2g_handle* h, double* c);
+int v2g_get_b(const v2g_handle* h, double* b);
+double v2g_efzc(const v2g_handle* h);
+
+/* Starting point: the reference's random guess (srand(0), glibc rand) or an
+ * explicit state (restart from a checkpoint, warm start). */
+int v2g_guess_random(v2g_handle* h);
+int v2g_set_state(v2g_handle* h, const double* x, const double* y, const double* z, double mu);
+int v2g_get_state(const v2g_handle* h, double* x, double* y, double* z, double* mu);
+
+/* Constraint maps on host vectors (copied through the device) and on device
+ * vectors.  out = A u (length nconstraints) or A^T u (length dimx). */
+int v2g_apply_A(v2g_handle* h, const double* u, double* out);
+int v2g_apply_AT(v2g_handle* h, const double* u, double* out);
+int v2g_apply_A_device(v2g_handle* h, const double* d_u, double* d_out);
+int v2g_apply_AT_device(v2g_handle* h, const double* d_u, double* d_out);
+
+/* One projection step on the handle's state, as Update_xz: with
+ * U = A^T y - c + mu x per block, x = U+/mu and z = -U-. */
+int v2g_update_xz(v2g_handle* h, double mu);
+
+/* The full BPSDP solve from the handle's current state. */
+int v2g_solve(v2g_handle* h, v2g_result* res);
+
+/* Solves count independent problems in one GPU run.  Handles with the same
+ * layout share index tables; each keeps its own convergence test and stops
+ * independently.  Returns V2G_OK when every instance converged. */
+int v2g_solve_batch(v2g_handle** hs, int count, v2g_result* res);
+
+/* The constraint matrix A (nconstraints x dimx) as CSR, built on the host;
+ * no GPU needed.  v2g_A_nnz gives the entry count; v2g_export_A fills
+ * rowptr (nconstraints + 1), col and val (nnz each).  These expose the
+ * operator that bpsdp_Au applies (v2rdm_solver.cc:3020-3065) for inspection
+ * and for integrations that apply it themselves. */
+long v2g_A_nnz(v2g_handle* h);
+int v2g_export_A(v2g_handle* h, long* rowptr, int* col, double* val);
+
+/* Per-iteration trace (oiter, iiter, E(p), E(d), gap, mu, eps(p), eps(d)) of
+ * the last solve when record_trace was set; returns the number of rows. */
+long v2g_trace(const v2g_handle* h, double* rows, long cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* V2RDM_GPU_H */

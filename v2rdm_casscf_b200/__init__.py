@@ -1,0 +1,321 @@
+"""B200 boundary-point SDP solver for the active-space hot path of v2RDM-CASSCF.
+
+Python mirror of the plugin surface over the C ABI in include/v2rdm_gpu.h
+(libv2rdm_b200.so, built in-tree by ``v2rdm_casscf_b200.build``).  Option names
+and defaults follow the plugin's read_options (plugin.cc:66-124); the solver
+object follows v2RDMSolver (v2rdm_solver.h:79-575): its primal/dual vectors x,
+y, z, the PSD block list ``dimensions``, and ``compute_energy``.
+
+The solve runs on the GPU only.  If the library is missing, importing works but
+creating a solver raises; there is no CPU path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import hamiltonian  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libv2rdm_b200.so")
+
+V2G_OK = 0
+V2G_ERR_ARG = -1
+V2G_ERR_CUDA = -2
+V2G_ERR_NOT_CONVERGED = -3
+V2G_ERR_NONFINITE = -4
+V2G_ERR_UNSUPPORTED = -5
+V2G_ERR_NO_DEVICE = -6
+
+# Functions declared in include/v2rdm_gpu.h (checked by the tests).
+EXPORTS = [
+    "v2g_default_options", "v2g_last_error", "v2g_create", "v2g_destroy", "v2g_dimx", "v2g_nconstraints",
+    "v2g_nblocks", "v2g_block_dims", "v2g_set_hamiltonian", "v2g_get_c", "v2g_get_b", "v2g_efzc",
+    "v2g_guess_random", "v2g_set_state", "v2g_get_state", "v2g_apply_A", "v2g_apply_AT", "v2g_apply_A_device",
+    "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
+    "v2g_trace",
+]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("positivity", ctypes.c_char_p),
+        ("constrain_spin", ctypes.c_int),
+        ("constrain_sz", ctypes.c_int),
+        ("r_convergence", ctypes.c_double),
+        ("e_convergence", ctypes.c_double),
+        ("cg_convergence", ctypes.c_double),
+        ("maxiter", ctypes.c_int),
+        ("cg_maxiter", ctypes.c_int),
+        ("tau_parameter", ctypes.c_double),
+        ("mu_update_frequency", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("record_trace", ctypes.c_int),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("e_total", ctypes.c_double),
+        ("e_primal", ctypes.c_double),
+        ("e_dual", ctypes.c_double),
+        ("ep", ctypes.c_double),
+        ("ed", ctypes.c_double),
+        ("mu", ctypes.c_double),
+        ("efzc", ctypes.c_double),
+        ("enuc", ctypes.c_double),
+        ("oiter", ctypes.c_long),
+        ("iiter", ctypes.c_long),
+        ("status", ctypes.c_int),
+        ("t_cg", ctypes.c_double),
+        ("t_xz", ctypes.c_double),
+        ("t_total", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """The loaded solver library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m v2rdm_casscf_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, D, L_ = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
+        IP = ctypes.POINTER(ctypes.c_int)
+        DP = ctypes.POINTER(ctypes.c_double)
+        LP = ctypes.POINTER(ctypes.c_long)
+        L.v2g_default_options.argtypes = [ctypes.POINTER(Options)]
+        L.v2g_last_error.restype = ctypes.c_char_p
+        L.v2g_create.argtypes = [ctypes.POINTER(Options), I, IP, IP, IP, IP, IP, I, I, I, ctypes.POINTER(P)]
+        L.v2g_destroy.argtypes = [P]
+        for f in ("v2g_dimx", "v2g_nconstraints", "v2g_A_nnz"):
+            getattr(L, f).restype = L_
+            getattr(L, f).argtypes = [P]
+        L.v2g_nblocks.argtypes = [P]
+        L.v2g_block_dims.argtypes = [P, IP]
+        L.v2g_set_hamiltonian.argtypes = [P, DP, DP, I, D]
+        L.v2g_get_c.argtypes = [P, DP]
+        L.v2g_get_b.argtypes = [P, DP]
+        L.v2g_efzc.restype = D
+        L.v2g_efzc.argtypes = [P]
+        L.v2g_guess_random.argtypes = [P]
+        L.v2g_set_state.argtypes = [P, DP, DP, DP, D]
+        L.v2g_get_state.argtypes = [P, DP, DP, DP, DP]
+        for f in ("v2g_apply_A", "v2g_apply_AT"):
+            getattr(L, f).argtypes = [P, DP, DP]
+        for f in ("v2g_apply_A_device", "v2g_apply_AT_device"):
+            getattr(L, f).argtypes = [P, P, P]
+        L.v2g_update_xz.argtypes = [P, D]
+        L.v2g_solve.argtypes = [P, ctypes.POINTER(Result)]
+        L.v2g_solve_batch.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(Result)]
+        L.v2g_export_A.argtypes = [P, LP, IP, DP]
+        L.v2g_trace.restype = L_
+        L.v2g_trace.argtypes = [P, DP, L_]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class V2GError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"v2g error {code}: {msg}")
+        self.code = code
+
+
+def _check(code):
+    if code != V2G_OK:
+        raise V2GError(code, lib().v2g_last_error().decode())
+
+
+# Plugin options on this path and their defaults (plugin.cc:66-124).
+DEFAULT_OPTIONS = dict(
+    POSITIVITY="DQG",
+    CONSTRAIN_SPIN=True,
+    CONSTRAIN_SZ=True,
+    R_CONVERGENCE=1e-4,
+    E_CONVERGENCE=1e-4,
+    CG_CONVERGENCE=1e-9,
+    MAXITER=10000,
+    CG_MAXITER=10000,
+    TAU_PARAMETER=1.0,
+    MU_UPDATE_FREQUENCY=500,
+)
+
+
+class V2RDMSolver:
+    """One active-space BPSDP problem on the GPU.
+
+    Parameters mirror Psi4's per-irrep orbital arrays (FROZEN_DOCC,
+    RESTRICTED_DOCC, ACTIVE, RESTRICTED_UOCC, FROZEN_UOCC) and the reference
+    wavefunction's nalpha/nbeta/multiplicity; ``options`` takes the plugin's
+    option names.
+    """
+
+    def __init__(self, active, nalpha, nbeta, multiplicity=1, frozen_docc=None, restricted_docc=None,
+                 restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False):
+        L = lib()
+        opts = dict(DEFAULT_OPTIONS)
+        for k, v in (options or {}).items():
+            k = k.upper()
+            if k not in opts:
+                raise KeyError(f"unknown option {k}")
+            opts[k] = v
+        self.options = opts
+        o = Options()
+        L.v2g_default_options(ctypes.byref(o))
+        self._pos = str(opts["POSITIVITY"]).upper().encode()
+        o.positivity = self._pos
+        o.constrain_spin = int(bool(opts["CONSTRAIN_SPIN"]))
+        o.constrain_sz = int(bool(opts["CONSTRAIN_SZ"]))
+        o.r_convergence = float(opts["R_CONVERGENCE"])
+        o.e_convergence = float(opts["E_CONVERGENCE"])
+        o.cg_convergence = float(opts["CG_CONVERGENCE"])
+        o.maxiter = int(opts["MAXITER"])
+        o.cg_maxiter = int(opts["CG_MAXITER"])
+        o.tau_parameter = float(opts["TAU_PARAMETER"])
+        o.mu_update_frequency = int(opts["MU_UPDATE_FREQUENCY"])
+        o.device = int(device)
+        o.record_trace = int(bool(record_trace))
+        nirrep = len(active)
+        zero = [0] * nirrep
+        arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)
+                for v in (frozen_docc, restricted_docc, active, restricted_uocc, frozen_uocc)]
+        self.spaces = arrs
+        h = ctypes.c_void_p()
+        _check(L.v2g_create(ctypes.byref(o), nirrep, *[_ip(a) for a in arrs], int(nalpha), int(nbeta),
+                            int(multiplicity), ctypes.byref(h)))
+        self.h = h
+        self.nirrep = nirrep
+        self.dimx = L.v2g_dimx(h)
+        self.nconstraints = L.v2g_nconstraints(h)
+        nb = L.v2g_nblocks(h)
+        dims = np.zeros(nb, dtype=np.int32)
+        L.v2g_block_dims(h, _ip(dims))
+        self.dimensions = dims
+        self.result = None
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            lib().v2g_destroy(h)
+            self.h = None
+
+    # -- inputs ---------------------------------------------------------------
+    def set_hamiltonian(self, oei_packed, qmo, nq, enuc=0.0):
+        oei = np.ascontiguousarray(oei_packed, dtype=np.float64)
+        q = np.ascontiguousarray(qmo, dtype=np.float64)
+        _check(lib().v2g_set_hamiltonian(self.h, _dp(oei), _dp(q), int(nq), float(enuc)))
+
+    @classmethod
+    def from_active_space(cls, space, options=None, **kw):
+        """Solver for a hamiltonian.ActiveSpace (all orbitals active, C1)."""
+        s = cls([space.n], space.na, space.nb, space.multiplicity, options=options, **kw)
+        s.set_hamiltonian(space.oei_packed, space.qmo, space.nq, space.enuc)
+        return s
+
+    @property
+    def c(self):
+        out = np.zeros(self.dimx)
+        _check(lib().v2g_get_c(self.h, _dp(out)))
+        return out
+
+    @property
+    def b(self):
+        out = np.zeros(self.nconstraints)
+        _check(lib().v2g_get_b(self.h, _dp(out)))
+        return out
+
+    @property
+    def efzc(self):
+        return lib().v2g_efzc(self.h)
+
+    def guess(self):
+        """The plugin's TPDM_GUESS=RANDOM start (srand(0))."""
+        _check(lib().v2g_guess_random(self.h))
+
+    def set_state(self, x, y, z, mu=1.0):
+        x, y, z = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z))
+        assert x.size == self.dimx and z.size == self.dimx and y.size == self.nconstraints
+        _check(lib().v2g_set_state(self.h, _dp(x), _dp(y), _dp(z), float(mu)))
+
+    def get_state(self):
+        x, z = np.zeros(self.dimx), np.zeros(self.dimx)
+        y = np.zeros(self.nconstraints)
+        mu = ctypes.c_double()
+        _check(lib().v2g_get_state(self.h, _dp(x), _dp(y), _dp(z), ctypes.byref(mu)))
+        return x, y, z, mu.value
+
+    # -- maps -------------------------------------------------------------------
+    def Au(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.size == self.dimx
+        out = np.zeros(self.nconstraints)
+        _check(lib().v2g_apply_A(self.h, _dp(u), _dp(out)))
+        return out
+
+    def ATu(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.size == self.nconstraints
+        out = np.zeros(self.dimx)
+        _check(lib().v2g_apply_AT(self.h, _dp(u), _dp(out)))
+        return out
+
+    def A_csr(self):
+        """(rowptr, col, val) of A, built on the host."""
+        L = lib()
+        nnz = L.v2g_A_nnz(self.h)
+        if nnz < 0:
+            raise V2GError(V2G_ERR_UNSUPPORTED, "constraint table not available")
+        rowptr = np.zeros(self.nconstraints + 1, dtype=np.int64)
+        col = np.zeros(nnz, dtype=np.int32)
+        val = np.zeros(nnz)
+        _check(L.v2g_export_A(self.h, rowptr.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), _ip(col), _dp(val)))
+        return rowptr, col, val
+
+    def update_xz(self, mu):
+        _check(lib().v2g_update_xz(self.h, float(mu)))
+
+    # -- solve ------------------------------------------------------------------
+    def compute_energy(self):
+        """Runs the BPSDP loop; returns the total energy (raises if not converged)."""
+        r = Result()
+        code = lib().v2g_solve(self.h, ctypes.byref(r))
+        self.result = r.as_dict()
+        if code == V2G_ERR_NOT_CONVERGED:
+            raise V2GError(code, "v2RDM did not converge.")
+        _check(code)
+        return r.e_total
+
+    def trace(self):
+        L = lib()
+        n = L.v2g_trace(self.h, None, 0)
+        rows = np.zeros(8 * max(n, 1))
+        L.v2g_trace(self.h, _dp(rows), n)
+        return rows[: 8 * n].reshape(n, 8)
+
+
+def solve_batch(solvers):
+    """Solves many problems in one GPU run; returns one result dict per solver."""
+    n = len(solvers)
+    hs = (ctypes.c_void_p * n)(*[s.h.value for s in solvers])
+    res = (Result * n)()
+    code = lib().v2g_solve_batch(hs, n, res)
+    if code not in (V2G_OK, V2G_ERR_NOT_CONVERGED, V2G_ERR_NONFINITE):
+        _check(code)
+    out = [r.as_dict() for r in res]
+    for s, r in zip(solvers, out):
+        s.result = r
+    return out

@@ -1,0 +1,550 @@
+// Constraint rows, b and c (see constraints.h).
+#include "constraints.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace v2g {
+
+namespace {
+
+// Collects one row at a time; entries hitting the same primal element are
+// summed, exact zeros dropped, and columns sorted.
+class RowSink {
+  public:
+    explicit RowSink(Csr& A) : A_(A) {
+        A_.rowptr.assign(1, 0);
+        A_.col.clear();
+        A_.val.clear();
+    }
+    void add(int64_t c, double v) { cur_.push_back({c, v}); }
+    void end() {
+        std::sort(cur_.begin(), cur_.end(), [](const E& a, const E& b) { return a.c < b.c; });
+        size_t k = 0;
+        while (k < cur_.size()) {
+            int64_t c = cur_[k].c;
+            double s = 0.0;
+            while (k < cur_.size() && cur_[k].c == c) s += cur_[k++].v;
+            if (s != 0.0) {
+                A_.col.push_back((int32_t)c);
+                A_.val.push_back(s);
+            }
+        }
+        A_.rowptr.push_back((int64_t)A_.col.size());
+        cur_.clear();
+    }
+    int64_t rows() const { return (int64_t)A_.rowptr.size() - 1; }
+
+  private:
+    struct E {
+        int64_t c;
+        double v;
+    };
+    Csr& A_;
+    std::vector<E> cur_;
+};
+
+// D1-type element (p,q) of a family stored per irrep as amopi x amopi blocks;
+// p and q are absolute active indices of the same irrep.
+inline int64_t d1(const Layout& L, Fam f, int p, int q) {
+    const int h = L.symmetry[p];
+    const int o = L.pitzer_offset[h];
+    return L.off[f][h] + (int64_t)(p - o) * L.amopi[h] + (q - o);
+}
+inline int64_t gem(const Layout& L, Fam f, int h, int64_t dim, int r, int c) {
+    return L.off[f][h] + (int64_t)r * dim + c;
+}
+
+// d2.cc:296-547 (D2_constraints_Au)
+void rows_d2(const Layout& L, RowSink& S) {
+    const int n = L.amo;
+    const auto& o = L.off;
+    if (L.opt.constrain_sz) {
+        // Tr(D2ab), Tr(D2aa), Tr(D2bb): d2.cc:301-346
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                int h = L.sym_pair(L.symmetry[i], L.symmetry[j]);
+                int ij = L.ab(h, i, j);
+                S.add(gem(L, F_D2AB, h, L.gems_ab[h], ij, ij), 1.0);
+            }
+        S.end();
+        for (Fam f : {F_D2AA, F_D2BB}) {
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    if (i == j) continue;
+                    int h = L.sym_pair(L.symmetry[i], L.symmetry[j]);
+                    int ij = L.aa(h, i, j);
+                    S.add(gem(L, f, h, L.gems_aa[h], ij, ij), 1.0);
+                }
+            S.end();
+        }
+    } else {
+        // Tr(D2ab + D2aa + D2bb): d2.cc:347-367
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                int h = L.sym_pair(L.symmetry[i], L.symmetry[j]);
+                int ij = L.ab(h, i, j);
+                S.add(gem(L, F_D2AB, h, L.gems_ab[h], ij, ij), 2.0);
+                if (i == j) continue;
+                ij = L.aa(h, i, j);
+                S.add(gem(L, F_D2AA, h, L.gems_aa[h], ij, ij), 1.0);
+                S.add(gem(L, F_D2BB, h, L.gems_aa[h], ij, ij), 1.0);
+            }
+        S.end();
+    }
+    // D1 + Q1 = I: row (i,j) = D1(j,i) + Q1(i,j), d2.cc:369-387
+    for (Fam fd : {F_D1A, F_D1B}) {
+        Fam fq = (fd == F_D1A) ? F_Q1A : F_Q1B;
+        for (int h = 0; h < L.nirrep; h++)
+            for (int i = 0; i < L.amopi[h]; i++)
+                for (int j = 0; j < L.amopi[h]; j++) {
+                    S.add(o[fd][h] + (int64_t)j * L.amopi[h] + i, 1.0);
+                    S.add(o[fq][h] + (int64_t)i * L.amopi[h] + j, 1.0);
+                    S.end();
+                }
+    }
+    const double na = L.na, nb = L.nb, ntot = na + nb;
+    // contraction rows D2 -> D1
+    auto ab_to_d1 = [&](Fam fd, double coef, bool alpha, bool with_aa, Fam faa) {
+        for (int h = 0; h < L.nirrep; h++)
+            for (int i = 0; i < L.amopi[h]; i++)
+                for (int j = 0; j < L.amopi[h]; j++) {
+                    int ii = i + L.pitzer_offset[h], jj = j + L.pitzer_offset[h];
+                    S.add(o[fd][h] + (int64_t)i * L.amopi[h] + j, coef);
+                    for (int k = 0; k < n; k++) {
+                        int h2 = L.sym_pair(L.symmetry[ii], L.symmetry[k]);
+                        int ik = alpha ? L.ab(h2, ii, k) : L.ab(h2, k, ii);
+                        int jk = alpha ? L.ab(h2, jj, k) : L.ab(h2, k, jj);
+                        S.add(gem(L, F_D2AB, h2, L.gems_ab[h2], ik, jk), -1.0);
+                    }
+                    if (with_aa) {
+                        for (int k = 0; k < n; k++) {
+                            if (ii == k || jj == k) continue;
+                            int h2 = L.sym_pair(L.symmetry[ii], L.symmetry[k]);
+                            int ik = L.aa(h2, ii, k), jk = L.aa(h2, jj, k);
+                            int s = ((ii < k) ? 1 : -1) * ((jj < k) ? 1 : -1);
+                            S.add(gem(L, faa, h2, L.gems_aa[h2], ik, jk), -(double)s);
+                        }
+                    }
+                    S.end();
+                }
+    };
+    auto aa_to_d1 = [&](Fam fd, double coef, Fam faa) {
+        for (int h = 0; h < L.nirrep; h++)
+            for (int i = 0; i < L.amopi[h]; i++)
+                for (int j = 0; j < L.amopi[h]; j++) {
+                    int ii = i + L.pitzer_offset[h], jj = j + L.pitzer_offset[h];
+                    S.add(o[fd][h] + (int64_t)i * L.amopi[h] + j, coef);
+                    for (int k = 0; k < n; k++) {
+                        if (ii == k || jj == k) continue;
+                        int h2 = L.sym_pair(L.symmetry[ii], L.symmetry[k]);
+                        int ik = L.aa(h2, ii, k), jk = L.aa(h2, jj, k);
+                        int s = ((ii < k) ? 1 : -1) * ((jj < k) ? 1 : -1);
+                        S.add(gem(L, faa, h2, L.gems_aa[h2], ik, jk), -(double)s);
+                    }
+                    S.end();
+                }
+    };
+    if (!L.opt.constrain_sz) {
+        // d2.cc:395-458
+        ab_to_d1(F_D1A, ntot - 1.0, true, true, F_D2AA);
+        ab_to_d1(F_D1B, ntot - 1.0, false, true, F_D2BB);
+    } else {
+        // d2.cc:459-545
+        ab_to_d1(F_D1A, nb, true, false, F_D2AA);
+        ab_to_d1(F_D1B, na, false, false, F_D2AA);
+        aa_to_d1(F_D1A, na - 1.0, F_D2AA);
+        aa_to_d1(F_D1B, nb - 1.0, F_D2BB);
+    }
+}
+
+// spin.cc:274-493 (Spin_constraints_Au)
+void rows_spin(const Layout& L, RowSink& S) {
+    const int n = L.amo;
+    const auto& o = L.off;
+    // <S^2> row, spin.cc:280-291
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            int h = L.sym_pair(L.symmetry[i], L.symmetry[j]);
+            S.add(gem(L, F_D2AB, h, L.gems_ab[h], L.ab(h, i, j), L.ab(h, j, i)), 1.0);
+        }
+    S.end();
+    const double r2 = std::sqrt(2.0);
+    if (L.singlet()) {
+        // D1a = D1b, spin.cc:319-324
+        for (int h = 0; h < L.nirrep; h++)
+            for (int64_t k = 0; k < (int64_t)L.amopi[h] * L.amopi[h]; k++) {
+                S.add(o[F_D1A][h] + k, 1.0);
+                S.add(o[F_D1B][h] + k, -1.0);
+                S.end();
+            }
+        // D2aa = D2bb, spin.cc:326-331
+        for (int h = 0; h < L.nirrep; h++)
+            for (int64_t k = 0; k < (int64_t)L.gems_aa[h] * L.gems_aa[h]; k++) {
+                S.add(o[F_D2AA][h] + k, 1.0);
+                S.add(o[F_D2BB][h] + k, -1.0);
+                S.end();
+            }
+        // D2aa / D2bb = antisymmetrised D2ab, spin.cc:332-373
+        for (Fam f : {F_D2AA, F_D2BB}) {
+            for (int h = 0; h < L.nirrep; h++) {
+                const int ga = L.gems_aa[h], gb = L.gems_ab[h];
+                for (int ij = 0; ij < ga; ij++) {
+                    int i = L.bas_aa[h][ij][0], j = L.bas_aa[h][ij][1];
+                    int ijb = L.ab(h, i, j), jib = L.ab(h, j, i);
+                    for (int kl = 0; kl < ga; kl++) {
+                        int k = L.bas_aa[h][kl][0], l = L.bas_aa[h][kl][1];
+                        int klb = L.ab(h, k, l), lkb = L.ab(h, l, k);
+                        S.add(gem(L, f, h, ga, ij, kl), 1.0);
+                        S.add(gem(L, F_D2AB, h, gb, ijb, klb), -0.5);
+                        S.add(gem(L, F_D2AB, h, gb, jib, klb), 0.5);
+                        S.add(gem(L, F_D2AB, h, gb, ijb, lkb), 0.5);
+                        S.add(gem(L, F_D2AB, h, gb, jib, lkb), -0.5);
+                        S.end();
+                    }
+                }
+            }
+        }
+        // D200 = symmetrised D2ab, spin.cc:374-394
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_ab[h];
+            for (int ij = 0; ij < g; ij++) {
+                int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                int ji = L.ab(h, j, i);
+                double dij = (i == j) ? r2 : 1.0;
+                for (int kl = 0; kl < g; kl++) {
+                    int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                    int lk = L.ab(h, l, k);
+                    double dkl = (k == l) ? r2 : 1.0;
+                    double w = -0.5 / (dij * dkl);
+                    S.add(gem(L, F_D200, h, g, ij, kl), 1.0);
+                    S.add(gem(L, F_D2AB, h, g, ij, kl), w);
+                    S.add(gem(L, F_D2AB, h, g, ji, kl), w);
+                    S.add(gem(L, F_D2AB, h, g, ij, lk), w);
+                    S.add(gem(L, F_D2AB, h, g, ji, lk), w);
+                    S.end();
+                }
+            }
+        }
+    } else {
+        // non-singlets: the 2g x 2g block of D200/D201/D210/D211, spin.cc:395-468
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_ab[h];
+            for (int r = 0; r < 2 * g; r++)
+                for (int cc = 0; cc < 2 * g; cc++) {
+                    const int ij = r % g, kl = cc % g;
+                    const bool rb = r >= g, cb = cc >= g;
+                    int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                    int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                    int ji = L.ab(h, j, i), lk = L.ab(h, l, k);
+                    double dij = (i == j) ? r2 : 1.0, dkl = (k == l) ? r2 : 1.0;
+                    S.add(gem(L, F_D200, h, 2 * g, r, cc), 1.0);
+                    double a, b2, c2, d;  // coefficients of (ij,kl), (ji,kl), (ij,lk), (ji,lk)
+                    if (!rb && !cb) {
+                        a = b2 = c2 = d = -0.5 / (dij * dkl);
+                    } else if (!rb && cb) {
+                        a = -0.5 / dij; c2 = 0.5 / dij; b2 = -0.5 / dij; d = 0.5 / dij;
+                    } else if (rb && !cb) {
+                        a = -0.5 / dkl; c2 = -0.5 / dkl; b2 = 0.5 / dkl; d = 0.5 / dkl;
+                    } else {
+                        a = -0.5; b2 = 0.5; c2 = 0.5; d = -0.5;
+                    }
+                    S.add(gem(L, F_D2AB, h, g, ij, kl), a);
+                    S.add(gem(L, F_D2AB, h, g, ji, kl), b2);
+                    S.add(gem(L, F_D2AB, h, g, ij, lk), c2);
+                    S.add(gem(L, F_D2AB, h, g, ji, lk), d);
+                    S.end();
+                }
+        }
+    }
+    if (L.opt.constrain_g2) {
+        // maximal spin: sum_i G2ba(kl,ii) = 0 and sum_i G2ba(ii,kl) = 0, irrep 0
+        // only, spin.cc:470-491
+        const int g = L.gems_ab[0];
+        for (int kl = 0; kl < g; kl++) {
+            for (int i = 0; i < n; i++) S.add(gem(L, F_G2BA, 0, g, kl, L.ab(0, i, i)), 1.0);
+            S.end();
+        }
+        for (int kl = 0; kl < g; kl++) {
+            for (int i = 0; i < n; i++) S.add(gem(L, F_G2BA, 0, g, L.ab(0, i, i), kl), 1.0);
+            S.end();
+        }
+    }
+}
+
+// q2.cc:801-950 (Q2_constraints_Au, not spin adapted)
+void rows_q2(const Layout& L, RowSink& S) {
+    // Q2ab: D2ab(ij,kl) - Q2ab(ij,kl) - d_jl D1a(k,i) - d_ik D1b(l,j)
+    for (int h = 0; h < L.nirrep; h++) {
+        const int g = L.gems_ab[h];
+        for (int ij = 0; ij < g; ij++) {
+            int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+            for (int kl = 0; kl < g; kl++) {
+                int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                S.add(gem(L, F_D2AB, h, g, ij, kl), 1.0);
+                S.add(gem(L, F_Q2AB, h, g, ij, kl), -1.0);
+                if (j == l) S.add(d1(L, F_D1A, k, i), -1.0);
+                if (i == k) S.add(d1(L, F_D1B, l, j), -1.0);
+                S.end();
+            }
+        }
+    }
+    // Q2aa / Q2bb
+    for (int spin = 0; spin < 2; spin++) {
+        Fam fd2 = spin ? F_D2BB : F_D2AA, fq2 = spin ? F_Q2BB : F_Q2AA, fd1 = spin ? F_D1B : F_D1A;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_aa[h];
+            for (int ij = 0; ij < g; ij++) {
+                int i = L.bas_aa[h][ij][0], j = L.bas_aa[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    int k = L.bas_aa[h][kl][0], l = L.bas_aa[h][kl][1];
+                    S.add(gem(L, fd2, h, g, ij, kl), 1.0);
+                    S.add(gem(L, fq2, h, g, ij, kl), -1.0);
+                    if (j == l) S.add(d1(L, fd1, k, i), -1.0);
+                    if (j == k) S.add(d1(L, fd1, l, i), 1.0);
+                    if (i == l) S.add(d1(L, fd1, k, j), 1.0);
+                    if (i == k) S.add(d1(L, fd1, l, j), -1.0);
+                    S.end();
+                }
+            }
+        }
+    }
+}
+
+// g2.cc:1061-1260 (G2_constraints_Au, not spin adapted)
+void rows_g2(const Layout& L, RowSink& S) {
+    // G2ab: -G2ab(ij,kl) + d_jl D1a(i,k) - D2ab(il,kj)
+    // G2ba: -G2ba(ij,kl) + d_jl D1b(i,k) - D2ab(li,jk)
+    for (int which = 0; which < 2; which++) {
+        Fam fg = which ? F_G2BA : F_G2AB, fd1 = which ? F_D1B : F_D1A;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_ab[h];
+            for (int ij = 0; ij < g; ij++) {
+                int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                    S.add(gem(L, fg, h, g, ij, kl), -1.0);
+                    if (j == l) S.add(d1(L, fd1, i, k), 1.0);
+                    int h2 = L.sym_pair(L.symmetry[i], L.symmetry[l]);
+                    int g2 = L.gems_ab[h2];
+                    if (!which)
+                        S.add(gem(L, F_D2AB, h2, g2, L.ab(h2, i, l), L.ab(h2, k, j)), -1.0);
+                    else
+                        S.add(gem(L, F_D2AB, h2, g2, L.ab(h2, l, i), L.ab(h2, j, k)), -1.0);
+                    S.end();
+                }
+            }
+        }
+    }
+    // G2 2g x 2g block: aaaa | aabb / bbaa | bbbb, g2.cc:1131-1257
+    for (int h = 0; h < L.nirrep; h++) {
+        const int g = L.gems_ab[h];
+        for (int r = 0; r < 2 * g; r++)
+            for (int cc = 0; cc < 2 * g; cc++) {
+                const int ij = r % g, kl = cc % g;
+                const bool rb = r >= g, cb = cc >= g;
+                int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                int h2 = L.sym_pair(L.symmetry[i], L.symmetry[l]);
+                S.add(gem(L, F_G2AA, h, 2 * g, r, cc), -1.0);
+                if (rb == cb) {
+                    // G2aaaa / G2bbbb
+                    if (j == l) S.add(d1(L, rb ? F_D1B : F_D1A, i, k), 1.0);
+                    if (i != l && k != j) {
+                        int s = ((i < l) ? 1 : -1) * ((k < j) ? 1 : -1);
+                        int ga = L.gems_aa[h2];
+                        S.add(gem(L, rb ? F_D2BB : F_D2AA, h2, ga, L.aa(h2, i, l), L.aa(h2, k, j)), -(double)s);
+                    }
+                } else if (!rb) {
+                    // G2aabb: + D2ab(il,jk)
+                    S.add(gem(L, F_D2AB, h2, L.gems_ab[h2], L.ab(h2, i, l), L.ab(h2, j, k)), 1.0);
+                } else {
+                    // G2bbaa: + D2ab(li,kj)
+                    S.add(gem(L, F_D2AB, h2, L.gems_ab[h2], L.ab(h2, l, i), L.ab(h2, k, j)), 1.0);
+                }
+                S.end();
+            }
+    }
+}
+
+}  // namespace
+
+std::string build_A(const Layout& L, Csr& A) {
+    if (L.dimx >= (int64_t)INT32_MAX) return "primal vector too long for 32-bit column indices";
+    RowSink S(A);
+    rows_d2(L, S);
+    if (L.opt.constrain_spin) rows_spin(L, S);
+    if (L.opt.constrain_q2) rows_q2(L, S);
+    if (L.opt.constrain_g2) rows_g2(L, S);
+    if (L.opt.constrain_t1) return "T1 constraints are not built yet";
+    if (L.opt.constrain_t2) return "T2 constraints are not built yet";
+    A.nrows = S.rows();
+    A.ncols = L.dimx;
+    if (A.nrows != L.ncon) return "internal error: constraint row count mismatch";
+    return "";
+}
+
+void transpose(const Csr& A, Csr& AT) {
+    AT.nrows = A.ncols;
+    AT.ncols = A.nrows;
+    AT.rowptr.assign(AT.nrows + 1, 0);
+    for (int32_t c : A.col) AT.rowptr[c + 1]++;
+    for (int64_t r = 0; r < AT.nrows; r++) AT.rowptr[r + 1] += AT.rowptr[r];
+    AT.col.resize(A.col.size());
+    AT.val.resize(A.val.size());
+    std::vector<int64_t> fill(AT.rowptr.begin(), AT.rowptr.end() - 1);
+    for (int64_t r = 0; r < A.nrows; r++)
+        for (int64_t k = A.rowptr[r]; k < A.rowptr[r + 1]; k++) {
+            int64_t dst = fill[A.col[k]]++;
+            AT.col[dst] = (int32_t)r;
+            AT.val[dst] = A.val[k];
+        }
+}
+
+void build_b(const Layout& L, std::vector<double>& b) {
+    b.assign(L.ncon, 0.0);
+    int64_t o = 0;
+    const double na = L.na, nb = L.nb, ntot = na + nb;
+    if (L.opt.constrain_sz) {
+        b[o++] = na * nb;
+        b[o++] = na * (na - 1.0);
+        b[o++] = nb * (nb - 1.0);
+    } else {
+        b[o++] = ntot * (ntot - 1.0);
+    }
+    for (int s = 0; s < 2; s++)
+        for (int h = 0; h < L.nirrep; h++) {
+            for (int i = 0; i < L.amopi[h]; i++)
+                for (int j = 0; j < L.amopi[h]; j++) b[o + (int64_t)i * L.amopi[h] + j] = (i == j);
+            o += (int64_t)L.amopi[h] * L.amopi[h];
+        }
+    for (int h = 0; h < L.nirrep; h++) o += (L.opt.constrain_sz ? 4 : 2) * (int64_t)L.amopi[h] * L.amopi[h];
+    if (L.opt.constrain_spin) {
+        // "funny ab trace": N/2 + Ms^2 - Ms(Ms+1), v2rdm_solver.cc:2616-2618
+        double ms = (L.multiplicity - 1.0) / 2.0;
+        b[o++] = 0.5 * (na + nb) + ms * ms - ms * (ms + 1.0);
+        for (int h = 0; h < L.nirrep; h++) {
+            if (L.singlet())
+                o += (int64_t)L.amopi[h] * L.amopi[h] + 3 * (int64_t)L.gems_aa[h] * L.gems_aa[h] +
+                     (int64_t)L.gems_ab[h] * L.gems_ab[h];
+            else
+                o += 4 * (int64_t)L.gems_ab[h] * L.gems_ab[h];
+        }
+        if (L.opt.constrain_g2) o += 2 * (int64_t)L.gems_ab[0];
+    }
+    if (L.opt.constrain_q2) {
+        // v2rdm_solver.cc:2650-2695
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_ab[h];
+            for (int ij = 0; ij < g; ij++)
+                for (int kl = 0; kl < g; kl++) {
+                    int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                    int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                    b[o + (int64_t)ij * g + kl] = -(double)((i == k) * (j == l));
+                }
+            o += (int64_t)g * g;
+        }
+        for (int s = 0; s < 2; s++)
+            for (int h = 0; h < L.nirrep; h++) {
+                const int g = L.gems_aa[h];
+                for (int ij = 0; ij < g; ij++)
+                    for (int kl = 0; kl < g; kl++) {
+                        int i = L.bas_aa[h][ij][0], j = L.bas_aa[h][ij][1];
+                        int k = L.bas_aa[h][kl][0], l = L.bas_aa[h][kl][1];
+                        b[o + (int64_t)ij * g + kl] = -(double)((i == k) * (j == l)) + (double)((i == l) * (j == k));
+                    }
+                o += (int64_t)g * g;
+            }
+    }
+    // G2, T1 and T2 rows have b = 0.
+}
+
+std::string build_c(const Layout& L, const OrbitalSpaces& sp, const double* oei, const double* qmo, int nq,
+                    std::vector<double>& c, double& efzc) {
+    const int H = L.nirrep;
+    if ((int)sp.frzcpi.size() != H || (int)sp.rstcpi.size() != H || (int)sp.amopi.size() != H ||
+        (int)sp.rstvpi.size() != H || (int)sp.frzvpi.size() != H)
+        return "orbital space arrays must have nirrep entries";
+    for (int h = 0; h < H; h++)
+        if (sp.amopi[h] != L.amopi[h]) return "active orbitals per irrep differ from the layout";
+    // "full" space = all orbitals except frozen virtuals, Pitzer order.
+    std::vector<int> nfull(H), full_off(H), oei_off(H);
+    int nf = 0, no = 0;
+    for (int h = 0; h < H; h++) {
+        nfull[h] = sp.frzcpi[h] + sp.rstcpi[h] + sp.amopi[h] + sp.rstvpi[h];
+        full_off[h] = nf;
+        oei_off[h] = no;
+        nf += nfull[h];
+        no += nfull[h] * (nfull[h] + 1) / 2;
+    }
+    const int64_t ntri = (int64_t)nf * (nf + 1) / 2;
+    auto idx = [](int64_t i, int64_t j) { return i > j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; };
+    // TEI via the three-index factors, tei.cc:315-321
+    auto tei = [&](int i, int j, int k, int l) {
+        const double* a = qmo + idx(i, j);
+        const double* b = qmo + idx(k, l);
+        double s = 0.0;
+        for (int q = 0; q < nq; q++) s += a[q * ntri] * b[q * ntri];
+        return s;
+    };
+    // active orbital -> full-space index (basis.cc:122-129)
+    std::vector<int> full_basis(L.amo);
+    for (int h = 0; h < H; h++)
+        for (int i = 0; i < L.amopi[h]; i++)
+            full_basis[L.pitzer_offset[h] + i] = full_off[h] + sp.frzcpi[h] + sp.rstcpi[h] + i;
+
+    c.assign(L.dimx, 0.0);
+    // FrozenCoreEnergy, tei.cc:230-313
+    efzc = 0.0;
+    for (int h = 0; h < H; h++)
+        for (int i = 0; i < sp.frzcpi[h] + sp.rstcpi[h]; i++) {
+            int ifull = i + full_off[h];
+            efzc += 2.0 * oei[oei_off[h] + idx(i, i)];
+            for (int h2 = 0; h2 < H; h2++)
+                for (int j = 0; j < sp.frzcpi[h2] + sp.rstcpi[h2]; j++) {
+                    int jfull = j + full_off[h2];
+                    efzc += 2.0 * tei(ifull, ifull, jfull, jfull) - tei(ifull, jfull, ifull, jfull);
+                }
+        }
+    for (int h = 0; h < H; h++) {
+        const int core = sp.frzcpi[h] + sp.rstcpi[h];
+        for (int i = core; i < core + sp.amopi[h]; i++)
+            for (int j = core; j < core + sp.amopi[h]; j++) {
+                int ifull = i + full_off[h], jfull = j + full_off[h];
+                double dum = 0.0;
+                for (int h2 = 0; h2 < H; h2++)
+                    for (int k = 0; k < sp.frzcpi[h2] + sp.rstcpi[h2]; k++) {
+                        int kfull = k + full_off[h2];
+                        dum += 2.0 * tei(ifull, jfull, kfull, kfull) - tei(ifull, kfull, jfull, kfull);
+                    }
+                double v = oei[oei_off[h] + idx(i, j)] + dum;
+                int64_t e = (int64_t)(i - core) * L.amopi[h] + (j - core);
+                c[L.off[F_D1A][h] + e] = v;
+                c[L.off[F_D1B][h] + e] = v;
+            }
+    }
+    // RepackIntegrals two-electron part, tei.cc:144-228
+    for (int h = 0; h < H; h++) {
+        const int g = L.gems_ab[h];
+        for (int ij = 0; ij < g; ij++) {
+            int ii = full_basis[L.bas_ab[h][ij][0]], jj = full_basis[L.bas_ab[h][ij][1]];
+            for (int kl = 0; kl < g; kl++) {
+                int kk = full_basis[L.bas_ab[h][kl][0]], ll = full_basis[L.bas_ab[h][kl][1]];
+                c[L.off[F_D2AB][h] + (int64_t)ij * g + kl] = tei(ii, kk, jj, ll);
+            }
+        }
+        const int ga = L.gems_aa[h];
+        for (int ij = 0; ij < ga; ij++) {
+            int ii = full_basis[L.bas_aa[h][ij][0]], jj = full_basis[L.bas_aa[h][ij][1]];
+            for (int kl = 0; kl < ga; kl++) {
+                int kk = full_basis[L.bas_aa[h][kl][0]], ll = full_basis[L.bas_aa[h][kl][1]];
+                double v = tei(ii, kk, jj, ll) - tei(ii, ll, jj, kk);
+                c[L.off[F_D2AA][h] + (int64_t)ij * ga + kl] = v;
+                c[L.off[F_D2BB][h] + (int64_t)ij * ga + kl] = v;
+            }
+        }
+    }
+    return "";
+}
+
+}  // namespace v2g

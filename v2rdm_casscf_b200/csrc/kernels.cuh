@@ -1,0 +1,128 @@
+// Device kernels of the boundary-point SDP solver (declarations of the
+// host-side launchers).
+//
+// Vector layout: a group of B instances that share one constraint layout is
+// stored instance-interleaved, element e of instance b at [e * B + b].  A
+// gather through the shared index tables then reads B contiguous doubles per
+// table entry, and the table itself is read once for all B instances.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace v2g {
+
+struct DevCsr {
+    int64_t nrows = 0;
+    const int64_t* rowptr = nullptr;
+    const int32_t* col = nullptr;
+    const double* val = nullptr;
+};
+
+// out[r,b] = coef[b] * (sum_k val[k] in[col[k],b] - sub[r]) + add[r,b]
+// (each of sub, coef, add optional); instances with mask[b] == 0 are skipped.
+void launch_spmv(const DevCsr& A, int B, const double* in, double* out, const double* sub, const double* coef,
+                 const double* add, const int* mask, cudaStream_t s);
+
+// Per-instance reductions over interleaved vectors of n elements.
+enum ReduceMode {
+    RED_DOT = 0,      // sum u*v
+    RED_ED = 1,       // sum ((u + v) - w)^2       (dual error, v2rdm_solver.cc:1829-1832)
+    RED_EP = 2,       // sum (u - row[e])^2        (primal error, v2rdm_solver.cc:1835-1837)
+    RED_DOT_ROW = 3,  // sum u * row[e]            (b . y)
+};
+// Writes one value per instance to out[0..B).  partial must hold
+// reduce_partial_size(B) doubles.  Deterministic summation order.
+void launch_reduce(ReduceMode mode, int64_t n, int B, const double* u, const double* v, const double* w,
+                   const double* row, double* partial, double* out, cudaStream_t s);
+int64_t reduce_partial_size(int B);
+
+// z = c - z for active instances (v2rdm_solver.cc:1789-1790)
+void launch_c_minus_z(int64_t n, int B, const double* c, double* z, const int* mask, cudaStream_t s);
+
+// CG pieces (cg_solver.cc:125-177), per instance with cg_active masks.
+struct CgScalars {
+    double rr, pap, alpha, beta, rrnew, tol;
+    int active;   // still iterating
+    int iter;     // iter_ of the reference
+    int do_p;     // p update pending this iteration
+    int maxiter;
+};
+// r = rhs - Ap ; p = r
+void launch_cg_init(int64_t n, int B, const double* rhs, const double* Ap, double* r, double* p, const CgScalars* cs,
+                    cudaStream_t s);
+// alpha = rr / pap
+void launch_cg_alpha(int B, CgScalars* cs, const double* pap, cudaStream_t s);
+// y += alpha p ; r -= alpha Ap
+void launch_cg_update_yr(int64_t n, int B, double* y, double* r, const double* p, const double* Ap,
+                         const CgScalars* cs, cudaStream_t s);
+// convergence test and beta; counts instances still active into *n_active
+void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cudaStream_t s);
+// p = beta p + r
+void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s);
+// rr <- initial r.r
+void launch_cg_set_rr(int B, CgScalars* cs, const double* rr, int* n_active, cudaStream_t s);
+
+// ---- projection (Update_xz) ----------------------------------------------
+
+// Description of one PSD block of one instance.
+struct BlockTask {
+    int64_t xoff;   // offset of the block in the (per-instance) primal vector
+    int n;          // block dimension
+    int inst;       // instance index within the group (for interleaving)
+    int64_t woff;   // offset of the padded workspace matrix (large blocks)
+    int np;         // padded dimension (multiple of 64, large blocks)
+    int nb;         // number of 32-wide column blocks (np / 32)
+    int64_t qoff;   // offset of the pair-rotation buffer (large blocks)
+    int64_t doff;   // offset of the np-long weight vector (large blocks)
+};
+
+// Blocks with n <= 64: form U, diagonalise in shared memory, write x and z.
+void launch_small_project(const BlockTask* tasks, int ntasks, int B, const double* aty, const double* c, double* x,
+                          double* z, const double* mu, const int* mask, cudaStream_t s);
+
+// Large blocks (n > 64), block Jacobi on a padded np x np workspace.
+// U = sym(A^T y - c + mu x), zero padded.
+void launch_form_u(const BlockTask* tasks, int ntasks, int max_np, int B, const double* aty, const double* c,
+                   const double* x, const double* mu, const int* mask, double* Uw, cudaStream_t s);
+// W = U (cold start) and V = I
+void launch_cold_start(const BlockTask* tasks, int ntasks, int max_np, const double* Uw, double* Ww, double* Vw,
+                       const int* bmask, cudaStream_t s);
+// batched 64x64-tiled FP64 GEMM on the padded workspaces:
+// C = op(A) diag(d) op(B), with d optional.
+struct GemmTile {
+    int task;   // block task index
+    int ti, tj; // tile coordinates
+};
+void launch_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
+                 const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s);
+// One block-Jacobi round: solve each 64x64 pair problem, then rotate W and V.
+struct PairTask {
+    int task;   // block task
+    int k;      // pair index within the round
+};
+struct WTileTask {
+    int task, k1, k2;
+};
+struct VTileTask {
+    int task, chunk, k;
+};
+void launch_bj_solve(const BlockTask* tasks, const PairTask* pt, int npt, int round, double* Ww, double* Qbuf,
+                     const int* bmask, cudaStream_t s);
+void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, int round, double* Ww,
+                        const double* Qbuf, const int* bmask, cudaStream_t s);
+void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, int round, double* Vw,
+                        const double* Qbuf, const int* bmask, cudaStream_t s);
+// Per-block off-diagonal and total Frobenius norms of W; sets bmask[t] = 0
+// for blocks whose off-diagonal norm is below tol * total (converged).
+void launch_bj_check(const BlockTask* tasks, int ntasks, const double* Ww, double tol, int* bmask, int* n_open,
+                     cudaStream_t s);
+// d = max(diag(W), 0) / mu (per block, length np)
+void launch_pos_weights(const BlockTask* tasks, int ntasks, const double* Ww, const double* mu, double* dw,
+                        cudaStream_t s);
+// x = X (unpadded, interleaved) and z = mu X - U
+void launch_write_xz(const BlockTask* tasks, int ntasks, int max_n, int B, const double* Xw, const double* Uw,
+                     const double* mu, const int* mask, double* x, double* z, cudaStream_t s);
+
+}  // namespace v2g

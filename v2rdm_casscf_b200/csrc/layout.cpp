@@ -1,0 +1,253 @@
+// Layout of the boundary-point SDP (see layout.h for the reference map).
+#include "layout.h"
+
+#include <algorithm>
+
+namespace v2g {
+
+bool parse_positivity(const std::string& p, Options& o) {
+    // v2rdm_solver.cc:490-522
+    o.constrain_q2 = true;
+    o.constrain_g2 = true;
+    o.constrain_t1 = false;
+    o.constrain_t2 = false;
+    if (p == "D") {
+        o.constrain_q2 = false;
+        o.constrain_g2 = false;
+    } else if (p == "DQ") {
+        o.constrain_g2 = false;
+    } else if (p == "DG") {
+        o.constrain_q2 = false;
+    } else if (p == "DQG") {
+    } else if (p == "DQGT1") {
+        o.constrain_t1 = true;
+    } else if (p == "DQGT2") {
+        o.constrain_t2 = true;
+    } else if (p == "DQGT1T2" || p == "DQGT") {
+        o.constrain_t1 = true;
+        o.constrain_t2 = true;
+    } else {
+        return false;
+    }
+    return true;
+}
+
+static void build_geminals(Layout& L) {
+    const int n = L.amo, H = L.nirrep;
+    L.gems_ab.assign(H, 0);
+    L.gems_aa.assign(H, 0);
+    L.gems_00.assign(H, 0);
+    L.bas_ab.assign(H, {});
+    L.bas_aa.assign(H, {});
+    L.ibas_ab.assign(H, std::vector<int>(n * n, -1));
+    L.ibas_aa.assign(H, std::vector<int>(n * n, -1));
+    for (int h = 0; h < H; h++) {
+        // basis.cc:439-450 pushes (j,i) with i the outer index; basis.cc:526-546
+        // numbers ab pairs in that order and aa pairs as those with first > second.
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                if (L.sym_pair(L.symmetry[i], L.symmetry[j]) != h) continue;
+                const int p = j, q = i;
+                L.ibas_ab[h][p * n + q] = (int)L.bas_ab[h].size();
+                L.bas_ab[h].push_back({p, q});
+                if (p <= q) continue;
+                const int c = (int)L.bas_aa[h].size();
+                L.ibas_aa[h][p * n + q] = c;
+                L.ibas_aa[h][q * n + p] = c;
+                L.bas_aa[h].push_back({p, q});
+            }
+        L.gems_ab[h] = (int)L.bas_ab[h].size();
+        L.gems_aa[h] = (int)L.bas_aa[h].size();
+    }
+    // gems_00: unordered pairs i >= j per irrep (basis.cc:626-652)
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j <= i; j++) L.gems_00[L.sym_pair(L.symmetry[i], L.symmetry[j])]++;
+}
+
+static void build_triplets(Layout& L) {
+    // basis.cc:655-757: aba = all (i,j,k) of irrep h in i,j,k loop order;
+    // aab = those with i < j; aaa = those with i < j < k.
+    const int n = L.amo, H = L.nirrep;
+    L.trip_aaa.assign(H, 0);
+    L.trip_aab.assign(H, 0);
+    L.trip_aba.assign(H, 0);
+    L.bas_aaa.assign(H, {});
+    L.bas_aab.assign(H, {});
+    L.bas_aba.assign(H, {});
+    L.ibas_aaa.assign(H, std::vector<int>(n * n * n, -1));
+    L.ibas_aab.assign(H, std::vector<int>(n * n * n, -1));
+    L.ibas_aba.assign(H, std::vector<int>(n * n * n, -1));
+    auto at = [n](int i, int j, int k) { return (i * n + j) * n + k; };
+    for (int h = 0; h < H; h++) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                const int s1 = L.sym_pair(L.symmetry[i], L.symmetry[j]);
+                for (int k = 0; k < n; k++) {
+                    if (L.sym_pair(s1, L.symmetry[k]) != h) continue;
+                    L.ibas_aba[h][at(i, j, k)] = (int)L.bas_aba[h].size();
+                    L.bas_aba[h].push_back({i, j, k});
+                    if (i >= j) continue;
+                    const int c = (int)L.bas_aab[h].size();
+                    L.ibas_aab[h][at(i, j, k)] = c;
+                    L.ibas_aab[h][at(j, i, k)] = c;
+                    L.bas_aab[h].push_back({i, j, k});
+                    if (j >= k) continue;
+                    const int d = (int)L.bas_aaa[h].size();
+                    for (auto t : {at(i, j, k), at(i, k, j), at(j, i, k), at(j, k, i), at(k, i, j), at(k, j, i)})
+                        L.ibas_aaa[h][t] = d;
+                    L.bas_aaa[h].push_back({i, j, k});
+                }
+            }
+        L.trip_aaa[h] = (int)L.bas_aaa[h].size();
+        L.trip_aab[h] = (int)L.bas_aab[h].size();
+        L.trip_aba[h] = (int)L.bas_aba[h].size();
+    }
+}
+
+std::string build_layout(const Options& opt, int nirrep, const std::vector<int>& amopi, double na, double nb,
+                         int multiplicity, Layout& L) {
+    if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) return "nirrep must be 1, 2, 4 or 8";
+    if ((int)amopi.size() != nirrep) return "amopi must have nirrep entries";
+    if (opt.constrain_t1 || opt.constrain_t2) {
+        // (spin-adapted Q2/G2 are not offered, so the t1/t2 restriction of
+        // v2rdm_solver.cc:538-545 never triggers)
+    }
+    L = Layout();
+    L.opt = opt;
+    L.nirrep = nirrep;
+    L.amopi = amopi;
+    L.na = na;
+    L.nb = nb;
+    L.multiplicity = multiplicity;
+    L.amo = 0;
+    for (int h = 0; h < nirrep; h++) {
+        if (amopi[h] < 0) return "negative orbital count";
+        L.pitzer_offset.push_back(L.amo);
+        for (int i = 0; i < amopi[h]; i++) L.symmetry.push_back(h);
+        L.amo += amopi[h];
+    }
+    if (L.amo == 0) return "empty active space";
+    if (na < 0 || nb < 0 || na > L.amo || nb > L.amo) return "electron counts outside the active space";
+    build_geminals(L);
+    if (opt.constrain_t1 || opt.constrain_t2) build_triplets(L);
+
+    const int H = nirrep;
+    const auto& gab = L.gems_ab;
+    const auto& gaa = L.gems_aa;
+    const auto& amp = L.amopi;
+    for (auto& v : L.off) v.assign(H, -1);
+    int64_t o = 0;
+    auto place = [&](Fam f, const std::vector<int>& d, int mult) {
+        for (int h = 0; h < H; h++) {
+            L.off[f][h] = o;
+            o += (int64_t)mult * d[h] * mult * d[h];
+        }
+    };
+    auto tsum = [&](int h) { return L.trip_aab[h] + L.trip_aba[h]; };
+
+    // offsets in x, v2rdm_solver.cc:698-885
+    place(F_D2AB, gab, 1);
+    place(F_D2AA, gaa, 1);
+    place(F_D2BB, gaa, 1);
+    if (opt.constrain_spin) place(F_D200, gab, L.singlet() ? 1 : 2);
+    place(F_D1A, amp, 1);
+    place(F_D1B, amp, 1);
+    place(F_Q1A, amp, 1);
+    place(F_Q1B, amp, 1);
+    if (opt.constrain_q2) {
+        place(F_Q2AB, gab, 1);
+        place(F_Q2AA, gaa, 1);
+        place(F_Q2BB, gaa, 1);
+    }
+    if (opt.constrain_g2) {
+        place(F_G2AB, gab, 1);
+        place(F_G2BA, gab, 1);
+        place(F_G2AA, gab, 2);
+    }
+    if (opt.constrain_t1) {
+        place(F_T1AAA, L.trip_aaa, 1);
+        place(F_T1BBB, L.trip_aaa, 1);
+        place(F_T1AAB, L.trip_aab, 1);
+        place(F_T1BBA, L.trip_aab, 1);
+    }
+    if (opt.constrain_t2) {
+        std::vector<int> big(H);
+        for (int h = 0; h < H; h++) big[h] = tsum(h);
+        place(F_T2AAA, big, 1);
+        place(F_T2BBB, big, 1);
+        place(F_T2AAB, L.trip_aab, 1);
+        place(F_T2BBA, L.trip_aab, 1);
+    }
+    L.dimx = o;
+
+    // constraint count, v2rdm_solver.cc:887-1127
+    int64_t m = 0;
+    auto sq = [](int64_t a) { return a * a; };
+    m += opt.constrain_sz ? 3 : 1;
+    for (int h = 0; h < H; h++) m += 2 * sq(amp[h]);
+    for (int h = 0; h < H; h++) m += (opt.constrain_sz ? 4 : 2) * sq(amp[h]);
+    if (opt.constrain_spin) {
+        m += 1;
+        if (L.singlet()) {
+            for (int h = 0; h < H; h++) m += sq(amp[h]) + 3 * sq(gaa[h]) + sq(gab[h]);
+        } else {
+            for (int h = 0; h < H; h++) m += 4 * sq(gab[h]);
+        }
+        if (opt.constrain_g2) m += 2 * (int64_t)gab[0];
+    }
+    if (opt.constrain_q2)
+        for (int h = 0; h < H; h++) m += sq(gab[h]) + 2 * sq(gaa[h]);
+    if (opt.constrain_g2)
+        for (int h = 0; h < H; h++) m += 2 * sq(gab[h]) + sq(2 * gab[h]);
+    if (opt.constrain_t1)
+        for (int h = 0; h < H; h++) m += 2 * sq(L.trip_aaa[h]) + 2 * sq(L.trip_aab[h]);
+    if (opt.constrain_t2)
+        for (int h = 0; h < H; h++) m += 2 * sq(tsum(h)) + 2 * sq(L.trip_aab[h]);
+    L.ncon = m;
+
+    // block dimensions, v2rdm_solver.cc:1129-1270 (same order as the offsets)
+    auto dims = [&](const std::vector<int>& d, int mult) {
+        for (int h = 0; h < H; h++) L.block_dims.push_back(mult * d[h]);
+    };
+    dims(gab, 1);
+    dims(gaa, 1);
+    dims(gaa, 1);
+    if (opt.constrain_spin) dims(gab, L.singlet() ? 1 : 2);
+    dims(amp, 1);
+    dims(amp, 1);
+    dims(amp, 1);
+    dims(amp, 1);
+    if (opt.constrain_q2) {
+        dims(gab, 1);
+        dims(gaa, 1);
+        dims(gaa, 1);
+    }
+    if (opt.constrain_g2) {
+        dims(gab, 1);
+        dims(gab, 1);
+        dims(gab, 2);
+    }
+    if (opt.constrain_t1) {
+        dims(L.trip_aaa, 1);
+        dims(L.trip_aaa, 1);
+        dims(L.trip_aab, 1);
+        dims(L.trip_aab, 1);
+    }
+    if (opt.constrain_t2) {
+        std::vector<int> big(H);
+        for (int h = 0; h < H; h++) big[h] = tsum(h);
+        dims(big, 1);
+        dims(big, 1);
+        dims(L.trip_aab, 1);
+        dims(L.trip_aab, 1);
+    }
+    int64_t bo = 0;
+    for (int d : L.block_dims) {
+        L.block_off.push_back(bo);
+        bo += (int64_t)d * d;
+    }
+    if (bo != L.dimx) return "internal error: block dimensions do not tile the primal vector";
+    return "";
+}
+
+}  // namespace v2g

@@ -1,0 +1,237 @@
+// Constraint maps, CG vector kernels and per-instance reductions (FP64).
+//
+// The maps A and A^T are applied as gathers over CSR tables shared by all
+// instances of a group (see kernels.cuh for the interleaved layout).  A^T is
+// the transpose of A's table, so every primal element sums its contributing
+// constraints itself: no atomics, deterministic order, and the two maps are
+// exact adjoints.  These kernels are HBM-bound; their algorithmic traffic per
+// application is 8 * (dimx + nconstraints) bytes per instance.
+#include "kernels.cuh"
+
+namespace v2g {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int grid_for(int64_t work, int threads = kThreads) {
+    int64_t g = (work + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > 148 * 64) g = 148 * 64;
+    return (int)g;
+}
+
+__global__ void spmv_kernel(int64_t nrows, int B, const int64_t* __restrict__ rowptr,
+                            const int32_t* __restrict__ col, const double* __restrict__ val,
+                            const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ sub,
+                            const double* __restrict__ coef, const double* __restrict__ add,
+                            const int* __restrict__ mask) {
+    const int64_t total = nrows * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = t / B;
+        const int b = (int)(t - r * B);
+        if (mask && !mask[b]) continue;
+        double s = 0.0;
+        const int64_t k1 = rowptr[r + 1];
+        for (int64_t k = rowptr[r]; k < k1; k++) s += val[k] * in[(int64_t)col[k] * B + b];
+        if (sub) s -= sub[r];
+        if (coef) s *= coef[b];
+        if (add) s += add[t];
+        out[t] = s;
+    }
+}
+
+constexpr int kRedBlocks = 148 * 4;
+
+// Stage 1: block g reduces a contiguous chunk of elements for every instance;
+// thread t handles instance t % B on element rows t / B, t / B + T/B, ...
+__global__ void reduce_stage1(int mode, int64_t n, int B, const double* __restrict__ u, const double* __restrict__ v,
+                              const double* __restrict__ w, const double* __restrict__ row,
+                              double* __restrict__ partial) {
+    __shared__ double sh[kThreads];
+    const int rows_per_pass = blockDim.x / B;
+    const int lanes = rows_per_pass * B;
+    const int b = threadIdx.x % B;
+    const int rsub = threadIdx.x / B;
+    double acc = 0.0;
+    if (threadIdx.x < lanes) {
+        const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+        const int64_t e0 = blockIdx.x * chunk;
+        const int64_t e1 = (e0 + chunk < n) ? e0 + chunk : n;
+        for (int64_t e = e0 + rsub; e < e1; e += rows_per_pass) {
+            const int64_t i = e * B + b;
+            double term;
+            switch (mode) {
+                case RED_DOT: term = u[i] * v[i]; break;
+                case RED_ED: {
+                    double d = (u[i] + v[i]) - w[i];
+                    term = d * d;
+                    break;
+                }
+                case RED_EP: {
+                    double d = u[i] - row[e];
+                    term = d * d;
+                    break;
+                }
+                default: term = u[i] * row[e]; break;
+            }
+            acc += term;
+        }
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < B) {
+        double s = 0.0;
+        for (int k = 0; k < rows_per_pass; k++) s += sh[b + k * B];
+        partial[(int64_t)blockIdx.x * B + b] = s;
+    }
+}
+
+__global__ void reduce_stage2(int nblk, int B, const double* __restrict__ partial, double* __restrict__ out) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    double s = 0.0;
+    for (int k = 0; k < nblk; k++) s += partial[(int64_t)k * B + b];
+    out[b] = s;
+}
+
+__global__ void c_minus_z_kernel(int64_t n, int B, const double* __restrict__ c, double* __restrict__ z,
+                                 const int* __restrict__ mask) {
+    const int64_t total = n * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t % B);
+        if (mask && !mask[b]) continue;
+        z[t] = -z[t] + c[t];
+    }
+}
+
+__global__ void cg_init_kernel(int64_t n, int B, const double* __restrict__ rhs, const double* __restrict__ Ap,
+                               double* __restrict__ r, double* __restrict__ p, const CgScalars* __restrict__ cs) {
+    const int64_t total = n * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t % B);
+        if (!cs[b].active) continue;
+        const double v = rhs[t] - Ap[t];
+        r[t] = v;
+        p[t] = v;
+    }
+}
+
+__global__ void cg_set_rr_kernel(int B, CgScalars* cs, const double* rr, int* n_active) {
+    int cnt = 0;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) {
+        if (cs[b].active) {
+            cs[b].rr = rr[b];
+            cnt++;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    if (threadIdx.x == 0) *n_active = cnt;
+}
+
+__global__ void cg_alpha_kernel(int B, CgScalars* cs, const double* pap) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B || !cs[b].active) return;
+    cs[b].pap = pap[b];
+    cs[b].alpha = cs[b].rr / pap[b];
+}
+
+__global__ void cg_update_yr_kernel(int64_t n, int B, double* __restrict__ y, double* __restrict__ r,
+                                    const double* __restrict__ p, const double* __restrict__ Ap,
+                                    const CgScalars* __restrict__ cs) {
+    const int64_t total = n * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t % B);
+        if (!cs[b].active) continue;
+        const double a = cs[b].alpha;
+        y[t] += a * p[t];
+        r[t] += -a * Ap[t];
+    }
+}
+
+// One warp: per instance, test ||r|| < tol (cg_solver.cc:167-171), else beta
+// and iteration count; counts the instances still iterating.
+__global__ void cg_beta_kernel(int B, CgScalars* cs, const double* rrnew, int* n_active) {
+    int cnt = 0;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) {
+        CgScalars c = cs[b];
+        c.do_p = 0;
+        if (c.active) {
+            const double rn = rrnew[b];
+            const double nrm = sqrt(rn);
+            c.rrnew = rn;
+            if (!(nrm < c.tol)) {
+                c.beta = rn / c.rr;
+                c.rr = rn;
+                c.do_p = 1;
+                c.iter += 1;
+                if (c.iter >= c.maxiter) c.active = 0;
+            } else {
+                c.active = 0;
+            }
+            if (!isfinite(rn)) c.active = 0;
+        }
+        cnt += c.active;
+        cs[b] = c;
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    if (threadIdx.x == 0) *n_active = cnt;
+}
+
+__global__ void cg_update_p_kernel(int64_t n, int B, double* __restrict__ p, const double* __restrict__ r,
+                                   const CgScalars* __restrict__ cs) {
+    const int64_t total = n * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t % B);
+        if (!cs[b].do_p) continue;
+        p[t] = cs[b].beta * p[t] + r[t];
+    }
+}
+
+}  // namespace
+
+void launch_spmv(const DevCsr& A, int B, const double* in, double* out, const double* sub, const double* coef,
+                 const double* add, const int* mask, cudaStream_t s) {
+    spmv_kernel<<<grid_for(A.nrows * B), kThreads, 0, s>>>(A.nrows, B, A.rowptr, A.col, A.val, in, out, sub, coef,
+                                                           add, mask);
+}
+
+int64_t reduce_partial_size(int B) { return (int64_t)kRedBlocks * B; }
+
+void launch_reduce(ReduceMode mode, int64_t n, int B, const double* u, const double* v, const double* w,
+                   const double* row, double* partial, double* out, cudaStream_t s) {
+    reduce_stage1<<<kRedBlocks, kThreads, 0, s>>>((int)mode, n, B, u, v, w, row, partial);
+    reduce_stage2<<<(B + 127) / 128, 128, 0, s>>>(kRedBlocks, B, partial, out);
+}
+
+void launch_c_minus_z(int64_t n, int B, const double* c, double* z, const int* mask, cudaStream_t s) {
+    c_minus_z_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, c, z, mask);
+}
+
+void launch_cg_init(int64_t n, int B, const double* rhs, const double* Ap, double* r, double* p, const CgScalars* cs,
+                    cudaStream_t s) {
+    cg_init_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, rhs, Ap, r, p, cs);
+}
+void launch_cg_set_rr(int B, CgScalars* cs, const double* rr, int* n_active, cudaStream_t s) {
+    cg_set_rr_kernel<<<1, 32, 0, s>>>(B, cs, rr, n_active);
+}
+void launch_cg_alpha(int B, CgScalars* cs, const double* pap, cudaStream_t s) {
+    cg_alpha_kernel<<<(B + 127) / 128, 128, 0, s>>>(B, cs, pap);
+}
+void launch_cg_update_yr(int64_t n, int B, double* y, double* r, const double* p, const double* Ap,
+                         const CgScalars* cs, cudaStream_t s) {
+    cg_update_yr_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, y, r, p, Ap, cs);
+}
+void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cudaStream_t s) {
+    cg_beta_kernel<<<1, 32, 0, s>>>(B, cs, rrnew, n_active);
+}
+void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s) {
+    cg_update_p_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, p, r, cs);
+}
+
+}  // namespace v2g

@@ -1,0 +1,811 @@
+// Host driver of the B200 boundary-point SDP solver and the C ABI of
+// include/v2rdm_gpu.h.
+//
+// The outer loop restates v2RDMSolver::compute_energy (v2rdm_solver.cc:
+// 1778-1908) and CGSolver::solve (cg_solver.cc:125-177) step for step, for a
+// group of B instances at once: every instance keeps its own mu, CG
+// tolerance, iteration counts and stopping test, and is masked out of all
+// updates once it has converged.  All vector work runs on the device; the
+// host reads back four scalars per instance per outer iteration (the same
+// ones the reference prints) to run the stopping test and the mu update.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/v2rdm_gpu.h"
+#include "constraints.h"
+#include "kernels.cuh"
+#include "layout.h"
+
+namespace v2g {
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                                         \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            throw ::v2g::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + __FILE__ + ":" + \
+                            std::to_string(__LINE__));                                                   \
+    } while (0)
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    void alloc(size_t count) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = count;
+        if (count) {
+            CK(cudaMalloc(&p, count * sizeof(T)));
+            CK(cudaMemset(p, 0, count * sizeof(T)));
+        }
+    }
+    void upload(const T* h, size_t count) {
+        alloc(count);
+        if (count) CK(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
+    }
+};
+
+// Index tables and b for one layout, shared by every instance with it.
+struct DeviceTables {
+    Layout L;
+    int device = 0;
+    Csr hA;  // kept on the host for adjoint checks and the nnz count
+    DevBuf<int64_t> A_rowptr, AT_rowptr;
+    DevBuf<int32_t> A_col, AT_col;
+    DevBuf<double> A_val, AT_val;
+    DevBuf<double> b;
+    std::vector<double> hb;
+    DevCsr A() const { return DevCsr{L.ncon, A_rowptr.p, A_col.p, A_val.p}; }
+    DevCsr AT() const { return DevCsr{L.dimx, AT_rowptr.p, AT_col.p, AT_val.p}; }
+};
+
+std::string layout_key(const Layout& L, int device) {
+    std::ostringstream s;
+    const Options& o = L.opt;
+    s << device << '|' << o.constrain_q2 << o.constrain_g2 << o.constrain_t1 << o.constrain_t2 << o.constrain_spin
+      << o.constrain_sz << '|' << L.nirrep << '|';
+    for (int a : L.amopi) s << a << ',';
+    s << '|' << L.na << '|' << L.nb << '|' << L.multiplicity;
+    return s.str();
+}
+
+std::mutex g_cache_mu;
+std::map<std::string, std::weak_ptr<DeviceTables>> g_cache;
+
+std::shared_ptr<DeviceTables> get_tables(const Layout& L, int device) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    const std::string key = layout_key(L, device);
+    auto it = g_cache.find(key);
+    if (it != g_cache.end())
+        if (auto sp = it->second.lock()) return sp;
+    auto T = std::make_shared<DeviceTables>();
+    T->L = L;
+    T->device = device;
+    std::string err = build_A(L, T->hA);
+    if (!err.empty()) throw std::invalid_argument(err);
+    Csr AT;
+    transpose(T->hA, AT);
+    CK(cudaSetDevice(device));
+    T->A_rowptr.upload(T->hA.rowptr.data(), T->hA.rowptr.size());
+    T->A_col.upload(T->hA.col.data(), T->hA.col.size());
+    T->A_val.upload(T->hA.val.data(), T->hA.val.size());
+    T->AT_rowptr.upload(AT.rowptr.data(), AT.rowptr.size());
+    T->AT_col.upload(AT.col.data(), AT.col.size());
+    T->AT_val.upload(AT.val.data(), AT.val.size());
+    build_b(L, T->hb);
+    T->b.upload(T->hb.data(), T->hb.size());
+    g_cache[key] = T;
+    return T;
+}
+
+}  // namespace
+
+// One active-space problem (a v2g_handle).
+struct Problem {
+    Options opt;
+    Layout L;
+    OrbitalSpaces sp;
+    int device = 0;
+    bool record_trace = false;
+    std::vector<double> c, x, y, z;
+    double mu = 1.0;
+    double efzc = 0.0, enuc = 0.0;
+    bool have_c = false;
+    std::shared_ptr<DeviceTables> T;
+    std::vector<std::array<double, 8>> trace;
+
+    DeviceTables& tables() {
+        if (!T) T = get_tables(L, device);
+        return *T;
+    }
+};
+
+namespace {
+
+// Lock-step solve of B instances that share one layout.
+class GroupRun {
+  public:
+    GroupRun(DeviceTables& T, std::vector<Problem*> probs) : T_(T), P_(std::move(probs)), B_((int)P_.size()) {
+        if (B_ < 1 || B_ > 256) throw std::invalid_argument("a group holds 1..256 instances");
+        CK(cudaSetDevice(T.device));
+        CK(cudaStreamCreate(&s_));
+        nx_ = T.L.dimx;
+        nc_ = T.L.ncon;
+        const size_t X = (size_t)nx_ * B_, C = (size_t)nc_ * B_;
+        c_.alloc(X);
+        x_.alloc(X);
+        z_.alloc(X);
+        aty_.alloc(X);
+        atp_.alloc(X);
+        y_.alloc(C);
+        ax_.alloc(C);
+        bv_.alloc(C);
+        r_.alloc(C);
+        p_.alloc(C);
+        ap_.alloc(C);
+        partial_.alloc(reduce_partial_size(B_));
+        red_.alloc(4 * B_);
+        mu_.alloc(B_);
+        coef_.alloc(B_);
+        mask_.alloc(B_);
+        cs_.alloc(B_);
+        nact_.alloc(4);
+        CK(cudaMallocHost(&hscal_, sizeof(double) * 4 * B_));
+        CK(cudaMallocHost(&hnact_, sizeof(int) * 4));
+        build_projection_plan();
+        upload_state();
+    }
+    ~GroupRun() {
+        if (hscal_) cudaFreeHost(hscal_);
+        if (hnact_) cudaFreeHost(hnact_);
+        if (s_) cudaStreamDestroy(s_);
+    }
+
+    // Interleave host vectors of all instances into [e * B + b].
+    void upload_vec(DevBuf<double>& d, int64_t n, const std::vector<double> Problem::*member) {
+        std::vector<double> h((size_t)n * B_);
+        for (int b = 0; b < B_; b++) {
+            const auto& v = P_[b]->*member;
+            for (int64_t e = 0; e < n; e++) h[(size_t)e * B_ + b] = v[e];
+        }
+        CK(cudaMemcpy(d.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    void download_vec(const DevBuf<double>& d, int64_t n, std::vector<double> Problem::*member) {
+        std::vector<double> h((size_t)n * B_);
+        CK(cudaMemcpy(h.data(), d.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int b = 0; b < B_; b++) {
+            auto& v = P_[b]->*member;
+            v.resize(n);
+            for (int64_t e = 0; e < n; e++) v[e] = h[(size_t)e * B_ + b];
+        }
+    }
+    void upload_state() {
+        upload_vec(c_, nx_, &Problem::c);
+        upload_vec(x_, nx_, &Problem::x);
+        upload_vec(z_, nx_, &Problem::z);
+        upload_vec(y_, nc_, &Problem::y);
+        std::vector<double> mu(B_);
+        for (int b = 0; b < B_; b++) mu[b] = P_[b]->mu;
+        CK(cudaMemcpy(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice));
+        std::vector<int> m(B_, 1);
+        CK(cudaMemcpy(mask_.p, m.data(), B_ * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    void download_state() {
+        download_vec(x_, nx_, &Problem::x);
+        download_vec(z_, nx_, &Problem::z);
+        download_vec(y_, nc_, &Problem::y);
+    }
+
+    // Update_xz for every instance with mask set; ATy is left in aty_.
+    void project() {
+        launch_spmv(T_.AT(), B_, y_.p, aty_.p, nullptr, nullptr, nullptr, mask_.p, s_);
+        launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_);
+        if (nlarge_ == 0) return;
+        launch_form_u(large_d_.p, nlarge_, max_np_, B_, aty_.p, c_.p, x_.p, mu_.p, mask_.p, U_.p, s_);
+        // blocks of active instances take part
+        set_block_masks();
+        if (!warm_) {
+            launch_cold_start(large_d_.p, nlarge_, max_np_, U_.p, W_.p, V_.p, bact_.p, s_);
+        } else {
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bact_.p, s_);
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bact_.p, s_);
+        }
+        CK(cudaMemcpyAsync(bwork_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
+        const int max_sweeps = 30;
+        for (int sweep = 0; sweep < max_sweeps; sweep++) {
+            launch_bj_check(large_d_.p, nlarge_, W_.p, 1e-14, bwork_.p, nact_.p + 1, s_);
+            CK(cudaMemcpyAsync(hnact_ + 1, nact_.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s_));
+            CK(cudaStreamSynchronize(s_));
+            if (hnact_[1] == 0) break;
+            for (int g = 0; g < max_rounds_; g++) {
+                launch_bj_solve(large_d_.p, pairs_.p, npairs_, g, W_.p, Q_.p, bwork_.p, s_);
+                launch_bj_update_w(large_d_.p, wtiles_.p, nwtiles_, g, W_.p, Q_.p, bwork_.p, s_);
+                launch_bj_update_v(large_d_.p, vtiles_.p, nvtiles_, g, V_.p, Q_.p, bwork_.p, s_);
+            }
+            sweeps_total_++;
+        }
+        launch_pos_weights(large_d_.p, nlarge_, W_.p, mu_.p, dw_.p, s_);
+        launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, V_.p, true, dw_.p, Tm_.p, bact_.p, s_);
+        launch_write_xz(large_d_.p, nlarge_, max_n_, B_, Tm_.p, U_.p, mu_.p, mask_.p, x_.p, z_.p, s_);
+        warm_ = true;
+    }
+
+    void apply_A(const double* d_in, double* d_out) {
+        launch_spmv(T_.A(), B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
+    }
+    void apply_AT(const double* d_in, double* d_out) {
+        launch_spmv(T_.AT(), B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
+    }
+    cudaStream_t stream() const { return s_; }
+    DevBuf<double>& xbuf() { return x_; }
+    DevBuf<double>& ybuf() { return y_; }
+    DevBuf<double>& zbuf() { return z_; }
+    DevBuf<double>& mubuf() { return mu_; }
+
+    // The outer BPSDP loop.  Returns per-instance results.
+    void solve(std::vector<v2g_result>& res) {
+        const Options& o = T_.L.opt;
+        res.assign(B_, v2g_result{});
+        std::vector<double> mu(B_), ep(B_, 0.0), ed(B_, 0.0), egap(B_, 0.0);
+        std::vector<int> active(B_, 1), oiter(B_, 0);
+        std::vector<long> iiter(B_, 0);
+        std::vector<double> coef(B_);
+        for (int b = 0; b < B_; b++) {
+            mu[b] = P_[b]->mu;
+            P_[b]->trace.clear();
+            res[b].status = V2G_ERR_NOT_CONVERGED;
+        }
+        cudaEvent_t e0, e1, e2, e3;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventCreate(&e2));
+        CK(cudaEventCreate(&e3));
+        double t_cg = 0, t_xz = 0;
+        CK(cudaEventRecord(e3, s_));
+        std::vector<CgScalars> cs(B_);
+        int it = 0;
+        while (true) {
+            int nactive = 0;
+            for (int b = 0; b < B_; b++) nactive += active[b];
+            if (nactive == 0) break;
+            CK(cudaMemcpyAsync(mask_.p, active.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+            for (int b = 0; b < B_; b++) coef[b] = -o.tau * mu[b];
+            CK(cudaMemcpyAsync(coef_.p, coef.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+            CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+            CK(cudaEventRecord(e0, s_));
+            // Ax = -tau mu (A x - b); z <- c - z; B = A z + Ax   (:1783-1794)
+            launch_spmv(T_.A(), B_, x_.p, ax_.p, T_.b.p, coef_.p, nullptr, mask_.p, s_);
+            launch_c_minus_z(nx_, B_, c_.p, z_.p, mask_.p, s_);
+            launch_spmv(T_.A(), B_, z_.p, bv_.p, nullptr, nullptr, ax_.p, mask_.p, s_);
+            // CG tolerance (:1797-1805)
+            for (int b = 0; b < B_; b++) {
+                double tol;
+                if (oiter[b] == 0)
+                    tol = 0.01;
+                else
+                    tol = (ep[b] > ed[b]) ? 0.01 * ed[b] : 0.01 * ep[b];
+                if (tol < o.cg_convergence) tol = o.cg_convergence;
+                cs[b] = CgScalars{};
+                cs[b].tol = tol;
+                cs[b].active = active[b];
+                cs[b].maxiter = o.cg_maxiter;
+            }
+            CK(cudaMemcpyAsync(cs_.p, cs.data(), B_ * sizeof(CgScalars), cudaMemcpyHostToDevice, s_));
+            cg_solve();
+            CK(cudaMemcpyAsync(cs.data(), cs_.p, B_ * sizeof(CgScalars), cudaMemcpyDeviceToHost, s_));
+            CK(cudaEventRecord(e1, s_));
+            project();
+            CK(cudaEventRecord(e2, s_));
+            // ed = ||A^T y + z - c||, ep = ||A x - b||, E = c.x, b.y (:1826-1852)
+            launch_reduce(RED_ED, nx_, B_, aty_.p, z_.p, c_.p, nullptr, partial_.p, red_.p, s_);
+            launch_spmv(T_.A(), B_, x_.p, ax_.p, nullptr, nullptr, nullptr, mask_.p, s_);
+            launch_reduce(RED_EP, nc_, B_, ax_.p, nullptr, nullptr, T_.b.p, partial_.p, red_.p + B_, s_);
+            launch_reduce(RED_DOT, nx_, B_, c_.p, x_.p, nullptr, nullptr, partial_.p, red_.p + 2 * B_, s_);
+            launch_reduce(RED_DOT_ROW, nc_, B_, y_.p, nullptr, nullptr, T_.b.p, partial_.p, red_.p + 3 * B_, s_);
+            CK(cudaMemcpyAsync(hscal_, red_.p, 4 * B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+            CK(cudaStreamSynchronize(s_));
+            float ms_cg = 0, ms_xz = 0;
+            CK(cudaEventElapsedTime(&ms_cg, e0, e1));
+            CK(cudaEventElapsedTime(&ms_xz, e1, e2));
+            t_cg += ms_cg * 1e-3;
+            t_xz += ms_xz * 1e-3;
+            for (int b = 0; b < B_; b++) {
+                if (!active[b]) continue;
+                Problem& P = *P_[b];
+                ed[b] = std::sqrt(hscal_[b]);
+                ep[b] = std::sqrt(hscal_[B_ + b]);
+                const double e_p = hscal_[2 * B_ + b], e_d = hscal_[3 * B_ + b];
+                const long ii = cs[b].iter;
+                iiter[b] += ii;
+                if (oiter[b] % o.mu_update_frequency == 0 && oiter[b] > 0) mu[b] = mu[b] * ep[b] / ed[b];
+                const double shift = P.enuc + P.efzc;
+                if (P.record_trace)
+                    P.trace.push_back({(double)oiter[b], (double)ii, e_p + shift, e_d + shift, std::fabs(e_p - e_d),
+                                       mu[b], ep[b], ed[b]});
+                oiter[b]++;
+                res[b].e_primal = e_p + shift;
+                res[b].e_dual = e_d + shift;
+                res[b].e_total = e_p + shift;
+                res[b].ep = ep[b];
+                res[b].ed = ed[b];
+                res[b].mu = mu[b];
+                res[b].oiter = oiter[b];
+                res[b].iiter = iiter[b];
+                res[b].efzc = P.efzc;
+                res[b].enuc = P.enuc;
+                if (!std::isfinite(ep[b]) || !std::isfinite(ed[b]) || !std::isfinite(e_p)) {
+                    res[b].status = V2G_ERR_NONFINITE;
+                    active[b] = 0;
+                    continue;
+                }
+                if (oiter[b] == o.maxiter) {
+                    res[b].status = V2G_ERR_NOT_CONVERGED;
+                    active[b] = 0;
+                    continue;
+                }
+                egap[b] = std::fabs(e_p - e_d);
+                if (!(ep[b] > o.r_convergence || ed[b] > o.r_convergence || egap[b] > o.e_convergence)) {
+                    res[b].status = V2G_OK;
+                    active[b] = 0;
+                }
+            }
+            it++;
+        }
+        CK(cudaEventRecord(e2, s_));
+        CK(cudaEventSynchronize(e2));
+        float ms_tot = 0;
+        CK(cudaEventElapsedTime(&ms_tot, e3, e2));
+        for (int b = 0; b < B_; b++) {
+            res[b].t_cg = t_cg;
+            res[b].t_xz = t_xz;
+            res[b].t_total = ms_tot * 1e-3;
+            P_[b]->mu = mu[b];
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaEventDestroy(e2);
+        cudaEventDestroy(e3);
+        download_state();
+    }
+
+    long jacobi_sweeps() const { return sweeps_total_; }
+
+  private:
+    // CGSolver::solve for every instance whose CG scalars are active.
+    void cg_solve() {
+        // Ap = A A^T y ; r = B - Ap ; p = r
+        launch_spmv(T_.AT(), B_, y_.p, atp_.p, nullptr, nullptr, nullptr, nullptr, s_);
+        launch_spmv(T_.A(), B_, atp_.p, ap_.p, nullptr, nullptr, nullptr, nullptr, s_);
+        launch_cg_init(nc_, B_, bv_.p, ap_.p, r_.p, p_.p, cs_.p, s_);
+        launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
+        launch_cg_set_rr(B_, cs_.p, red_.p, nact_.p, s_);
+        const int check_every = 4;
+        for (int k = 0;; k++) {
+            launch_spmv(T_.AT(), B_, p_.p, atp_.p, nullptr, nullptr, nullptr, nullptr, s_);
+            launch_spmv(T_.A(), B_, atp_.p, ap_.p, nullptr, nullptr, nullptr, nullptr, s_);
+            launch_reduce(RED_DOT, nc_, B_, p_.p, ap_.p, nullptr, nullptr, partial_.p, red_.p, s_);
+            launch_cg_alpha(B_, cs_.p, red_.p, s_);
+            launch_cg_update_yr(nc_, B_, y_.p, r_.p, p_.p, ap_.p, cs_.p, s_);
+            launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
+            launch_cg_beta(B_, cs_.p, red_.p, nact_.p, s_);
+            launch_cg_update_p(nc_, B_, p_.p, r_.p, cs_.p, s_);
+            if ((k + 1) % check_every == 0) {
+                CK(cudaMemcpyAsync(hnact_, nact_.p, sizeof(int), cudaMemcpyDeviceToHost, s_));
+                CK(cudaStreamSynchronize(s_));
+                if (hnact_[0] == 0) break;
+            }
+        }
+    }
+
+    void set_block_masks() {
+        // bact[t] = mask[inst(t)], computed on the host copy of the task list
+        std::vector<int> act(B_);
+        CK(cudaMemcpyAsync(act.data(), mask_.p, B_ * sizeof(int), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
+        std::vector<int> bm(nlarge_);
+        for (int t = 0; t < nlarge_; t++) bm[t] = act[hlarge_[t].inst];
+        CK(cudaMemcpyAsync(bact_.p, bm.data(), nlarge_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+    }
+
+    void build_projection_plan() {
+        const Layout& L = T_.L;
+        std::vector<BlockTask> small;
+        int64_t woff = 0, qoff = 0, doff = 0;
+        for (int b = 0; b < B_; b++)
+            for (size_t k = 0; k < L.block_dims.size(); k++) {
+                const int n = L.block_dims[k];
+                if (n == 0) continue;
+                BlockTask t{};
+                t.xoff = L.block_off[k];
+                t.n = n;
+                t.inst = b;
+                if (n <= 64) {
+                    small.push_back(t);
+                    continue;
+                }
+                t.np = (n + 63) / 64 * 64;
+                t.nb = t.np / 32;
+                t.woff = woff;
+                t.qoff = qoff;
+                t.doff = doff;
+                woff += (int64_t)t.np * t.np;
+                qoff += (int64_t)(t.nb / 2) * 4096;
+                doff += t.np;
+                hlarge_.push_back(t);
+            }
+        nsmall_ = (int)small.size();
+        nlarge_ = (int)hlarge_.size();
+        small_d_.upload(small.data(), small.size());
+        large_d_.upload(hlarge_.data(), hlarge_.size());
+        if (nlarge_ == 0) return;
+        U_.alloc(woff);
+        W_.alloc(woff);
+        V_.alloc(woff);
+        Tm_.alloc(woff);
+        Q_.alloc(qoff);
+        dw_.alloc(doff);
+        bact_.alloc(nlarge_);
+        bwork_.alloc(nlarge_);
+        std::vector<GemmTile> gt;
+        std::vector<PairTask> pt;
+        std::vector<WTileTask> wt;
+        std::vector<VTileTask> vt;
+        for (int ti = 0; ti < nlarge_; ti++) {
+            const BlockTask& t = hlarge_[ti];
+            const int nt = t.np / 64, npair = t.nb / 2;
+            max_np_ = std::max(max_np_, t.np);
+            max_n_ = std::max(max_n_, t.n);
+            max_rounds_ = std::max(max_rounds_, t.nb - 1);
+            for (int i = 0; i < nt; i++)
+                for (int j = 0; j < nt; j++) gt.push_back({ti, i, j});
+            for (int k = 0; k < npair; k++) pt.push_back({ti, k});
+            for (int k1 = 0; k1 < npair; k1++)
+                for (int k2 = 0; k2 < npair; k2++) wt.push_back({ti, k1, k2});
+            for (int ch = 0; ch < nt; ch++)
+                for (int k = 0; k < npair; k++) vt.push_back({ti, ch, k});
+        }
+        gtiles_.upload(gt.data(), gt.size());
+        pairs_.upload(pt.data(), pt.size());
+        wtiles_.upload(wt.data(), wt.size());
+        vtiles_.upload(vt.data(), vt.size());
+        ngtiles_ = (int)gt.size();
+        npairs_ = (int)pt.size();
+        nwtiles_ = (int)wt.size();
+        nvtiles_ = (int)vt.size();
+    }
+
+    DeviceTables& T_;
+    std::vector<Problem*> P_;
+    int B_;
+    int64_t nx_ = 0, nc_ = 0;
+    cudaStream_t s_ = nullptr;
+    DevBuf<double> c_, x_, z_, aty_, atp_, y_, ax_, bv_, r_, p_, ap_, partial_, red_, mu_, coef_;
+    DevBuf<int> mask_, nact_;
+    DevBuf<CgScalars> cs_;
+    double* hscal_ = nullptr;
+    int* hnact_ = nullptr;
+    // projection plan
+    std::vector<BlockTask> hlarge_;
+    DevBuf<BlockTask> small_d_, large_d_;
+    int nsmall_ = 0, nlarge_ = 0, max_np_ = 0, max_n_ = 0, max_rounds_ = 0;
+    DevBuf<double> U_, W_, V_, Tm_, Q_, dw_;
+    DevBuf<int> bact_, bwork_;
+    DevBuf<GemmTile> gtiles_;
+    DevBuf<PairTask> pairs_;
+    DevBuf<WTileTask> wtiles_;
+    DevBuf<VTileTask> vtiles_;
+    int ngtiles_ = 0, npairs_ = 0, nwtiles_ = 0, nvtiles_ = 0;
+    bool warm_ = false;
+    long sweeps_total_ = 0;
+};
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const CudaError& e) {
+        return fail(V2G_ERR_CUDA, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(V2G_ERR_ARG, e.what());
+    } catch (const std::exception& e) {
+        return fail(V2G_ERR_ARG, e.what());
+    }
+}
+
+void require_device() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw CudaError("no CUDA device visible");
+}
+
+}  // namespace
+}  // namespace v2g
+
+using v2g::Problem;
+
+struct v2g_handle {
+    Problem P;
+};
+
+extern "C" {
+
+void v2g_default_options(v2g_options* o) {
+    o->positivity = "DQG";
+    o->constrain_spin = 1;
+    o->constrain_sz = 1;
+    o->r_convergence = 1e-4;
+    o->e_convergence = 1e-4;
+    o->cg_convergence = 1e-9;
+    o->maxiter = 10000;
+    o->cg_maxiter = 10000;
+    o->tau_parameter = 1.0;
+    o->mu_update_frequency = 500;
+    o->device = 0;
+    o->record_trace = 0;
+}
+
+const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
+
+int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int* rstcpi, const int* amopi,
+               const int* rstvpi, const int* frzvpi, int nalpha, int nbeta, int multiplicity, v2g_handle** out) {
+    return v2g::guarded([&]() -> int {
+        if (!opt || !amopi || !out) return v2g::fail(V2G_ERR_ARG, "null argument");
+        *out = nullptr;
+        v2g::Options o;
+        if (!v2g::parse_positivity(opt->positivity ? opt->positivity : "", o))
+            return v2g::fail(V2G_ERR_ARG, "unknown POSITIVITY");
+        if (o.constrain_t1 || o.constrain_t2)
+            return v2g::fail(V2G_ERR_UNSUPPORTED, "T1/T2 positivity is not built in this version");
+        o.constrain_spin = opt->constrain_spin != 0;
+        o.constrain_sz = opt->constrain_sz != 0;
+        o.r_convergence = opt->r_convergence;
+        o.e_convergence = opt->e_convergence;
+        o.cg_convergence = opt->cg_convergence;
+        o.maxiter = opt->maxiter;
+        o.cg_maxiter = opt->cg_maxiter;
+        o.tau = opt->tau_parameter;
+        o.mu_update_frequency = opt->mu_update_frequency;
+        if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)
+            return v2g::fail(V2G_ERR_ARG, "iteration limits must be positive");
+        auto h = std::make_unique<v2g_handle>();
+        Problem& P = h->P;
+        P.opt = o;
+        P.device = opt->device;
+        P.record_trace = opt->record_trace != 0;
+        std::vector<int> z(nirrep, 0);
+        auto arr = [&](const int* a) { return a ? std::vector<int>(a, a + nirrep) : z; };
+        P.sp.frzcpi = arr(frzcpi);
+        P.sp.rstcpi = arr(rstcpi);
+        P.sp.amopi = arr(amopi);
+        P.sp.rstvpi = arr(rstvpi);
+        P.sp.frzvpi = arr(frzvpi);
+        int core = 0;
+        for (int hh = 0; hh < nirrep; hh++) core += P.sp.frzcpi[hh] + P.sp.rstcpi[hh];
+        const double na = nalpha - core, nb = nbeta - core;
+        std::string err = v2g::build_layout(o, nirrep, P.sp.amopi, na, nb, multiplicity, P.L);
+        if (!err.empty()) return v2g::fail(V2G_ERR_ARG, err);
+        P.c.assign(P.L.dimx, 0.0);
+        P.x.assign(P.L.dimx, 0.0);
+        P.z.assign(P.L.dimx, 0.0);
+        P.y.assign(P.L.ncon, 0.0);
+        *out = h.release();
+        return V2G_OK;
+    });
+}
+
+void v2g_destroy(v2g_handle* h) { delete h; }
+
+long v2g_dimx(const v2g_handle* h) { return h ? (long)h->P.L.dimx : -1; }
+long v2g_nconstraints(const v2g_handle* h) { return h ? (long)h->P.L.ncon : -1; }
+int v2g_nblocks(const v2g_handle* h) { return h ? (int)h->P.L.block_dims.size() : -1; }
+int v2g_block_dims(const v2g_handle* h, int* dims) {
+    if (!h || !dims) return V2G_ERR_ARG;
+    for (size_t i = 0; i < h->P.L.block_dims.size(); i++) dims[i] = h->P.L.block_dims[i];
+    return V2G_OK;
+}
+
+int v2g_set_hamiltonian(v2g_handle* h, const double* oei, const double* qmo, int nq, double enuc) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !oei || (!qmo && nq > 0) || nq < 0) return v2g::fail(V2G_ERR_ARG, "bad integral arguments");
+        Problem& P = h->P;
+        std::string err = v2g::build_c(P.L, P.sp, oei, qmo, nq, P.c, P.efzc);
+        if (!err.empty()) return v2g::fail(V2G_ERR_ARG, err);
+        P.enuc = enuc;
+        P.have_c = true;
+        return V2G_OK;
+    });
+}
+
+int v2g_get_c(const v2g_handle* h, double* c) {
+    if (!h || !c) return V2G_ERR_ARG;
+    std::copy(h->P.c.begin(), h->P.c.end(), c);
+    return V2G_OK;
+}
+
+int v2g_get_b(const v2g_handle* h, double* b) {
+    if (!h || !b) return V2G_ERR_ARG;
+    std::vector<double> bb;
+    v2g::build_b(h->P.L, bb);
+    std::copy(bb.begin(), bb.end(), b);
+    return V2G_OK;
+}
+
+double v2g_efzc(const v2g_handle* h) { return h ? h->P.efzc : 0.0; }
+
+int v2g_guess_random(v2g_handle* h) {
+    if (!h) return V2G_ERR_ARG;
+    Problem& P = h->P;
+    // v2rdm_solver.cc:2479-2490: srand(0); x_i, z_i interleaved, then y
+    srand(0);
+    for (int64_t i = 0; i < P.L.dimx; i++) {
+        P.x[i] = ((double)rand() / RAND_MAX - 1.0) * 2.0;
+        P.z[i] = ((double)rand() / RAND_MAX - 1.0) * 2.0;
+    }
+    for (int64_t i = 0; i < P.L.ncon; i++) P.y[i] = ((double)rand() / RAND_MAX - 1.0) * 2.0;
+    P.mu = 1.0;
+    return V2G_OK;
+}
+
+int v2g_set_state(v2g_handle* h, const double* x, const double* y, const double* z, double mu) {
+    if (!h || !x || !y || !z || !(mu > 0.0)) return V2G_ERR_ARG;
+    Problem& P = h->P;
+    std::copy(x, x + P.L.dimx, P.x.begin());
+    std::copy(z, z + P.L.dimx, P.z.begin());
+    std::copy(y, y + P.L.ncon, P.y.begin());
+    P.mu = mu;
+    return V2G_OK;
+}
+
+int v2g_get_state(const v2g_handle* h, double* x, double* y, double* z, double* mu) {
+    if (!h) return V2G_ERR_ARG;
+    const Problem& P = h->P;
+    if (x) std::copy(P.x.begin(), P.x.end(), x);
+    if (y) std::copy(P.y.begin(), P.y.end(), y);
+    if (z) std::copy(P.z.begin(), P.z.end(), z);
+    if (mu) *mu = P.mu;
+    return V2G_OK;
+}
+
+static int apply_map(v2g_handle* h, const double* u, double* out, bool transpose, bool device_ptrs) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !u || !out) return v2g::fail(V2G_ERR_ARG, "null argument");
+        v2g::require_device();
+        Problem& P = h->P;
+        v2g::DeviceTables& T = P.tables();
+        CK(cudaSetDevice(T.device));
+        const int64_t nin = transpose ? P.L.ncon : P.L.dimx, nout = transpose ? P.L.dimx : P.L.ncon;
+        v2g::DevCsr M = transpose ? T.AT() : T.A();
+        if (device_ptrs) {
+            v2g::launch_spmv(M, 1, u, out, nullptr, nullptr, nullptr, nullptr, 0);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(0));
+            return V2G_OK;
+        }
+        v2g::DevBuf<double> din, dout(nout);
+        din.upload(u, nin);
+        v2g::launch_spmv(M, 1, din.p, dout.p, nullptr, nullptr, nullptr, nullptr, 0);
+        CK(cudaGetLastError());
+        CK(cudaMemcpy(out, dout.p, nout * sizeof(double), cudaMemcpyDeviceToHost));
+        return V2G_OK;
+    });
+}
+
+int v2g_apply_A(v2g_handle* h, const double* u, double* out) { return apply_map(h, u, out, false, false); }
+int v2g_apply_AT(v2g_handle* h, const double* u, double* out) { return apply_map(h, u, out, true, false); }
+int v2g_apply_A_device(v2g_handle* h, const double* u, double* out) { return apply_map(h, u, out, false, true); }
+int v2g_apply_AT_device(v2g_handle* h, const double* u, double* out) { return apply_map(h, u, out, true, true); }
+
+int v2g_update_xz(v2g_handle* h, double mu) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !(mu > 0.0)) return v2g::fail(V2G_ERR_ARG, "bad argument");
+        v2g::require_device();
+        Problem& P = h->P;
+        P.mu = mu;
+        v2g::GroupRun g(P.tables(), {&P});
+        g.project();
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(g.stream()));
+        g.download_state();
+        return V2G_OK;
+    });
+}
+
+int v2g_solve_batch(v2g_handle** hs, int count, v2g_result* res) {
+    return v2g::guarded([&]() -> int {
+        if (!hs || !res || count < 1) return v2g::fail(V2G_ERR_ARG, "bad batch arguments");
+        v2g::require_device();
+        // group handles by layout (shared tables), at most 256 per group
+        std::map<v2g::DeviceTables*, std::vector<int>> groups;
+        for (int i = 0; i < count; i++) {
+            if (!hs[i]) return v2g::fail(V2G_ERR_ARG, "null handle in batch");
+            if (!hs[i]->P.have_c) return v2g::fail(V2G_ERR_ARG, "v2g_set_hamiltonian was not called");
+            groups[&hs[i]->P.tables()].push_back(i);
+        }
+        int worst = V2G_OK;
+        for (auto& kv : groups) {
+            const auto& idx = kv.second;
+            for (size_t s = 0; s < idx.size(); s += 256) {
+                std::vector<Problem*> probs;
+                std::vector<int> which;
+                for (size_t k = s; k < idx.size() && k < s + 256; k++) {
+                    probs.push_back(&hs[idx[k]]->P);
+                    which.push_back(idx[k]);
+                }
+                v2g::GroupRun g(*kv.first, probs);
+                std::vector<v2g_result> r;
+                g.solve(r);
+                CK(cudaGetLastError());
+                for (size_t k = 0; k < which.size(); k++) {
+                    res[which[k]] = r[k];
+                    if (r[k].status != V2G_OK && worst == V2G_OK) worst = r[k].status;
+                }
+            }
+        }
+        if (worst != V2G_OK) v2g::g_last_error = "at least one instance did not converge";
+        return worst;
+    });
+}
+
+int v2g_solve(v2g_handle* h, v2g_result* res) { return v2g_solve_batch(&h, 1, res); }
+
+long v2g_A_nnz(v2g_handle* h) {
+    if (!h) return -1;
+    v2g::Csr A;
+    if (!v2g::build_A(h->P.L, A).empty()) return -1;
+    return (long)A.nnz();
+}
+
+int v2g_export_A(v2g_handle* h, long* rowptr, int* col, double* val) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !rowptr || !col || !val) return v2g::fail(V2G_ERR_ARG, "null argument");
+        v2g::Csr A;
+        std::string err = v2g::build_A(h->P.L, A);
+        if (!err.empty()) return v2g::fail(V2G_ERR_UNSUPPORTED, err);
+        for (size_t i = 0; i < A.rowptr.size(); i++) rowptr[i] = (long)A.rowptr[i];
+        std::copy(A.col.begin(), A.col.end(), col);
+        std::copy(A.val.begin(), A.val.end(), val);
+        return V2G_OK;
+    });
+}
+
+long v2g_trace(const v2g_handle* h, double* rows, long cap) {
+    if (!h) return -1;
+    const auto& t = h->P.trace;
+    long n = (long)t.size();
+    if (rows)
+        for (long i = 0; i < n && i < cap; i++)
+            for (int k = 0; k < 8; k++) rows[i * 8 + k] = t[i][k];
+    return n;
+}
+
+}  // extern "C"

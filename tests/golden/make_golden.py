@@ -1,0 +1,119 @@
+#!/usr/bin/env python3
+"""Generates the golden fixtures in this directory from the reference itself.
+
+Runs the reference's own hot-path code, compiled from the reference tree into
+oracle/_ref/libv2rdm_ref.so (see oracle/Makefile), on seeded inputs and stores
+inputs and outputs as .npz files:
+
+  maps_<case>.npz   A u and A^T w of bpsdp_Au / bpsdp_ATu for seeded u, w, plus
+                    b (BuildConstraints) and the layout sizes
+  c_<case>.npz      c and efzc of RepackIntegrals/FrozenCoreEnergy for seeded
+                    integrals, with frozen/restricted orbitals
+  xz_<case>.npz     Update_xz on a seeded state (x, y, z, mu) -> x, z
+  solve_<case>.npz  a full BPSDP solve (random start, srand(0)) of a seeded
+                    synthetic active space: final energies, iteration counts,
+                    the per-iteration trace and the final x, y, z
+
+Usage: python tests/golden/make_golden.py   (needs `make -C oracle` first)
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.ref import RefSolver, set_threads  # noqa: E402
+from v2rdm_casscf_b200.hamiltonian import synthetic  # noqa: E402
+
+MAP_CASES = {
+    # name: (amopi, doccpi, soccpi, positivity, constrain_spin, constrain_sz)
+    "c1_n4_dqg": ([4], [2], [0], "DQG", True, True),
+    "c1_n6_dqg": ([6], [3], [0], "DQG", True, True),
+    "c1_n5_triplet_dqg": ([5], [2], [1], "DQG", True, True),
+    "c1_n5_dqg_nosz": ([5], [2], [1], "DQG", True, False),
+    "c2v_dqg": ([2, 1, 1, 2], [1, 0, 0, 1], [0, 0, 0, 0], "DQG", True, True),
+    "c1_n4_d": ([4], [2], [0], "D", True, True),
+}
+
+SOLVE_CASES = {
+    # name: (n, seed, r_conv, e_conv)
+    "synthetic_n4_s0": (4, 0, 1e-6, 1e-7),
+    "synthetic_n4_s1": (4, 1, 1e-6, 1e-7),
+    "synthetic_n5_s2": (5, 2, 1e-6, 1e-7),
+}
+
+
+def maps(name, spec):
+    amopi, docc, socc, pos, spin, sz = spec
+    r = RefSolver(amopi, docc, soccpi=socc, positivity=pos, constrain_spin=spin, constrain_sz=sz,
+                  multiplicity=sum(socc) + 1)
+    rng = np.random.default_rng(12345)
+    u = rng.standard_normal(r.dimx)
+    w = rng.standard_normal(r.ncon)
+    r.build_constraints()
+    np.savez_compressed(os.path.join(HERE, f"maps_{name}.npz"), amopi=amopi, doccpi=docc, soccpi=socc,
+                        positivity=pos, constrain_spin=spin, constrain_sz=sz, dimx=r.dimx, ncon=r.ncon,
+                        block_dims=r.block_dims, u=u, w=w, Au=r.Au(u), ATw=r.ATu(w), b=r.get("b"))
+
+
+def cvec():
+    frzc, rstc, amo, rstv, frzv = [1, 0], [0, 1], [3, 2], [1, 0], [0, 1]
+    docc, socc = [2, 2], [0, 0]
+    nmopi = [frzc[h] + rstc[h] + amo[h] + rstv[h] + frzv[h] for h in range(2)]
+    nfull = [nmopi[h] - frzv[h] for h in range(2)]
+    nf = sum(nfull)
+    rng = np.random.default_rng(7)
+    oei = rng.standard_normal(sum(n * (n + 1) // 2 for n in nfull))
+    nq = 7
+    qmo = rng.standard_normal(nq * nf * (nf + 1) // 2)
+    r = RefSolver(nmopi, docc, soccpi=socc, frzcpi=frzc, rstcpi=rstc, rstvpi=rstv, frzvpi=frzv)
+    r.set_integrals(oei, qmo, nq)
+    np.savez_compressed(os.path.join(HERE, "c_c2_core.npz"), frzc=frzc, rstc=rstc, amo=amo, rstv=rstv, frzv=frzv,
+                        docc=docc, socc=socc, oei=oei, qmo=qmo, nq=nq, c=r.get("c"), efzc=r.efzc)
+
+
+def xz():
+    for n in (4, 6):
+        r = RefSolver([n], [n // 2], positivity="DQG")
+        a = synthetic(n, 3)
+        r.set_integrals(a.oei_packed, a.qmo, a.nq)
+        rng = np.random.default_rng(99 + n)
+        x = rng.standard_normal(r.dimx)
+        z = rng.standard_normal(r.dimx)
+        y = rng.standard_normal(r.ncon)
+        mu = 0.7
+        r.set("x", x)
+        r.set("y", y)
+        r.set("z", z)
+        r.update_xz(mu)
+        np.savez_compressed(os.path.join(HERE, f"xz_n{n}.npz"), n=n, seed=3, x=x, y=y, z=z, mu=mu,
+                            x_out=r.get("x"), z_out=r.get("z"))
+
+
+def solve(name, spec):
+    n, seed, rc, ec = spec
+    a = synthetic(n, seed)
+    r = RefSolver([n], [a.nb], soccpi=[a.na - a.nb], multiplicity=a.multiplicity, positivity="DQG",
+                  r_convergence=rc, e_convergence=ec)
+    r.set_integrals(a.oei_packed, a.qmo, a.nq)
+    r.guess()
+    r.build_constraints()
+    out = r.solve(trace_cap=100000)
+    np.savez_compressed(os.path.join(HERE, f"solve_{name}.npz"), n=n, seed=seed, r_conv=rc, e_conv=ec,
+                        e_primal=out["e_primal"], e_dual=out["e_dual"], ep=out["ep"], ed=out["ed"],
+                        oiter=out["oiter"], iiter=out["iiter"], converged=out["converged"], trace=out["trace"],
+                        x=r.get("x"), y=r.get("y"), z=r.get("z"))
+
+
+if __name__ == "__main__":
+    set_threads(int(os.environ.get("OMP_NUM_THREADS", "4")))
+    for k, v in MAP_CASES.items():
+        maps(k, v)
+    cvec()
+    xz()
+    for k, v in SOLVE_CASES.items():
+        solve(k, v)
+    print("golden fixtures written to", HERE)

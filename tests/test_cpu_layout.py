@@ -1,0 +1,103 @@
+"""CPU tests: the C ABI library loads and exports its header, and the host-side
+layout, constraint table, b and c match the reference (golden fixtures made by
+tests/golden/make_golden.py from the reference's own code, and the compiled
+oracle when present)."""
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from tests.helpers import GOLDEN, ROOT, csr_of, load, make_solver
+
+
+
+
+def test_library_exports_every_header_symbol(v2g):
+    header = open(os.path.join(ROOT, "include", "v2rdm_gpu.h")).read()
+    declared = set(re.findall(r"\b(v2g_\w+)\s*\(", header))
+    assert declared == set(v2g.EXPORTS)
+    lib = v2g.lib()
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_sizes_match_reference_log(v2g):
+    # tests/v2rdm8/output.ref:429-430: H2 (2,2), POSITIVITY D, C1 -> 50 variables, 51 constraints
+    s = v2g.V2RDMSolver([2], 1, 1, options=dict(POSITIVITY="D"))
+    assert (s.dimx, s.nconstraints) == (50, 51)
+    # (10,10) DQG C1 and (20,20) DQG C1 sizes of the measured workloads
+    s = v2g.V2RDMSolver([10], 5, 5)
+    assert (s.dimx, s.nconstraints) == (98500, 91029)
+    assert sorted(set(s.dimensions.tolist())) == [10, 45, 100, 200]
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "maps_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_constraint_table_matches_golden(v2g, path):
+    g = load(path)
+    s = make_solver(v2g, g)
+    assert s.dimx == int(g["dimx"]) and s.nconstraints == int(g["ncon"])
+    assert s.dimensions.tolist() == g["block_dims"].tolist()
+    A = csr_of(s)
+    au, atw = A @ g["u"], A.T @ g["w"]
+    assert np.abs(au - g["Au"]).max() <= 1e-13 * np.abs(g["Au"]).max()
+    assert np.abs(atw - g["ATw"]).max() <= 1e-13 * np.abs(g["ATw"]).max()
+    assert np.array_equal(s.b, g["b"])
+
+
+def test_c_matches_golden(v2g):
+    g = load(os.path.join(GOLDEN, "c_c2_core.npz"))
+    docc, socc = g["docc"], g["socc"]
+    na, nb = int(docc.sum() + socc.sum()), int(docc.sum())
+    s = v2g.V2RDMSolver(g["amo"], na, nb, 1, frozen_docc=g["frzc"], restricted_docc=g["rstc"],
+                        restricted_uocc=g["rstv"], frozen_uocc=g["frzv"])
+    s.set_hamiltonian(g["oei"], g["qmo"], int(g["nq"]))
+    assert np.abs(s.c - g["c"]).max() <= 1e-13 * np.abs(g["c"]).max()
+    assert abs(s.efzc - float(g["efzc"])) <= 1e-12 * max(1.0, abs(float(g["efzc"])))
+
+
+def test_oracle_reproduces_golden(ref):
+    g = load(os.path.join(GOLDEN, "maps_c1_n4_dqg.npz"))
+    r = ref.RefSolver(g["amopi"].tolist(), g["doccpi"].tolist(), soccpi=g["soccpi"].tolist(),
+                      positivity=str(g["positivity"]))
+    assert np.array_equal(r.Au(g["u"]), g["Au"])
+    assert np.array_equal(r.ATu(g["w"]), g["ATw"])
+
+
+@pytest.mark.parametrize("spec", [
+    ([7], 3, 3, 1, "DQG"), ([6], 3, 2, 2, "DQG"), ([3, 3], 3, 3, 1, "DQG"), ([2, 2, 2, 1], 3, 3, 1, "DQ"),
+])
+def test_constraint_table_matches_oracle(v2g, ref, spec):
+    amopi, na, nb, mult, pos = spec
+    docc = [0] * len(amopi)
+    socc = [0] * len(amopi)
+    # distribute electrons over irreps (only the totals matter for the layout)
+    left_b, left_s = nb, na - nb
+    for h in range(len(amopi)):
+        d = min(amopi[h], left_b)
+        docc[h] = d
+        left_b -= d
+        s_ = min(amopi[h] - d, left_s)
+        socc[h] = s_
+        left_s -= s_
+    r = ref.RefSolver(amopi, docc, soccpi=socc, multiplicity=mult, positivity=pos)
+    s = v2g.V2RDMSolver(amopi, na, nb, mult, options=dict(POSITIVITY=pos))
+    A = csr_of(s)
+    rng = np.random.default_rng(5)
+    u, w = rng.standard_normal(s.dimx), rng.standard_normal(s.nconstraints)
+    a = r.Au(u)
+    t = r.ATu(w)
+    assert np.abs(A @ u - a).max() <= 1e-13 * np.abs(a).max()
+    assert np.abs(A.T @ w - t).max() <= 1e-13 * np.abs(t).max()
+
+
+def test_invalid_options_fail_loudly(v2g):
+    with pytest.raises(v2g.V2GError):
+        v2g.V2RDMSolver([4], 2, 2, options=dict(POSITIVITY="DQX"))
+    with pytest.raises(v2g.V2GError):
+        v2g.V2RDMSolver([4], 2, 2, options=dict(MAXITER=0))
+    with pytest.raises(KeyError):
+        v2g.V2RDMSolver([4], 2, 2, options=dict(NOT_AN_OPTION=1))

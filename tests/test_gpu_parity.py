@@ -1,0 +1,120 @@
+"""GPU parity tests through the C ABI against the reference.
+
+Golden fixtures come from the reference's own code (tests/golden/make_golden.py);
+when the compiled oracle is present it is also run on fresh seeds.
+Tolerances: the maps are FP64 gathers, within 1e-12 relative;
+the projection within 1e-10 relative to the block norms (eigensolvers differ);
+total energies within 1e-6 Eh of the reference at the same convergence
+thresholds.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from tests.helpers import GOLDEN, load, make_solver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "maps_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_maps_match_reference(v2g, path):
+    g = load(path)
+    s = make_solver(v2g, g)
+    au = s.Au(g["u"])
+    atw = s.ATu(g["w"])
+    assert np.abs(au - g["Au"]).max() <= 1e-12 * np.abs(g["Au"]).max()
+    assert np.abs(atw - g["ATw"]).max() <= 1e-12 * np.abs(g["ATw"]).max()
+
+
+def test_maps_adjoint(v2g):
+    s = v2g.V2RDMSolver([8], 4, 4)
+    rng = np.random.default_rng(0)
+    u, w = rng.standard_normal(s.dimx), rng.standard_normal(s.nconstraints)
+    lhs = np.dot(s.Au(u), w)
+    rhs = np.dot(u, s.ATu(w))
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.parametrize("n", [4, 6])
+def test_update_xz_matches_reference(v2g, n):
+    # n=4: every block <= 64 (shared-memory Jacobi); n=6: G2 block of 72 (block Jacobi)
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, f"xz_n{n}.npz"))
+    a = synthetic(n, int(g["seed"]))
+    s = v2g.V2RDMSolver.from_active_space(a)
+    s.set_state(g["x"], g["y"], g["z"], float(g["mu"]))
+    s.update_xz(float(g["mu"]))
+    x, y, z, _ = s.get_state()
+    scale = max(np.abs(g["x_out"]).max(), np.abs(g["z_out"]).max())
+    assert np.abs(x - g["x_out"]).max() <= 1e-10 * scale
+    assert np.abs(z - g["z_out"]).max() <= 1e-10 * scale
+
+
+def _solve_golden(v2g, name):
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, f"solve_{name}.npz"))
+    a = synthetic(int(g["n"]), int(g["seed"]))
+    s = v2g.V2RDMSolver.from_active_space(
+        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])), record_trace=True)
+    s.guess()
+    return g, s
+
+
+@pytest.mark.parametrize("name", ["synthetic_n4_s0", "synthetic_n4_s1", "synthetic_n5_s2"])
+def test_solve_matches_reference(v2g, name):
+    # Converged energies agree; individual iterations do not have to, since CG
+    # on A A^T from the random start amplifies rounding (a sparse vs dense
+    # matvec on the CPU already moves iteration 0 by 5e-5 Eh).
+    g, s = _solve_golden(v2g, name)
+    e = s.compute_energy()
+    r = s.result
+    assert r["status"] == 0
+    assert abs(e - float(g["e_primal"])) <= 1e-6
+    assert abs(r["e_dual"] - float(g["e_dual"])) <= 1e-6
+    assert r["ep"] <= float(g["r_conv"]) and r["ed"] <= float(g["r_conv"])
+    assert abs(r["oiter"] - int(g["oiter"])) <= 0.25 * int(g["oiter"])
+    tr = s.trace()
+    assert len(tr) == r["oiter"]
+    assert np.all(np.diff(tr[:, 0]) == 1)
+
+
+def test_batch_equals_individual_solves(v2g):
+    g0, s0 = _solve_golden(v2g, "synthetic_n4_s0")
+    g1, s1 = _solve_golden(v2g, "synthetic_n4_s1")
+    g2, s2 = _solve_golden(v2g, "synthetic_n5_s2")  # another layout in the same call
+    # looser thresholds for one instance: options are per instance
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    s3 = v2g.V2RDMSolver.from_active_space(synthetic(4, 1), options=dict(R_CONVERGENCE=1e-4, E_CONVERGENCE=1e-4))
+    s3.guess()
+    res = v2g.solve_batch([s0, s1, s2, s3])
+    assert all(r["status"] == 0 for r in res)
+    for r, g in zip(res[:3], (g0, g1, g2)):
+        assert abs(r["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert res[3]["oiter"] < res[1]["oiter"]
+    g1b, s1b = _solve_golden(v2g, "synthetic_n4_s1")
+    e1 = s1b.compute_energy()
+    assert e1 == res[1]["e_total"] and s1b.result["oiter"] == res[1]["oiter"]
+
+
+def test_solve_matches_oracle_fresh_seed(v2g, ref):
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a2 = synthetic(5, 11)  # doublet (5e,5o)
+    opts = dict(R_CONVERGENCE=1e-6, E_CONVERGENCE=1e-7)
+    r = ref.RefSolver([5], [2], soccpi=[1], multiplicity=2, positivity="DQG", r_convergence=1e-6,
+                      e_convergence=1e-7)
+    r.set_integrals(a2.oei_packed, a2.qmo, a2.nq)
+    r.guess()
+    r.build_constraints()
+    out = r.solve()
+    s = v2g.V2RDMSolver.from_active_space(a2, options=opts)
+    s.guess()
+    e = s.compute_energy()
+    assert out["converged"]
+    assert abs(e - out["e_primal"]) <= 1e-6

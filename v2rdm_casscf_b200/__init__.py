@@ -209,8 +209,11 @@ class V2RDMSolver:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value:
-            lib().v2g_destroy(h)
+        if h is not None and h.value and _lib is not None:
+            try:
+                _lib.v2g_destroy(h)
+            except Exception:
+                pass
             self.h = None
 
     # -- inputs ---------------------------------------------------------------

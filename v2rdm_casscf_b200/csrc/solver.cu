@@ -270,7 +270,8 @@ class GroupRun {
 
     // The outer BPSDP loop.  Returns per-instance results.
     void solve(std::vector<v2g_result>& res) {
-        const Options& o = T_.L.opt;
+        // loop options are per instance; the shared tables only fix the layout
+        auto opt = [&](int b) -> const Options& { return P_[b]->opt; };
         res.assign(B_, v2g_result{});
         std::vector<double> mu(B_), ep(B_, 0.0), ed(B_, 0.0), egap(B_, 0.0);
         std::vector<int> active(B_, 1), oiter(B_, 0);
@@ -295,7 +296,7 @@ class GroupRun {
             for (int b = 0; b < B_; b++) nactive += active[b];
             if (nactive == 0) break;
             CK(cudaMemcpyAsync(mask_.p, active.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
-            for (int b = 0; b < B_; b++) coef[b] = -o.tau * mu[b];
+            for (int b = 0; b < B_; b++) coef[b] = -opt(b).tau * mu[b];
             CK(cudaMemcpyAsync(coef_.p, coef.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
             CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
             CK(cudaEventRecord(e0, s_));
@@ -305,6 +306,7 @@ class GroupRun {
             launch_spmv(T_.A(), B_, z_.p, bv_.p, nullptr, nullptr, ax_.p, mask_.p, s_);
             // CG tolerance (:1797-1805)
             for (int b = 0; b < B_; b++) {
+                const Options& o = opt(b);
                 double tol;
                 if (oiter[b] == 0)
                     tol = 0.01;
@@ -338,6 +340,7 @@ class GroupRun {
             for (int b = 0; b < B_; b++) {
                 if (!active[b]) continue;
                 Problem& P = *P_[b];
+                const Options& o = opt(b);
                 ed[b] = std::sqrt(hscal_[b]);
                 ep[b] = std::sqrt(hscal_[B_ + b]);
                 const double e_p = hscal_[2 * B_ + b], e_d = hscal_[3 * B_ + b];

@@ -89,7 +89,7 @@ def synthetic(n, seed, nq=None):
     L = rng_l.normal(0.0, 0.25, size=(nq, n, n))
     L = np.tril(L)
     L = L + np.transpose(np.tril(L, -1), (0, 2, 1))
-    return ActiveSpace(h, L, n // 2, n - n // 2, 0.0, name=f"synthetic(n={n},seed={seed})")
+    return ActiveSpace(h, L, n - n // 2, n // 2, 0.0, name=f"synthetic(n={n},seed={seed})")
 
 
 def batch_sizes(count=256, nmin=8, nmax=20, seed=2024):

@@ -1,0 +1,367 @@
+#!/usr/bin/env python3
+"""Benchmark: time to a converged (E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6) v2RDM
+boundary-point SDP solve of a batch of active spaces on B200.
+
+Workload (default "batch256"): 256 seeded synthetic active spaces, n ~ U{8..20}
+orbitals with N = n electrons (singlet for even n, doublet for odd n), C1, DQG
+with CONSTRAIN_SPIN, each started from the reference's random guess (srand(0)),
+all solved in one batched call of the C ABI (v2g_solve_batch).  One step = one
+full batched solve.  Inputs are far larger than L2 (the primal/dual vectors of
+the batch take several GB), so no L2 flush is needed between steps.
+
+  value     device seconds of the batched solve, inputs resident in HBM
+            (CUDA events around the iteration phase, max over ranks)
+  e2e       the same solve through the public C ABI from host buffers,
+            host-to-device and device-to-host copies inside the timed region
+  roofline  the dominant kernel, the FP64 gather map (A / A^T) of the CG:
+            algorithmic bytes 8*(rows+cols) per instance per launch over its
+            CUDA-event duration, against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own hot-path code (oracle/_ref, OpenMP + the
+            OpenBLAS of scipy on all host cores) timed per outer iteration on a
+            sample of sizes and extrapolated to the batch with the iteration
+            counts of the same instances
+
+Multi-GPU (torchrun): instances are dealt round-robin to ranks (no exchange
+during the solve); value is the max over ranks.  `--impl reference` times the
+reference CPU path instead (rank 0 only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from v2rdm_casscf_b200.hamiltonian import batch_sizes, synthetic  # noqa: E402
+
+METRIC = "time-to-1e-6Eh v2RDM solve: mixed+warm-start vs plain FP64 GPU vs ref CPU"
+OPTIONS = dict(R_CONVERGENCE=1e-6, E_CONVERGENCE=1e-7)
+ITER_FILE = os.path.join(ROOT, "profiles", "batch256_outer_iterations.json")
+
+
+def workload(name, count):
+    if name == "batch256":
+        ns = batch_sizes(count)
+        return [synthetic(int(n), s) for s, n in enumerate(ns)]
+    if name.startswith("uniform"):  # uniformN: count instances of n = N (experiments)
+        n = int(name[len("uniform"):])
+        return [synthetic(n, s) for s in range(count)]
+    raise SystemExit(f"unknown workload {name}")
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, gpu_index, path):
+        self.path = path
+        self.proc = None
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [v.strip() for v in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm = float(p[1])
+                mx = float(p[2])
+            except ValueError:
+                continue
+            sms.append(sm)
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sms:
+            return None
+        loaded = [s for s in sms if mx and s > 0.5 * mx] or sms
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_gpu(args):
+    import torch
+
+    import v2rdm_casscf_b200 as V
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(minutes=30))
+    dev = local
+    all_spaces = workload(args.workload, args.count)
+    mine = list(range(rank, len(all_spaces), world))
+    opts = dict(OPTIONS)
+    if args.max_outer:
+        opts["MAXITER"] = args.max_outer
+    solvers = [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
+                                               projection=args.projection)
+               for i in mine]
+    # the random start of the reference depends only on the layout: compute once per size
+    starts = {}
+    for s in solvers:
+        key = (s.dimx, s.nconstraints)
+        if key not in starts:
+            s.guess()
+            starts[key] = s.get_state()
+    def reset():
+        for s in solvers:
+            x, y, z, mu = starts[(s.dimx, s.nconstraints)]
+            s.set_state(x, y, z, mu)
+
+    def step():
+        reset()
+        res = V.solve_batch(solvers)
+        st = V.last_batch_stats()
+        return res, st
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(dev, os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
+                                   f"clocks_rank{rank}.csv")) if args.clocks else None
+    t0 = time.time()
+    dev_s, e2e_s, stats, results = [], [], [], None
+    for _ in range(args.steps):
+        results, st = step()
+        dev_s.append(st["device_seconds"])
+        e2e_s.append(st["e2e_seconds"])
+        stats.append(st)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    wall = time.time() - t0
+    clocks = clk.stop() if clk else None
+    value = float(np.mean(dev_s))
+    e2e = float(np.mean(e2e_s))
+    map_s = sum(s["map_seconds"] for s in stats)
+    map_n = sum(s["map_launches"] for s in stats)
+    map_b = sum(s["map_bytes"] for s in stats)
+    launches = sum(s["kernel_launches"] for s in stats)
+    h2d = float(np.mean([s["h2d_bytes"] for s in stats]))
+    d2h = float(np.mean([s["d2h_bytes"] for s in stats]))
+    if world > 1:
+        t = torch.tensor([value, e2e], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        value, e2e = float(t[0]), float(t[1])
+        t = torch.tensor([float(launches), h2d, d2h], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        launches, h2d, d2h = int(t[0]), float(t[1]), float(t[2])
+    conv = [r["status"] == 0 for r in results]
+    if rank == 0:
+        oiters = {}
+        for i, r in zip(mine, results):
+            oiters.setdefault(int(all_spaces[i].n), []).append(int(r["oiter"]))
+    pk, pk_kind = peaks()
+    achieved = (map_b / map_s / 1e9) if map_s > 0 else None
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value * 1e3,
+        "higher_is_better": False,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Philox active spaces; no public dataset involved)",
+        "config": {
+            "workload": f"{args.workload}: {args.count} synthetic active spaces n~U{{8..20}}, N=n, C1, DQG, "
+                        "CONSTRAIN_SPIN, E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6, random start (srand(0))",
+            "instances": args.count,
+            "precision": "FP64 (maps, CG, projection)",
+            "projection": args.projection,
+            "l2": "inputs larger than L2 (no flush needed)",
+            "parallelism": f"instances dealt to {world} rank(s), no exchange",
+            "max_outer": args.max_outer or None,
+        },
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": {
+            "kernel": "spmv_kernel (A / A^T gather inside CG)",
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": pk,
+            "peak_kind": pk_kind,
+            "unit": "GB/s",
+            "frac": (achieved / pk) if achieved else None,
+            "traffic": None,
+            "launches_timed": map_n,
+        },
+        "converged": int(sum(conv)),
+        "wall_s": wall,
+    }
+    if clocks:
+        out["clocks"] = clocks
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0:
+        out["outer_iterations"] = {str(k): v for k, v in sorted(oiters.items())}
+        if args.cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(all_spaces, [results[k]["oiter"] for k in range(len(results))],
+                                               args.cpu_sample)
+        if args.save_iterations and world == 1 and not args.max_outer:
+            os.makedirs(os.path.dirname(ITER_FILE), exist_ok=True)
+            json.dump({"workload": args.workload, "count": args.count,
+                       "outer_iterations": [int(r["oiter"]) for r in results],
+                       "n": [int(a.n) for a in all_spaces]}, open(ITER_FILE, "w"))
+        print(json.dumps(out))
+
+
+def ref_time_per_iteration(space, iters, threads):
+    """Seconds per outer iteration of the reference on one instance (after one warm-up iteration)."""
+    from oracle import ref as R
+
+    R.set_threads(threads)
+    r = R.RefSolver([space.n], [space.nb], soccpi=[space.na - space.nb], multiplicity=space.multiplicity,
+                    positivity="DQG", r_convergence=OPTIONS["R_CONVERGENCE"], e_convergence=OPTIONS["E_CONVERGENCE"])
+    r.set_integrals(space.oei_packed, space.qmo, space.nq)
+    r.guess()
+    r.build_constraints()
+    out = r.solve(max_outer=iters + 1, trace_cap=0)
+    t1 = out["t_total"]
+    r2 = R.RefSolver([space.n], [space.nb], soccpi=[space.na - space.nb], multiplicity=space.multiplicity,
+                     positivity="DQG", r_convergence=OPTIONS["R_CONVERGENCE"], e_convergence=OPTIONS["E_CONVERGENCE"])
+    r2.set_integrals(space.oei_packed, space.qmo, space.nq)
+    r2.guess()
+    r2.build_constraints()
+    t0 = r2.solve(max_outer=1, trace_cap=0)["t_total"]
+    return max(t1 - t0, 1e-9) / iters
+
+
+def cpu_baseline(spaces, oiters, sample_sizes):
+    """Reference CPU time for the batch, extrapolated from a timed sample."""
+    from oracle import ref as R
+
+    if not R.available():
+        return {"unavailable": "oracle/_ref not built"}
+    threads = os.cpu_count() or 1
+    by_n = {}
+    for a in spaces:
+        by_n.setdefault(a.n, a)
+    sample = [n for n in sample_sizes if n in by_n]
+    t0 = time.time()
+    per_it = {}
+    for n in sample:
+        iters = 1 if n >= 16 else (2 if n >= 12 else 3)
+        per_it[n] = ref_time_per_iteration(by_n[n], iters, threads)
+    # power-law fit t(n) = a n^p over the sampled sizes for the others
+    xs = np.log(np.array(sample, dtype=float))
+    ys = np.log(np.array([per_it[n] for n in sample]))
+    p, lna = np.polyfit(xs, ys, 1)
+    total = 0.0
+    for a, k in zip(spaces, oiters):
+        t = per_it.get(a.n, float(np.exp(lna) * a.n ** p))
+        total += t * k
+    return {"value": total, "unit": "s", "cores": threads, "kind": "reference",
+            "sample": f"reference oracle/_ref (OpenMP, {threads} threads) timed per outer iteration on one "
+                      f"instance of n in {sample} ({', '.join(f'{n}: {per_it[n]:.3g} s' for n in sample)}), "
+                      f"power law n^{p:.2f} for other sizes, times the outer-iteration counts of the same "
+                      f"instances; extrapolated, sampling took {time.time() - t0:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import ref as R
+
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built on this box"}))
+        return
+    spaces = workload(args.workload, args.count)
+    if os.path.exists(ITER_FILE):
+        d = json.load(open(ITER_FILE))
+        oiters = d["outer_iterations"]
+        src = "outer-iteration counts of the same instances from the GPU solve (profiles/)"
+    else:
+        oiters = [2500] * len(spaces)
+        src = "2500 outer iterations per instance (no recorded counts)"
+    vals = []
+    base = None
+    for _ in range(args.warmup + args.steps):
+        base = cpu_baseline(spaces, oiters, args.cpu_sample)
+        vals.append(base["value"])
+    value = float(np.mean(vals[args.warmup:]))
+    base["value"] = value
+    base["sample"] += "; iteration counts: " + src
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+           "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"{args.workload}: {args.count} synthetic active spaces (see GPU arm)",
+                      "instances": args.count},
+           "cpu_baseline": base,
+           "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="batch256")
+    ap.add_argument("--count", type=int, default=256)
+    ap.add_argument("--max-outer", type=int, default=0, help="cap outer iterations (experiments only)")
+    ap.add_argument("--projection", default="adaptive", choices=["exact", "adaptive"])
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-sample", type=lambda s: [int(v) for v in s.split(",")], default=[8, 12, 16, 20])
+    ap.add_argument("--no-clocks", dest="clocks", action="store_false")
+    ap.add_argument("--save-iterations", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -59,6 +59,11 @@ typedef struct v2g_options {
     int mu_update_frequency;    /* MU_UPDATE_FREQUENCY (500) */
     int device;                 /* CUDA device ordinal (0) */
     int record_trace;           /* keep the per-iteration line of v2rdm_solver.cc:1881 (0) */
+    int profile;                /* time every A / A^T launch of the CG with CUDA events (0) */
+    int adaptive_projection;    /* 1: Update_xz accepts an eigendecomposition whose off-diagonal
+                                   residual is below 0.01 min(eps(p), eps(d)), the CG tolerance
+                                   rule (x, z stay PSD); 0: every projection converged, as the
+                                   plugin (0) */
 } v2g_options;
 
 typedef struct v2g_result {
@@ -126,6 +131,28 @@ int v2g_solve(v2g_handle* h, v2g_result* res);
  * layout share index tables; each keeps its own convergence test and stops
  * independently.  Returns V2G_OK when every instance converged. */
 int v2g_solve_batch(v2g_handle** hs, int count, v2g_result* res);
+
+/* Timing of the last v2g_solve / v2g_solve_batch call on this thread.
+ * device_seconds covers the solve with inputs already on the device (CUDA
+ * events around the iteration phase); e2e_seconds covers the whole call,
+ * host-to-device copies of x, y, z, c and device-to-host copies of the results
+ * included.  map_* are filled when the handles were created with profile=1:
+ * summed CUDA-event durations of the A and A^T launches inside CG, their count
+ * and their algorithmic bytes (8 * (rows + columns) per instance). */
+typedef struct v2g_batch_stats {
+    double device_seconds;
+    double e2e_seconds;
+    long kernel_launches;     /* kernels issued by this library during the solve */
+    double map_seconds;
+    long map_launches;
+    double map_bytes;
+    long groups;              /* layouts solved concurrently */
+    double h2d_bytes, d2h_bytes;
+    long refine_sweeps;       /* Ogita-Aishima sweeps over the large PSD blocks */
+    long jacobi_sweeps;       /* block-Jacobi sweeps (cold starts and fallbacks) */
+    long jacobi_blocks;       /* large blocks that fell back to block Jacobi */
+} v2g_batch_stats;
+int v2g_last_batch_stats(v2g_batch_stats* out);
 
 /* The constraint matrix A (nconstraints x dimx) as CSR, built on the host;
  * no GPU needed.  v2g_A_nnz gives the entry count; v2g_export_A fills

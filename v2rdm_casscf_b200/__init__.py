@@ -33,7 +33,7 @@ EXPORTS = [
     "v2g_nblocks", "v2g_block_dims", "v2g_set_hamiltonian", "v2g_get_c", "v2g_get_b", "v2g_efzc",
     "v2g_guess_random", "v2g_set_state", "v2g_get_state", "v2g_apply_A", "v2g_apply_AT", "v2g_apply_A_device",
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
-    "v2g_trace",
+    "v2g_trace", "v2g_last_batch_stats",
 ]
 
 
@@ -51,7 +51,29 @@ class Options(ctypes.Structure):
         ("mu_update_frequency", ctypes.c_int),
         ("device", ctypes.c_int),
         ("record_trace", ctypes.c_int),
+        ("profile", ctypes.c_int),
+        ("adaptive_projection", ctypes.c_int),
     ]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [
+        ("device_seconds", ctypes.c_double),
+        ("e2e_seconds", ctypes.c_double),
+        ("kernel_launches", ctypes.c_long),
+        ("map_seconds", ctypes.c_double),
+        ("map_launches", ctypes.c_long),
+        ("map_bytes", ctypes.c_double),
+        ("groups", ctypes.c_long),
+        ("h2d_bytes", ctypes.c_double),
+        ("d2h_bytes", ctypes.c_double),
+        ("refine_sweeps", ctypes.c_long),
+        ("jacobi_sweeps", ctypes.c_long),
+        ("jacobi_blocks", ctypes.c_long),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Result(ctypes.Structure):
@@ -117,6 +139,7 @@ def lib():
         L.v2g_export_A.argtypes = [P, LP, IP, DP]
         L.v2g_trace.restype = L_
         L.v2g_trace.argtypes = [P, DP, L_]
+        L.v2g_last_batch_stats.argtypes = [ctypes.POINTER(BatchStats)]
         _lib = L
     return _lib
 
@@ -161,11 +184,15 @@ class V2RDMSolver:
     Parameters mirror Psi4's per-irrep orbital arrays (FROZEN_DOCC,
     RESTRICTED_DOCC, ACTIVE, RESTRICTED_UOCC, FROZEN_UOCC) and the reference
     wavefunction's nalpha/nbeta/multiplicity; ``options`` takes the plugin's
-    option names.
+    option names.  ``projection="adaptive"`` lets Update_xz accept an
+    eigendecomposition whose residual is below 0.01 min(eps(p), eps(d)) (the
+    CG tolerance rule); the default "exact" converges every projection, as
+    the plugin does.
     """
 
     def __init__(self, active, nalpha, nbeta, multiplicity=1, frozen_docc=None, restricted_docc=None,
-                 restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False):
+                 restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False,
+                 profile=False, projection="exact"):
         L = lib()
         opts = dict(DEFAULT_OPTIONS)
         for k, v in (options or {}).items():
@@ -189,6 +216,10 @@ class V2RDMSolver:
         o.mu_update_frequency = int(opts["MU_UPDATE_FREQUENCY"])
         o.device = int(device)
         o.record_trace = int(bool(record_trace))
+        o.profile = int(bool(profile))
+        if projection not in ("exact", "adaptive"):
+            raise ValueError("projection is 'exact' or 'adaptive'")
+        o.adaptive_projection = int(projection == "adaptive")
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)
@@ -308,6 +339,13 @@ class V2RDMSolver:
         rows = np.zeros(8 * max(n, 1))
         L.v2g_trace(self.h, _dp(rows), n)
         return rows[: 8 * n].reshape(n, 8)
+
+
+def last_batch_stats():
+    """Timing of the last solve on this thread (see v2g_batch_stats)."""
+    st = BatchStats()
+    _check(lib().v2g_last_batch_stats(ctypes.byref(st)))
+    return st.as_dict()
 
 
 def solve_batch(solvers):

@@ -59,28 +59,32 @@ __device__ double block_sum(double v, double* red) {
 }
 
 // Parallel cyclic Jacobi on the symmetric N x N matrix A (shared memory,
-// leading dimension kLd).  On return A is diagonal to tol_rel (relative
-// Frobenius off-diagonal norm) and V holds the eigenvectors as columns.
-__device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double tol_rel) {
+// leading dimension kLd), round-robin ordering.  A pair (p,q) is rotated when
+// |a_pq| > rot_eps * sqrt(|a_pp a_qq|) and above an absolute floor of
+// 1e-17 ||A||_F; the method stops after a sweep without rotations (the
+// classical threshold criterion, which a relative off-norm test near the
+// rounding floor would never reach) or after max_sweeps.  On return V holds
+// the eigenvectors as columns and diag(A) the eigenvalues.
+__device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double rot_eps) {
     __shared__ double rc[kJ / 2], rs[kJ / 2];
     __shared__ int rp[kJ / 2], rq[kJ / 2];
     __shared__ double red[33];
+    __shared__ int rotated;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int Ne = N + (N & 1);
     const int npairs = Ne / 2;
     for (int i = tid; i < N * N; i += nt) V[(i / N) * kLd + (i % N)] = (i / N == i % N) ? 1.0 : 0.0;
     __syncthreads();
     if (N < 2) return;
+    double tot = 0.0;
+    for (int i = tid; i < N * N; i += nt) {
+        const double a = A[(i / N) * kLd + (i % N)];
+        tot += a * a;
+    }
+    const double floor_abs = 1e-17 * sqrt(block_sum(tot, red));
     for (int sweep = 0; sweep < max_sweeps; sweep++) {
-        double off = 0.0, tot = 0.0;
-        for (int i = tid; i < N * N; i += nt) {
-            const double a = A[(i / N) * kLd + (i % N)];
-            tot += a * a;
-            if (i / N != i % N) off += a * a;
-        }
-        off = block_sum(off, red);
-        tot = block_sum(tot, red);
-        if (!(off > tol_rel * tol_rel * tot)) break;
+        if (tid == 0) rotated = 0;
+        __syncthreads();
         for (int r = 0; r < Ne - 1; r++) {
             for (int k = tid; k < npairs; k += nt) {
                 int p, q;
@@ -89,11 +93,12 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
                 if (q < N) {
                     const double apq = A[p * kLd + q];
                     const double app = A[p * kLd + p], aqq = A[q * kLd + q];
-                    if (fabs(apq) > 1e-18 * (fabs(app) + fabs(aqq)) && apq != 0.0) {
+                    if (fabs(apq) > floor_abs && fabs(apq) > rot_eps * sqrt(fabs(app) * fabs(aqq))) {
                         const double tau = (aqq - app) / (2.0 * apq);
                         const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                         c = 1.0 / sqrt(1.0 + t * t);
                         s = t * c;
+                        rotated = 1;
                     }
                 }
                 rc[k] = c;
@@ -130,11 +135,14 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
             }
             __syncthreads();
         }
+        if (!rotated) break;
+        __syncthreads();
     }
 }
 
-constexpr double kJacobiTol = 1e-15;
-constexpr int kJacobiSweeps = 40;
+constexpr double kJacobiRotEps = 1e-15;
+constexpr int kJacobiSweeps = 20;
+constexpr int kPairSweeps = 3;
 
 __global__ void __launch_bounds__(kJThreads) small_project_kernel(const BlockTask* __restrict__ tasks, int B,
                                                                   const double* __restrict__ aty,
@@ -158,7 +166,7 @@ __global__ void __launch_bounds__(kJThreads) small_project_kernel(const BlockTas
         A[p * kLd + q] = 0.5 * (t1 + t2);
     }
     __syncthreads();
-    jacobi_smem(A, V, N, kJacobiSweeps, kJacobiTol);
+    jacobi_smem(A, V, N, kJacobiSweeps, kJacobiRotEps);
     __syncthreads();
     for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
         const int p = i / N, q = i % N;
@@ -214,74 +222,116 @@ __global__ void cold_start_kernel(const BlockTask* __restrict__ tasks, const dou
     }
 }
 
-// C = op(A) diag(d) op(B) on 64 x 64 tiles; 256 threads, 4 x 4 outputs each.
-__global__ void __launch_bounds__(256) gemm_kernel(const BlockTask* __restrict__ tasks,
-                                                   const GemmTile* __restrict__ tiles, const double* __restrict__ A,
-                                                   int transA, const double* __restrict__ Bm, int transB,
-                                                   const double* __restrict__ dvec, double* __restrict__ C,
-                                                   const int* __restrict__ bmask) {
-    constexpr int BK = 16;
-    __shared__ double As[BK][64 + 1];
-    __shared__ double Bs[BK][64 + 1];
+// C = op(A) diag(d) op(B) on 64 x 64 tiles of the padded workspaces.
+// 64 threads per tile, each holding an 8 x 8 block of C in registers (rows
+// ty + 8i, columns tx + 8j): 16 shared-memory loads feed 64 FMAs, which
+// matches the FP64 FMA rate to the shared-memory bandwidth.  The K loop is
+// double buffered through registers.
+constexpr int kGemmBK = 16;
+constexpr int kGemmLd = 64 + 1;
+
+__device__ __forceinline__ void gemm_load_chunk(const double* __restrict__ a, const double* __restrict__ bb, int np,
+                                                int i0, int j0, int k0, bool transA, bool transB, double ra[16],
+                                                double rb[16]) {
+    // 1024 elements per operand chunk, 16 per thread
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+        const int l = threadIdx.x + 64 * u;
+        if (transA) {
+            const int kk = l >> 6, ii = l & 63;
+            ra[u] = a[(int64_t)(k0 + kk) * np + i0 + ii];
+        } else {
+            const int ii = l >> 4, kk = l & 15;
+            ra[u] = a[(int64_t)(i0 + ii) * np + k0 + kk];
+        }
+        if (transB) {
+            const int jj = l >> 4, kk = l & 15;
+            rb[u] = bb[(int64_t)(j0 + jj) * np + k0 + kk];
+        } else {
+            const int kk = l >> 6, jj = l & 63;
+            rb[u] = bb[(int64_t)(k0 + kk) * np + j0 + jj];
+        }
+    }
+}
+
+__device__ __forceinline__ void gemm_store_chunk(double (*As)[kGemmLd], double (*Bs)[kGemmLd], bool transA,
+                                                 bool transB, const double ra[16], const double rb[16],
+                                                 const double* __restrict__ d, int k0) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+        const int l = threadIdx.x + 64 * u;
+        int kk, ii, jj;
+        if (transA) {
+            kk = l >> 6;
+            ii = l & 63;
+        } else {
+            ii = l >> 4;
+            kk = l & 15;
+        }
+        As[kk][ii] = d ? ra[u] * d[k0 + kk] : ra[u];
+        if (transB) {
+            jj = l >> 4;
+            kk = l & 15;
+        } else {
+            kk = l >> 6;
+            jj = l & 63;
+        }
+        Bs[kk][jj] = rb[u];
+    }
+}
+
+__global__ void __launch_bounds__(64) gemm_kernel(const BlockTask* __restrict__ tasks,
+                                                  const GemmTile* __restrict__ tiles, const double* __restrict__ A,
+                                                  int transA, const double* __restrict__ Bm, int transB,
+                                                  const double* __restrict__ dvec, double* __restrict__ C,
+                                                  const int* __restrict__ bmask) {
+    __shared__ double As[2][kGemmBK][kGemmLd];
+    __shared__ double Bs[2][kGemmBK][kGemmLd];
     const GemmTile tl = tiles[blockIdx.x];
     if (bmask && !bmask[tl.task]) return;
     const BlockTask t = tasks[tl.task];
     const int np = t.np;
     const double* a = A + t.woff;
     const double* bb = Bm + t.woff;
-    const double* d = dvec ? dvec + t.doff : nullptr;  // one weight vector (np) per block
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const double* d = dvec ? dvec + t.doff : nullptr;
+    const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
     const int i0 = tl.ti * 64, j0 = tl.tj * 64;
-    double acc[4][4] = {};
-    for (int k0 = 0; k0 < np; k0 += BK) {
-        for (int l = threadIdx.x; l < BK * 64; l += 256) {
-            int kk, ii;
-            if (transA) {
-                kk = l / 64;
-                ii = l % 64;
-                As[kk][ii] = a[(int64_t)(k0 + kk) * np + i0 + ii];
-            } else {
-                ii = l / BK;
-                kk = l % BK;
-                As[kk][ii] = a[(int64_t)(i0 + ii) * np + k0 + kk];
-            }
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+    double ra[16], rb[16];
+    gemm_load_chunk(a, bb, np, i0, j0, 0, transA, transB, ra, rb);
+    gemm_store_chunk(As[0], Bs[0], transA, transB, ra, rb, d, 0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < np; k0 += kGemmBK) {
+        const bool more = k0 + kGemmBK < np;
+        if (more) gemm_load_chunk(a, bb, np, i0, j0, k0 + kGemmBK, transA, transB, ra, rb);
+#pragma unroll
+        for (int kk = 0; kk < kGemmBK; kk++) {
+            double av[8], bv[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) av[i] = As[buf][kk][ty + 8 * i];
+#pragma unroll
+            for (int j = 0; j < 8; j++) bv[j] = Bs[buf][kk][tx + 8 * j];
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
         }
-        for (int l = threadIdx.x; l < BK * 64; l += 256) {
-            int kk, jj;
-            if (transB) {
-                jj = l / BK;
-                kk = l % BK;
-                Bs[kk][jj] = bb[(int64_t)(j0 + jj) * np + k0 + kk];
-            } else {
-                kk = l / 64;
-                jj = l % 64;
-                Bs[kk][jj] = bb[(int64_t)(k0 + kk) * np + j0 + jj];
-            }
-        }
-        __syncthreads();
-        if (d) {
-            for (int l = threadIdx.x; l < BK * 64; l += 256) As[l / 64][l % 64] *= d[k0 + l / 64];
+        if (more) {
+            gemm_store_chunk(As[buf ^ 1], Bs[buf ^ 1], transA, transB, ra, rb, d, k0 + kGemmBK);
             __syncthreads();
+            buf ^= 1;
         }
-#pragma unroll
-        for (int kk = 0; kk < BK; kk++) {
-            double av[4], bv[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) av[i] = As[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; j++) bv[j] = Bs[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] += av[i] * bv[j];
-        }
-        __syncthreads();
     }
     double* cc = C + t.woff;
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 8; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) cc[(int64_t)(i0 + ty + 16 * i) * np + j0 + tx + 16 * j] = acc[i][j];
+        for (int j = 0; j < 8; j++) cc[(int64_t)(i0 + ty + 8 * i) * np + j0 + tx + 8 * j] = acc[i][j];
 }
 
 // Global index of local row a (0..63) of pair (I, J): first 32 rows are column
@@ -305,7 +355,8 @@ __global__ void __launch_bounds__(kJThreads) bj_solve_kernel(const BlockTask* __
         S[a * kLd + bq] = w[(int64_t)pair_idx(I, J, a) * t.np + pair_idx(I, J, bq)];
     }
     __syncthreads();
-    jacobi_smem(S, Q, 64, kJacobiSweeps, kJacobiTol);
+    // the outer block-Jacobi sweeps iterate anyway: a few inner sweeps suffice
+    jacobi_smem(S, Q, 64, kPairSweeps, kJacobiRotEps);
     __syncthreads();
     double* qo = Qbuf + t.qoff + (int64_t)pk.k * 4096;
     for (int l = threadIdx.x; l < 64 * 64; l += blockDim.x) qo[l] = Q[(l / 64) * kLd + (l % 64)];
@@ -416,10 +467,13 @@ __global__ void __launch_bounds__(256) bj_update_v_kernel(const BlockTask* __res
     }
 }
 
-__global__ void bj_check_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ Ww, double tol,
+__global__ void bj_check_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ Ww,
+                                const double* __restrict__ tols, const double* __restrict__ abs_tols,
                                 int* __restrict__ bmask) {
     __shared__ double red[33];
     if (!bmask[blockIdx.x]) return;
+    const double tol = tols[blockIdx.x];
+    const double atol = abs_tols ? abs_tols[blockIdx.x] : 0.0;
     const BlockTask t = tasks[blockIdx.x];
     const double* w = Ww + t.woff;
     double off = 0.0, tot = 0.0;
@@ -431,7 +485,7 @@ __global__ void bj_check_kernel(const BlockTask* __restrict__ tasks, const doubl
     }
     off = block_sum(off, red);
     tot = block_sum(tot, red);
-    if (threadIdx.x == 0 && !(off > tol * tol * tot)) bmask[blockIdx.x] = 0;
+    if (threadIdx.x == 0 && !(off > fmax(tol * tol * tot, atol * atol))) bmask[blockIdx.x] = 0;
 }
 
 __global__ void count_open_kernel(int n, const int* __restrict__ bmask, int* out) {
@@ -448,32 +502,252 @@ __global__ void count_open_kernel(int n, const int* __restrict__ bmask, int* out
     }
 }
 
-__global__ void pos_weights_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ Ww,
-                                   const double* __restrict__ mu, double* __restrict__ dw) {
+// dx = max(lam, 0) / mu and dz = max(-lam, 0), zero on padding
+__global__ void pos_weights_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ lam,
+                                   const double* __restrict__ mu, const int* __restrict__ bmask,
+                                   double* __restrict__ dx, double* __restrict__ dz) {
+    if (bmask && !bmask[blockIdx.x]) return;
     const BlockTask t = tasks[blockIdx.x];
     const double m = mu[t.inst];
-    double* d = dw + t.doff;
     for (int j = threadIdx.x; j < t.np; j += blockDim.x) {
-        const double lam = Ww[t.woff + (int64_t)j * t.np + j];
-        d[j] = (lam > 0.0) ? lam / m : 0.0;
+        const double l = lam[t.doff + j];
+        const bool real = j < t.n;
+        dx[t.doff + j] = (real && l > 0.0) ? l / m : 0.0;
+        dz[t.doff + j] = (real && l < 0.0) ? -l : 0.0;
+    }
+}
+
+// lam = diag(W) for blocks diagonalised by Jacobi
+__global__ void lam_from_diag_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ Ww,
+                                     const int* __restrict__ bmask, double* __restrict__ lam) {
+    if (bmask && !bmask[blockIdx.x]) return;
+    const BlockTask t = tasks[blockIdx.x];
+    for (int j = threadIdx.x; j < t.np; j += blockDim.x) lam[t.doff + j] = Ww[t.woff + (int64_t)j * t.np + j];
+}
+
+// ---- Ogita-Aishima refinement of the previous eigenvectors -------------------
+//
+// With S = V^T U V and G = V^T V (R = I - G), the refined eigenvalues are
+// lam_i = s_ii / g_ii and the correction V <- V (I + E) has
+//   E_ij = (s_ij - lam_j g_ij) / (lam_j - lam_i)   (i != j),   E_ii = (1 - g_ii) / 2,
+// which removes the off-diagonal part of S to first order and restores
+// orthogonality (Ogita and Aishima, Japan J. Indust. Appl. Math. 35 (2018)
+// 1007-1035, Algorithm 1).  A pair whose coupling is negligible gets the
+// orthogonality term only; a pair with |E_ij| > kHard (nearly degenerate and
+// strongly coupled, where the first-order step is invalid) marks its block
+// for the Jacobi fallback.  emax[block] = max |E_ij| decides convergence:
+// the error left after the update is of order emax^2.
+
+constexpr double kHard = 0.1;
+
+__global__ void oa_lambda_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ S,
+                                 const double* __restrict__ G, const int* __restrict__ bmask,
+                                 double* __restrict__ lam, double* __restrict__ scale) {
+    __shared__ double red[33];
+    if (bmask && !bmask[blockIdx.x]) return;
+    const BlockTask t = tasks[blockIdx.x];
+    double mx = 0.0;
+    for (int i = threadIdx.x; i < t.np; i += blockDim.x) {
+        const int64_t d = t.woff + (int64_t)i * t.np + i;
+        const double l = (i < t.n) ? S[d] / G[d] : 0.0;
+        lam[t.doff + i] = l;
+        mx = fmax(mx, fabs(l));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, red[w]);
+        scale[blockIdx.x] = m;
+    }
+}
+
+// One pass per row: partner[i] = the single j that is strongly coupled to i
+// (|num| > kHard |gap|, not negligible), -1 for none, -2 for several.
+__global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ S,
+                                const double* __restrict__ G, const double* __restrict__ lam,
+                                const double* __restrict__ scale, const int* __restrict__ bmask,
+                                int* __restrict__ partner, int* __restrict__ hard) {
+    __shared__ int cnt, who;
+    const int task = blockIdx.y;
+    if (bmask && !bmask[task]) return;
+    const BlockTask t = tasks[task];
+    const int i = blockIdx.x;
+    if (i >= t.np) return;
+    if (threadIdx.x == 0) {
+        cnt = 0;
+        who = -1;
+    }
+    __syncthreads();
+    if (i < t.n) {
+        const double negligible = 1e-15 * scale[task];
+        const double li = lam[t.doff + i];
+        for (int j = threadIdx.x; j < t.n; j += blockDim.x) {
+            if (j == i) continue;
+            const int64_t w = t.woff + (int64_t)i * t.np + j;
+            const double lj = lam[t.doff + j];
+            const double num = S[w] - lj * G[w];
+            if (fabs(num) > negligible && !(fabs(num) <= kHard * fabs(lj - li))) {
+                atomicAdd(&cnt, 1);
+                who = j;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int pj = cnt == 0 ? -1 : (cnt == 1 ? who : -2);
+        partner[t.doff + i] = pj;
+        if (pj == -2) atomicOr(hard + task, 1);
+    }
+}
+
+// M = I + E.  Isolated strongly coupled pairs (partner of each other) get
+// the exact Jacobi rotation of their 2 x 2 problem instead of the first-order
+// step; the next sweep sees them decoupled.
+__global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ S,
+                                 const double* __restrict__ G, const double* __restrict__ lam,
+                                 const double* __restrict__ scale, const int* __restrict__ partner,
+                                 const int* __restrict__ bmask, double* __restrict__ M,
+                                 unsigned long long* __restrict__ emax, int* __restrict__ hard) {
+    const int task = blockIdx.y;
+    if (bmask && !bmask[task]) return;
+    const BlockTask t = tasks[task];
+    const int i = blockIdx.x;
+    if (i >= t.np) return;
+    const double negligible = 1e-15 * scale[task];
+    const double li = lam[t.doff + i];
+    const int pi = (i < t.n) ? partner[t.doff + i] : -1;
+    double emx = 0.0;
+    int hd = 0;
+    // exact rotation of an isolated pair (i, pi)
+    double rc = 1.0, rs = 0.0;
+    if (pi >= 0 && partner[t.doff + pi] == i) {
+        const int p = i < pi ? i : pi, q = i < pi ? pi : i;
+        const double app = lam[t.doff + p], aqq = lam[t.doff + q];
+        const int64_t wpq = t.woff + (int64_t)p * t.np + q;
+        const double apq = S[wpq] - aqq * G[wpq];
+        const double tau = (aqq - app) / (2.0 * apq);
+        const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        rc = 1.0 / sqrt(1.0 + tt * tt);
+        rs = tt * rc;
+        emx = fabs(rs);
+    } else if (pi >= 0) {
+        hd = 1;  // one-sided strong coupling: not an isolated pair
+    }
+    for (int j = threadIdx.x; j < t.np; j += blockDim.x) {
+        const int64_t w = t.woff + (int64_t)i * t.np + j;
+        double m;
+        if (i >= t.n || j >= t.n) {
+            m = (i == j) ? 1.0 : 0.0;
+        } else if (i == j) {
+            m = (pi >= 0) ? rc : 1.0 + 0.5 * (1.0 - G[w]);
+        } else if (j == pi) {
+            // J_pp = c, J_pq = s, J_qp = -s, J_qq = c with p < q
+            m = (i < j) ? rs : -rs;
+        } else {
+            const double lj = lam[t.doff + j];
+            const double num = S[w] - lj * G[w];
+            const double gap = lj - li;
+            double e;
+            if (fabs(num) <= negligible) {
+                e = -0.5 * G[w];
+            } else if (!(fabs(num) <= kHard * fabs(gap))) {
+                hd = 1;  // cannot happen for a consistent partner table
+                e = 0.0;
+            } else {
+                e = num / gap;
+            }
+            emx = fmax(emx, fabs(e));
+            m = e;
+        }
+        M[w] = m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        emx = fmax(emx, __shfl_down_sync(0xffffffffu, emx, o));
+        hd |= __shfl_down_sync(0xffffffffu, hd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (emx > 0.0) atomicMax(emax + task, (unsigned long long)__double_as_longlong(emx));
+        if (hd) atomicOr(hard + task, 1);
+    }
+}
+
+// After an analysis: upd = ref & !hard (apply V <- V M), jac |= ref & hard,
+// ref = upd & (emax > tol) (another sweep needed); counts ref into n_ref.
+__global__ void oa_masks_kernel(int ntasks, const unsigned long long* __restrict__ emax,
+                                const int* __restrict__ hard, const double* __restrict__ tols,
+                                const double* __restrict__ abs_tols, const double* __restrict__ scale,
+                                int* __restrict__ ref,
+                                int* __restrict__ upd, int* __restrict__ jac, int* __restrict__ n_ref) {
+    int cnt = 0;
+    for (int t = threadIdx.x; t < ntasks; t += blockDim.x) {
+        const int r = ref[t];
+        const int h = hard[t];
+        upd[t] = r && !h;
+        if (r && h) jac[t] = 1;
+        const double e = __longlong_as_double((long long)emax[t]);
+        // residual after the update ~ emax^2 * scale: stop when that is below the
+        // absolute tolerance, or when emax is below the relative one
+        double lim = tols[t];
+        if (abs_tols && scale[t] > 0.0) lim = fmax(lim, sqrt(abs_tols[t] / scale[t]));
+        const int again = r && !h && (e > lim);
+        ref[t] = again;
+        cnt += again;
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    __shared__ int s[32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += s[w];
+        *n_ref = tot;
+    }
+}
+
+__global__ void merge_mask_kernel(int n, const int* __restrict__ src, int* __restrict__ dst) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (src[i]) dst[i] = 1;
+}
+
+__global__ void copy_blocks_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ src,
+                                   double* __restrict__ dst, const int* __restrict__ bmask) {
+    if (bmask && !bmask[blockIdx.y]) return;
+    const BlockTask t = tasks[blockIdx.y];
+    const int p = blockIdx.x;
+    if (p >= t.np) return;
+    const int64_t o = t.woff + (int64_t)p * t.np;
+    for (int q = threadIdx.x; q < t.np; q += blockDim.x) dst[o + q] = src[o + q];
+}
+
+__global__ void count_kernel(int n, const int* __restrict__ mask, int* out) {
+    int c = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) c += mask[i] != 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    __shared__ int s[32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += s[w];
+        *out = tot;
     }
 }
 
 __global__ void write_xz_kernel(const BlockTask* __restrict__ tasks, int B, const double* __restrict__ Xw,
-                                const double* __restrict__ Uw, const double* __restrict__ mu,
-                                const int* __restrict__ mask, double* __restrict__ x, double* __restrict__ z) {
+                                const double* __restrict__ Zw, const int* __restrict__ mask, double* __restrict__ x,
+                                double* __restrict__ z) {
     const BlockTask t = tasks[blockIdx.y];
     const int p = blockIdx.x;
     if (p >= t.n) return;
     const int b = t.inst;
     if (mask && !mask[b]) return;
-    const double m = mu[b];
     for (int q = threadIdx.x; q < t.n; q += blockDim.x) {
         const int64_t w = t.woff + (int64_t)p * t.np + q;
         const int64_t e = (t.xoff + (int64_t)p * t.n + q) * B + b;
-        const double xv = Xw[w];
-        x[e] = xv;
-        z[e] = m * xv - Uw[w];
+        x[e] = Xw[w];
+        z[e] = Zw[w];
     }
 }
 
@@ -496,24 +770,28 @@ void launch_small_project(const BlockTask* tasks, int ntasks, int B, const doubl
     if (ntasks == 0) return;
     set_smem_attrs();
     small_project_kernel<<<ntasks, kJThreads, kJacobiSmem, s>>>(tasks, B, aty, c, x, z, mu, mask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_form_u(const BlockTask* tasks, int ntasks, int max_np, int B, const double* aty, const double* c,
                       const double* x, const double* mu, const int* mask, double* Uw, cudaStream_t s) {
     if (ntasks == 0) return;
     form_u_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, B, aty, c, x, mu, mask, Uw);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_cold_start(const BlockTask* tasks, int ntasks, int max_np, const double* Uw, double* Ww, double* Vw,
                           const int* bmask, cudaStream_t s) {
     if (ntasks == 0) return;
     cold_start_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, Uw, Ww, Vw, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
                  const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s) {
     if (ntiles == 0) return;
-    gemm_kernel<<<ntiles, 256, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
+    gemm_kernel<<<ntiles, 64, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_bj_solve(const BlockTask* tasks, const PairTask* pt, int npt, int round, double* Ww, double* Qbuf,
@@ -521,6 +799,7 @@ void launch_bj_solve(const BlockTask* tasks, const PairTask* pt, int npt, int ro
     if (npt == 0) return;
     set_smem_attrs();
     bj_solve_kernel<<<npt, kJThreads, kJacobiSmem, s>>>(tasks, pt, round, Ww, Qbuf, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, int round, double* Ww,
@@ -528,6 +807,7 @@ void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, in
     if (nwt == 0) return;
     set_smem_attrs();
     bj_update_w_kernel<<<nwt, 256, kJacobiSmem, s>>>(tasks, wt, round, Ww, Qbuf, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, int round, double* Vw,
@@ -535,25 +815,76 @@ void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, in
     if (nvt == 0) return;
     set_smem_attrs();
     bj_update_v_kernel<<<nvt, 256, kJacobiSmem, s>>>(tasks, vt, round, Vw, Qbuf, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-void launch_bj_check(const BlockTask* tasks, int ntasks, const double* Ww, double tol, int* bmask, int* n_open,
+void launch_bj_check(const BlockTask* tasks, int ntasks, const double* Ww, const double* tol, const double* abs_tol,
+                     int* bmask, int* n_open, cudaStream_t s) {
+    if (ntasks == 0) return;
+    bj_check_kernel<<<ntasks, 256, 0, s>>>(tasks, Ww, tol, abs_tol, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    count_open_kernel<<<1, 1024, 0, s>>>(ntasks, bmask, n_open);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_pos_weights(const BlockTask* tasks, int ntasks, const double* lam, const double* mu, const int* bmask,
+                        double* dx, double* dz, cudaStream_t s) {
+    if (ntasks == 0) return;
+    pos_weights_kernel<<<ntasks, 128, 0, s>>>(tasks, lam, mu, bmask, dx, dz);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, const int* bmask, double* lam,
+                          cudaStream_t s) {
+    if (ntasks == 0) return;
+    lam_from_diag_kernel<<<ntasks, 128, 0, s>>>(tasks, Ww, bmask, lam);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
+                       const int* bmask, double* lam, double* scale, int* partner, double* M,
+                       unsigned long long* emax, int* hard, cudaStream_t s) {
+    if (ntasks == 0) return;
+    oa_lambda_kernel<<<ntasks, 256, 0, s>>>(tasks, S, G, bmask, lam, scale);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    oa_pairs_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, bmask, partner, hard);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    oa_update_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, partner, bmask, M, emax,
+                                                           hard);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_oa_masks(int ntasks, const unsigned long long* emax, const int* hard, const double* tol,
+                     const double* abs_tol, const double* scale, int* ref, int* upd, int* jac, int* n_ref,
                      cudaStream_t s) {
     if (ntasks == 0) return;
-    bj_check_kernel<<<ntasks, 256, 0, s>>>(tasks, Ww, tol, bmask);
-    count_open_kernel<<<1, 1024, 0, s>>>(ntasks, bmask, n_open);
+    oa_masks_kernel<<<1, 1024, 0, s>>>(ntasks, emax, hard, tol, abs_tol, scale, ref, upd, jac, n_ref);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-void launch_pos_weights(const BlockTask* tasks, int ntasks, const double* Ww, const double* mu, double* dw,
-                        cudaStream_t s) {
+void launch_copy_blocks(const BlockTask* tasks, int ntasks, int max_np, const double* src, double* dst,
+                        const int* bmask, cudaStream_t s) {
     if (ntasks == 0) return;
-    pos_weights_kernel<<<ntasks, 128, 0, s>>>(tasks, Ww, mu, dw);
+    copy_blocks_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, src, dst, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-void launch_write_xz(const BlockTask* tasks, int ntasks, int max_n, int B, const double* Xw, const double* Uw,
-                        const double* mu, const int* mask, double* x, double* z, cudaStream_t s) {
+void launch_merge_mask(int n, const int* src, int* dst, cudaStream_t s) {
+    if (n == 0) return;
+    merge_mask_kernel<<<1, 1024, 0, s>>>(n, src, dst);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_count(int n, const int* mask, int* out, cudaStream_t s) {
+    count_kernel<<<1, 1024, 0, s>>>(n, mask, out);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_write_xz(const BlockTask* tasks, int ntasks, int max_n, int B, const double* Xw, const double* Zw,
+                     const int* mask, double* x, double* z, cudaStream_t s) {
     if (ntasks == 0) return;
-    write_xz_kernel<<<dim3(max_n, ntasks), 128, 0, s>>>(tasks, B, Xw, Uw, mu, mask, x, z);
+    write_xz_kernel<<<dim3(max_n, ntasks), 128, 0, s>>>(tasks, B, Xw, Zw, mask, x, z);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 }  // namespace v2g

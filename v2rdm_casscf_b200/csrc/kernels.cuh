@@ -9,9 +9,13 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 namespace v2g {
+
+// Number of kernels the launchers below have issued (all threads, all devices).
+extern std::atomic<long> g_kernel_launches;
 
 struct DevCsr {
     int64_t nrows = 0;
@@ -24,6 +28,10 @@ struct DevCsr {
 // (each of sub, coef, add optional); instances with mask[b] == 0 are skipped.
 void launch_spmv(const DevCsr& A, int B, const double* in, double* out, const double* sub, const double* coef,
                  const double* add, const int* mask, cudaStream_t s);
+
+// out = A in, and dot_out[b] = sum_r dotv[r,b] out[r,b] (deterministic).
+void launch_spmv_dot(const DevCsr& A, int B, const double* in, double* out, const double* dotv, const int* mask,
+                     double* partial, double* dot_out, cudaStream_t s);
 
 // Per-instance reductions over interleaved vectors of n elements.
 enum ReduceMode {
@@ -54,9 +62,9 @@ void launch_cg_init(int64_t n, int B, const double* rhs, const double* Ap, doubl
                     cudaStream_t s);
 // alpha = rr / pap
 void launch_cg_alpha(int B, CgScalars* cs, const double* pap, cudaStream_t s);
-// y += alpha p ; r -= alpha Ap
+// y += alpha p ; r -= alpha Ap ; rr_out[b] = r.r
 void launch_cg_update_yr(int64_t n, int B, double* y, double* r, const double* p, const double* Ap,
-                         const CgScalars* cs, cudaStream_t s);
+                         const CgScalars* cs, double* partial, double* rr_out, cudaStream_t s);
 // convergence test and beta; counts instances still active into *n_active
 void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cudaStream_t s);
 // p = beta p + r
@@ -115,14 +123,33 @@ void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, in
 void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, int round, double* Vw,
                         const double* Qbuf, const int* bmask, cudaStream_t s);
 // Per-block off-diagonal and total Frobenius norms of W; sets bmask[t] = 0
-// for blocks whose off-diagonal norm is below tol * total (converged).
-void launch_bj_check(const BlockTask* tasks, int ntasks, const double* Ww, double tol, int* bmask, int* n_open,
+// for blocks whose off-diagonal norm is below max(tol[t] * total, abs_tol[t]).
+void launch_bj_check(const BlockTask* tasks, int ntasks, const double* Ww, const double* tol, const double* abs_tol,
+                     int* bmask, int* n_open, cudaStream_t s);
+// dx = max(lam, 0) / mu and dz = max(-lam, 0) (per block, length np; zero on padding)
+void launch_pos_weights(const BlockTask* tasks, int ntasks, const double* lam, const double* mu, const int* bmask,
+                        double* dx, double* dz, cudaStream_t s);
+// lam = diag(W)
+void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, const int* bmask, double* lam,
+                          cudaStream_t s);
+// Ogita-Aishima step: lam_i = s_ii / g_ii and M = I + E from S = V^T U V and
+// G = V^T V; emax[t] gets max |E_ij| (as the bits of a non-negative double)
+// and hard[t] is set for blocks needing the Jacobi fallback (an index
+// strongly coupled to more than one other; isolated strongly coupled pairs
+// are rotated exactly).  partner needs one int per padded row.
+void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
+                       const int* bmask, double* lam, double* scale, int* partner, double* M,
+                       unsigned long long* emax, int* hard, cudaStream_t s);
+void launch_oa_masks(int ntasks, const unsigned long long* emax, const int* hard, const double* tol,
+                     const double* abs_tol, const double* scale, int* ref, int* upd, int* jac, int* n_ref,
                      cudaStream_t s);
-// d = max(diag(W), 0) / mu (per block, length np)
-void launch_pos_weights(const BlockTask* tasks, int ntasks, const double* Ww, const double* mu, double* dw,
-                        cudaStream_t s);
-// x = X (unpadded, interleaved) and z = mu X - U
-void launch_write_xz(const BlockTask* tasks, int ntasks, int max_n, int B, const double* Xw, const double* Uw,
-                     const double* mu, const int* mask, double* x, double* z, cudaStream_t s);
+void launch_copy_blocks(const BlockTask* tasks, int ntasks, int max_np, const double* src, double* dst,
+                        const int* bmask, cudaStream_t s);
+void launch_count(int n, const int* mask, int* out, cudaStream_t s);
+// dst[i] |= src[i]
+void launch_merge_mask(int n, const int* src, int* dst, cudaStream_t s);
+// x = X and z = Z (unpadded, interleaved)
+void launch_write_xz(const BlockTask* tasks, int ntasks, int max_n, int B, const double* Xw, const double* Zw,
+                     const int* mask, double* x, double* z, cudaStream_t s);
 
 }  // namespace v2g

@@ -35,6 +35,10 @@ struct Options {
     int cg_maxiter = 10000;
     double tau = 1.0;
     int mu_update_frequency = 500;
+    // Accept an eigendecomposition whose off-diagonal residual is below
+    // 0.01 min(eps_p, eps_d) (the CG tolerance rule); off = every projection
+    // converged, as the reference's Update_xz.
+    bool adaptive_projection = false;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for

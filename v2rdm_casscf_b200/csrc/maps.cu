@@ -10,6 +10,8 @@
 
 namespace v2g {
 
+std::atomic<long> g_kernel_launches{0};
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -21,28 +23,73 @@ inline int grid_for(int64_t work, int threads = kThreads) {
     return (int)g;
 }
 
+constexpr int kRedBlocks = 148 * 4;
+constexpr int kSpmvBlocks = 148 * 64;
+
+// Thread mapping shared by the map and vector kernels that also reduce: the
+// rows are cut into passes of T/B rows; pass k goes to block k % G, where
+// thread t handles instance t % B of row t / B.  A thread therefore always
+// serves the same instance (per-instance partial sums come out in a fixed
+// order) and the rows in flight at any moment form one contiguous window,
+// which keeps the gathers of neighbouring rows in L2.
+struct Chunk {
+    int64_t first, stride, nrows;
+    int b, rsub, rows_per_pass;
+    bool live;
+};
+__device__ __forceinline__ Chunk chunk_of(int64_t nrows, int B) {
+    Chunk c;
+    c.rows_per_pass = blockDim.x / B;
+    const int lanes = c.rows_per_pass * B;
+    c.b = threadIdx.x % B;
+    c.rsub = threadIdx.x / B;
+    c.live = threadIdx.x < lanes;
+    c.first = (int64_t)blockIdx.x * c.rows_per_pass + c.rsub;
+    c.stride = (int64_t)gridDim.x * c.rows_per_pass;
+    c.nrows = nrows;
+    return c;
+}
+
+// Per-instance block partial of v, written to partial[block * B + b].
+__device__ __forceinline__ void block_partial(double v, int B, double* __restrict__ partial) {
+    __shared__ double sh[kThreads];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    if (threadIdx.x < B) {
+        const int rows_per_pass = blockDim.x / B;
+        double s = 0.0;
+        for (int k = 0; k < rows_per_pass; k++) s += sh[threadIdx.x + k * B];
+        partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
+    }
+}
+
+// out[r,b] = coef[b] * (sum_k val[k] in[col[k],b] - sub[r]) + add[r,b];
+// with dotv, also partial[., b] of sum_r dotv[r,b] * out[r,b].
 __global__ void spmv_kernel(int64_t nrows, int B, const int64_t* __restrict__ rowptr,
                             const int32_t* __restrict__ col, const double* __restrict__ val,
                             const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ sub,
                             const double* __restrict__ coef, const double* __restrict__ add,
-                            const int* __restrict__ mask) {
-    const int64_t total = nrows * B;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = t / B;
-        const int b = (int)(t - r * B);
-        if (mask && !mask[b]) continue;
-        double s = 0.0;
-        const int64_t k1 = rowptr[r + 1];
-        for (int64_t k = rowptr[r]; k < k1; k++) s += val[k] * in[(int64_t)col[k] * B + b];
-        if (sub) s -= sub[r];
-        if (coef) s *= coef[b];
-        if (add) s += add[t];
-        out[t] = s;
+                            const int* __restrict__ mask, const double* __restrict__ dotv,
+                            double* __restrict__ partial) {
+    const Chunk ch = chunk_of(nrows, B);
+    double acc = 0.0;
+    if (ch.live && !(mask && !mask[ch.b])) {
+        const int b = ch.b;
+        const double cf = coef ? coef[b] : 1.0;
+        for (int64_t r = ch.first; r < ch.nrows; r += ch.stride) {
+            double s = 0.0;
+            const int64_t k1 = rowptr[r + 1];
+            for (int64_t k = rowptr[r]; k < k1; k++) s += val[k] * in[(int64_t)col[k] * B + b];
+            const int64_t t = r * B + b;
+            if (sub) s -= sub[r];
+            if (coef) s *= cf;
+            if (add) s += add[t];
+            out[t] = s;
+            if (dotv) acc += dotv[t] * s;
+        }
     }
+    if (partial) block_partial(acc, B, partial);
 }
-
-constexpr int kRedBlocks = 148 * 4;
 
 // Stage 1: block g reduces a contiguous chunk of elements for every instance;
 // thread t handles instance t % B on element rows t / B, t / B + T/B, ...
@@ -88,12 +135,20 @@ __global__ void reduce_stage1(int mode, int64_t n, int B, const double* __restri
     }
 }
 
+// Stage 2: one block per instance sums its nblk partials with a fixed tree
+// (deterministic), instead of one thread walking a long dependent chain.
 __global__ void reduce_stage2(int nblk, int B, const double* __restrict__ partial, double* __restrict__ out) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B) return;
+    __shared__ double sh[kThreads];
+    const int b = blockIdx.x;
     double s = 0.0;
-    for (int k = 0; k < nblk; k++) s += partial[(int64_t)k * B + b];
-    out[b] = s;
+    for (int k = threadIdx.x; k < nblk; k += blockDim.x) s += partial[(int64_t)k * B + b];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[b] = sh[0];
 }
 
 __global__ void c_minus_z_kernel(int64_t n, int B, const double* __restrict__ c, double* __restrict__ z,
@@ -139,18 +194,28 @@ __global__ void cg_alpha_kernel(int B, CgScalars* cs, const double* pap) {
     cs[b].alpha = cs[b].rr / pap[b];
 }
 
+// y += alpha p ; r -= alpha Ap ; partial[., b] of r.r (cg_solver.cc:159-165)
 __global__ void cg_update_yr_kernel(int64_t n, int B, double* __restrict__ y, double* __restrict__ r,
                                     const double* __restrict__ p, const double* __restrict__ Ap,
-                                    const CgScalars* __restrict__ cs) {
-    const int64_t total = n * B;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int b = (int)(t % B);
-        if (!cs[b].active) continue;
+                                    const CgScalars* __restrict__ cs, double* __restrict__ partial) {
+    const Chunk ch = chunk_of(n, B);
+    double acc = 0.0;
+    if (ch.live) {
+        const int b = ch.b;
+        const bool act = cs[b].active;
         const double a = cs[b].alpha;
-        y[t] += a * p[t];
-        r[t] += -a * Ap[t];
+        for (int64_t e = ch.first; e < ch.nrows; e += ch.stride) {
+            const int64_t t = e * B + b;
+            double rv = r[t];
+            if (act) {
+                y[t] += a * p[t];
+                rv += -a * Ap[t];
+                r[t] = rv;
+            }
+            acc += rv * rv;
+        }
     }
+    block_partial(acc, B, partial);
 }
 
 // One warp: per instance, test ||r|| < tol (cg_solver.cc:167-171), else beta
@@ -195,43 +260,73 @@ __global__ void cg_update_p_kernel(int64_t n, int B, double* __restrict__ p, con
 
 }  // namespace
 
-void launch_spmv(const DevCsr& A, int B, const double* in, double* out, const double* sub, const double* coef,
-                 const double* add, const int* mask, cudaStream_t s) {
-    spmv_kernel<<<grid_for(A.nrows * B), kThreads, 0, s>>>(A.nrows, B, A.rowptr, A.col, A.val, in, out, sub, coef,
-                                                           add, mask);
+static int spmv_grid(int64_t nrows, int B) {
+    // enough blocks to fill the GPU; rows per block >= rows per pass
+    const int64_t rows_per_pass = kThreads / B;
+    int64_t g = (nrows + rows_per_pass - 1) / rows_per_pass;
+    if (g > kSpmvBlocks) g = kSpmvBlocks;
+    return (int)(g < 1 ? 1 : g);
 }
 
-int64_t reduce_partial_size(int B) { return (int64_t)kRedBlocks * B; }
+void launch_spmv(const DevCsr& A, int B, const double* in, double* out, const double* sub, const double* coef,
+                 const double* add, const int* mask, cudaStream_t s) {
+    spmv_kernel<<<spmv_grid(A.nrows, B), kThreads, 0, s>>>(A.nrows, B, A.rowptr, A.col, A.val, in, out, sub, coef,
+                                                           add, mask, nullptr, nullptr);
+}
+
+int64_t reduce_partial_size(int B) { return (int64_t)kSpmvBlocks * B; }
+
+void launch_spmv_dot(const DevCsr& A, int B, const double* in, double* out, const double* dotv, const int* mask,
+                     double* partial, double* dot_out, cudaStream_t s) {
+    const int g = spmv_grid(A.nrows, B);
+    spmv_kernel<<<g, kThreads, 0, s>>>(A.nrows, B, A.rowptr, A.col, A.val, in, out, nullptr, nullptr, nullptr,
+                                       mask, dotv, partial);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    reduce_stage2<<<B, kThreads, 0, s>>>(g, B, partial, dot_out);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
 
 void launch_reduce(ReduceMode mode, int64_t n, int B, const double* u, const double* v, const double* w,
                    const double* row, double* partial, double* out, cudaStream_t s) {
     reduce_stage1<<<kRedBlocks, kThreads, 0, s>>>((int)mode, n, B, u, v, w, row, partial);
-    reduce_stage2<<<(B + 127) / 128, 128, 0, s>>>(kRedBlocks, B, partial, out);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    reduce_stage2<<<B, kThreads, 0, s>>>(kRedBlocks, B, partial, out);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_c_minus_z(int64_t n, int B, const double* c, double* z, const int* mask, cudaStream_t s) {
     c_minus_z_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, c, z, mask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_cg_init(int64_t n, int B, const double* rhs, const double* Ap, double* r, double* p, const CgScalars* cs,
                     cudaStream_t s) {
     cg_init_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, rhs, Ap, r, p, cs);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 void launch_cg_set_rr(int B, CgScalars* cs, const double* rr, int* n_active, cudaStream_t s) {
     cg_set_rr_kernel<<<1, 32, 0, s>>>(B, cs, rr, n_active);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 void launch_cg_alpha(int B, CgScalars* cs, const double* pap, cudaStream_t s) {
     cg_alpha_kernel<<<(B + 127) / 128, 128, 0, s>>>(B, cs, pap);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 void launch_cg_update_yr(int64_t n, int B, double* y, double* r, const double* p, const double* Ap,
-                         const CgScalars* cs, cudaStream_t s) {
-    cg_update_yr_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, y, r, p, Ap, cs);
+                         const CgScalars* cs, double* partial, double* rr_out, cudaStream_t s) {
+    const int g = spmv_grid(n, B);
+    cg_update_yr_kernel<<<g, kThreads, 0, s>>>(n, B, y, r, p, Ap, cs, partial);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    reduce_stage2<<<B, kThreads, 0, s>>>(g, B, partial, rr_out);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cudaStream_t s) {
     cg_beta_kernel<<<1, 32, 0, s>>>(B, cs, rrnew, n_active);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s) {
     cg_update_p_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, p, r, cs);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 }  // namespace v2g

@@ -20,6 +20,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/v2rdm_gpu.h"
@@ -133,6 +134,7 @@ struct Problem {
     OrbitalSpaces sp;
     int device = 0;
     bool record_trace = false;
+    bool profile = false;
     std::vector<double> c, x, y, z;
     double mu = 1.0;
     double efzc = 0.0, enuc = 0.0;
@@ -180,8 +182,14 @@ class GroupRun {
         CK(cudaMallocHost(&hnact_, sizeof(int) * 4));
         build_projection_plan();
         upload_state();
+        for (auto* p : P_) profile_ = profile_ || p->profile;
+        if (profile_) {
+            prof_ev_.resize(256);
+            for (auto& e : prof_ev_) CK(cudaEventCreate(&e));
+        }
     }
     ~GroupRun() {
+        for (auto e : prof_ev_) cudaEventDestroy(e);
         if (hscal_) cudaFreeHost(hscal_);
         if (hnact_) cudaFreeHost(hnact_);
         if (s_) cudaStreamDestroy(s_);
@@ -223,23 +231,77 @@ class GroupRun {
     }
 
     // Update_xz for every instance with mask set; ATy is left in aty_.
-    void project() {
+    // rho[b] > 0 lets instance b accept an eigendecomposition whose
+    // off-diagonal residual is below rho[b] in absolute terms (the adaptive
+    // projection, rho = 0.01 min(eps_p, eps_d) like the CG tolerance rule);
+    // rho[b] = 0 asks for a converged one.  x = V D+ V^T / mu and z = V D- V^T
+    // are positive semidefinite either way.
+    void project(const std::vector<double>& rho = {}) {
         launch_spmv(T_.AT(), B_, y_.p, aty_.p, nullptr, nullptr, nullptr, mask_.p, s_);
         launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_);
         if (nlarge_ == 0) return;
         launch_form_u(large_d_.p, nlarge_, max_np_, B_, aty_.p, c_.p, x_.p, mu_.p, mask_.p, U_.p, s_);
-        // blocks of active instances take part
-        set_block_masks();
+        set_block_masks();  // bact_ = blocks of active instances
+        set_block_tolerances(rho);
         if (!warm_) {
+            // cold start: W = U, V = I, block Jacobi to convergence
             launch_cold_start(large_d_.p, nlarge_, max_np_, U_.p, W_.p, V_.p, bact_.p, s_);
+            CK(cudaMemcpyAsync(bjac_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
+            block_jacobi(40);
         } else {
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bact_.p, s_);
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bact_.p, s_);
+            refine();
         }
-        CK(cudaMemcpyAsync(bwork_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
-        const int max_sweeps = 30;
+        launch_pos_weights(large_d_.p, nlarge_, lam_.p, mu_.p, bact_.p, dw_.p, dz_.p, s_);
+        launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, V_.p, true, dw_.p, Tm_.p, bact_.p, s_);
+        launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, V_.p, true, dz_.p, M_.p, bact_.p, s_);
+        launch_write_xz(large_d_.p, nlarge_, max_n_, B_, Tm_.p, M_.p, mask_.p, x_.p, z_.p, s_);
+        warm_ = true;
+    }
+
+    // Ogita-Aishima sweeps from the previous eigenvectors; blocks with a hard
+    // pair or without convergence after kMaxOa sweeps go to block Jacobi.
+    void refine() {
+        constexpr int kMaxOa = 6;
+        CK(cudaMemcpyAsync(bref_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
+        CK(cudaMemsetAsync(bjac_.p, 0, nlarge_ * sizeof(int), s_));
+        int nref = 1;
+        for (int sweep = 0; sweep < kMaxOa && nref > 0; sweep++) {
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bref_.p, s_);
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bref_.p, s_);
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, V_.p, false, nullptr, G_.p, bref_.p, s_);
+            CK(cudaMemsetAsync(emax_.p, 0, nlarge_ * sizeof(unsigned long long), s_));
+            CK(cudaMemsetAsync(hard_.p, 0, nlarge_ * sizeof(int), s_));
+            launch_oa_analyze(large_d_.p, nlarge_, max_np_, W_.p, G_.p, bref_.p, lam_.p, scale_.p, partner_.p,
+                              M_.p, emax_.p, hard_.p, s_);
+            launch_oa_masks(nlarge_, emax_.p, hard_.p, otol_.p, atol_.p, scale_.p, bref_.p, bupd_.p, bjac_.p,
+                            nact_.p + 2, s_);
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, M_.p, false, nullptr, Tm_.p, bupd_.p, s_);
+            launch_copy_blocks(large_d_.p, nlarge_, max_np_, Tm_.p, V_.p, bupd_.p, s_);
+            CK(cudaMemcpyAsync(hnact_ + 2, nact_.p + 2, sizeof(int), cudaMemcpyDeviceToHost, s_));
+            CK(cudaStreamSynchronize(s_));
+            nref = hnact_[2];
+            oa_sweeps_++;
+        }
+        // blocks still unconverged join the Jacobi set (their OA update was applied)
+        if (nref > 0) launch_merge_mask(nlarge_, bref_.p, bjac_.p, s_);
+        launch_count(nlarge_, bjac_.p, nact_.p + 3, s_);
+        CK(cudaMemcpyAsync(hnact_ + 3, nact_.p + 3, sizeof(int), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
+        if (hnact_[3] > 0) {
+            jacobi_blocks_ += hnact_[3];
+            // warm block Jacobi on W = V^T U V with the current V
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bjac_.p, s_);
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bjac_.p, s_);
+            block_jacobi(30);
+        }
+    }
+
+    // Block Jacobi on the blocks flagged in bjac_ until their relative
+    // off-diagonal norm is below 1e-13; sets lam = diag(W) for them.
+    void block_jacobi(int max_sweeps) {
+        CK(cudaMemcpyAsync(bwork_.p, bjac_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
         for (int sweep = 0; sweep < max_sweeps; sweep++) {
-            launch_bj_check(large_d_.p, nlarge_, W_.p, 1e-14, bwork_.p, nact_.p + 1, s_);
+            launch_bj_check(large_d_.p, nlarge_, W_.p, jtol_.p, atol_.p, bwork_.p, nact_.p + 1, s_);
             CK(cudaMemcpyAsync(hnact_ + 1, nact_.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s_));
             CK(cudaStreamSynchronize(s_));
             if (hnact_[1] == 0) break;
@@ -250,10 +312,7 @@ class GroupRun {
             }
             sweeps_total_++;
         }
-        launch_pos_weights(large_d_.p, nlarge_, W_.p, mu_.p, dw_.p, s_);
-        launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, V_.p, true, dw_.p, Tm_.p, bact_.p, s_);
-        launch_write_xz(large_d_.p, nlarge_, max_n_, B_, Tm_.p, U_.p, mu_.p, mask_.p, x_.p, z_.p, s_);
-        warm_ = true;
+        launch_lam_from_diag(large_d_.p, nlarge_, W_.p, bjac_.p, lam_.p, s_);
     }
 
     void apply_A(const double* d_in, double* d_out) {
@@ -322,7 +381,11 @@ class GroupRun {
             cg_solve();
             CK(cudaMemcpyAsync(cs.data(), cs_.p, B_ * sizeof(CgScalars), cudaMemcpyDeviceToHost, s_));
             CK(cudaEventRecord(e1, s_));
-            project();
+            std::vector<double> rho(B_, 0.0);
+            for (int b = 0; b < B_; b++)
+                if (opt(b).adaptive_projection)
+                    rho[b] = (oiter[b] == 0) ? 0.01 : 0.01 * std::min(ep[b], ed[b]);
+            project(rho);
             CK(cudaEventRecord(e2, s_));
             // ed = ||A^T y + z - c||, ep = ||A x - b||, E = c.x, b.y (:1826-1852)
             launch_reduce(RED_ED, nx_, B_, aty_.p, z_.p, c_.p, nullptr, partial_.p, red_.p, s_);
@@ -394,28 +457,64 @@ class GroupRun {
         cudaEventDestroy(e1);
         cudaEventDestroy(e2);
         cudaEventDestroy(e3);
-        download_state();
     }
 
     long jacobi_sweeps() const { return sweeps_total_; }
+    long oa_sweeps() const { return oa_sweeps_; }
+    long jacobi_blocks() const { return jacobi_blocks_; }
+    double map_seconds() const { return map_sec_; }
+    long map_launches() const { return map_n_; }
+    double map_bytes() const { return map_bytes_; }
+    double h2d_bytes() const { return 8.0 * B_ * (3.0 * nx_ + nc_); }
+    double d2h_bytes() const { return 8.0 * B_ * (2.0 * nx_ + nc_); }
 
   private:
+    // CG map launch with optional CUDA-event timing (profile mode).
+    // With dotv, also red_[b] = sum dotv[., b] * out[., b].
+    void map_launch(const DevCsr& M, const double* in, double* out, const double* dotv = nullptr,
+                    const int* mask = nullptr) {
+        auto go = [&]() {
+            if (dotv)
+                launch_spmv_dot(M, B_, in, out, dotv, mask, partial_.p, red_.p, s_);
+            else
+                launch_spmv(M, B_, in, out, nullptr, nullptr, nullptr, mask, s_);
+        };
+        if (!profile_) {
+            go();
+            return;
+        }
+        if (prof_used_ + 2 > prof_ev_.size()) flush_profile();
+        CK(cudaEventRecord(prof_ev_[prof_used_], s_));
+        go();
+        CK(cudaEventRecord(prof_ev_[prof_used_ + 1], s_));
+        prof_used_ += 2;
+        map_bytes_ += 8.0 * (double)(M.nrows + (M.nrows == nc_ ? nx_ : nc_)) * B_;
+    }
+    void flush_profile() {
+        if (prof_used_ == 0) return;
+        CK(cudaEventSynchronize(prof_ev_[prof_used_ - 1]));
+        for (size_t i = 0; i + 1 < prof_used_; i += 2) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, prof_ev_[i], prof_ev_[i + 1]));
+            map_sec_ += ms * 1e-3;
+            map_n_++;
+        }
+        prof_used_ = 0;
+    }
     // CGSolver::solve for every instance whose CG scalars are active.
     void cg_solve() {
         // Ap = A A^T y ; r = B - Ap ; p = r
-        launch_spmv(T_.AT(), B_, y_.p, atp_.p, nullptr, nullptr, nullptr, nullptr, s_);
-        launch_spmv(T_.A(), B_, atp_.p, ap_.p, nullptr, nullptr, nullptr, nullptr, s_);
+        map_launch(T_.AT(), y_.p, atp_.p, nullptr, mask_.p);
+        map_launch(T_.A(), atp_.p, ap_.p, nullptr, mask_.p);
         launch_cg_init(nc_, B_, bv_.p, ap_.p, r_.p, p_.p, cs_.p, s_);
         launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
         launch_cg_set_rr(B_, cs_.p, red_.p, nact_.p, s_);
         const int check_every = 4;
         for (int k = 0;; k++) {
-            launch_spmv(T_.AT(), B_, p_.p, atp_.p, nullptr, nullptr, nullptr, nullptr, s_);
-            launch_spmv(T_.A(), B_, atp_.p, ap_.p, nullptr, nullptr, nullptr, nullptr, s_);
-            launch_reduce(RED_DOT, nc_, B_, p_.p, ap_.p, nullptr, nullptr, partial_.p, red_.p, s_);
+            map_launch(T_.AT(), p_.p, atp_.p, nullptr, mask_.p);
+            map_launch(T_.A(), atp_.p, ap_.p, p_.p, mask_.p);  // Ap and p.Ap
             launch_cg_alpha(B_, cs_.p, red_.p, s_);
-            launch_cg_update_yr(nc_, B_, y_.p, r_.p, p_.p, ap_.p, cs_.p, s_);
-            launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
+            launch_cg_update_yr(nc_, B_, y_.p, r_.p, p_.p, ap_.p, cs_.p, partial_.p, red_.p, s_);
             launch_cg_beta(B_, cs_.p, red_.p, nact_.p, s_);
             launch_cg_update_p(nc_, B_, p_.p, r_.p, cs_.p, s_);
             if ((k + 1) % check_every == 0) {
@@ -424,6 +523,24 @@ class GroupRun {
                 if (hnact_[0] == 0) break;
             }
         }
+        if (profile_) flush_profile();
+    }
+
+    // Jacobi: relative off-diagonal norm 1e-13 or the absolute rho share of
+    // the block; refinement: max |E| <= 1e-7 or residual (~max|E|^2 scale)
+    // below the block's rho share.
+    void set_block_tolerances(const std::vector<double>& rho) {
+        std::vector<int> nblk(B_, 0);
+        for (int t = 0; t < nlarge_; t++) nblk[hlarge_[t].inst]++;
+        std::vector<double> jt(nlarge_, 1e-13), ot(nlarge_, 1e-7), at(nlarge_, 0.0);
+        for (int t = 0; t < nlarge_; t++) {
+            const int b = hlarge_[t].inst;
+            if (!rho.empty() && rho[b] > 0.0) at[t] = rho[b] / std::sqrt((double)nblk[b]);
+        }
+        CK(cudaMemcpyAsync(jtol_.p, jt.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(otol_.p, ot.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(atol_.p, at.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaStreamSynchronize(s_));
     }
 
     void set_block_masks() {
@@ -471,10 +588,24 @@ class GroupRun {
         W_.alloc(woff);
         V_.alloc(woff);
         Tm_.alloc(woff);
+        G_.alloc(woff);
+        M_.alloc(woff);
         Q_.alloc(qoff);
         dw_.alloc(doff);
+        dz_.alloc(doff);
+        jtol_.alloc(nlarge_);
+        otol_.alloc(nlarge_);
+        atol_.alloc(nlarge_);
+        lam_.alloc(doff);
+        partner_.alloc(doff);
+        scale_.alloc(nlarge_);
+        emax_.alloc(nlarge_);
+        hard_.alloc(nlarge_);
         bact_.alloc(nlarge_);
         bwork_.alloc(nlarge_);
+        bref_.alloc(nlarge_);
+        bupd_.alloc(nlarge_);
+        bjac_.alloc(nlarge_);
         std::vector<GemmTile> gt;
         std::vector<PairTask> pt;
         std::vector<WTileTask> wt;
@@ -517,8 +648,10 @@ class GroupRun {
     std::vector<BlockTask> hlarge_;
     DevBuf<BlockTask> small_d_, large_d_;
     int nsmall_ = 0, nlarge_ = 0, max_np_ = 0, max_n_ = 0, max_rounds_ = 0;
-    DevBuf<double> U_, W_, V_, Tm_, Q_, dw_;
-    DevBuf<int> bact_, bwork_;
+    DevBuf<double> U_, W_, V_, Tm_, G_, M_, Q_, dw_, dz_, lam_, scale_, jtol_, otol_, atol_;
+    DevBuf<unsigned long long> emax_;
+    DevBuf<int> hard_, bact_, bwork_, bref_, bupd_, bjac_, partner_;
+    long oa_sweeps_ = 0, jacobi_blocks_ = 0;
     DevBuf<GemmTile> gtiles_;
     DevBuf<PairTask> pairs_;
     DevBuf<WTileTask> wtiles_;
@@ -526,7 +659,15 @@ class GroupRun {
     int ngtiles_ = 0, npairs_ = 0, nwtiles_ = 0, nvtiles_ = 0;
     bool warm_ = false;
     long sweeps_total_ = 0;
+    // profile mode
+    bool profile_ = false;
+    std::vector<cudaEvent_t> prof_ev_;
+    size_t prof_used_ = 0;
+    double map_sec_ = 0.0, map_bytes_ = 0.0;
+    long map_n_ = 0;
 };
+
+thread_local v2g_batch_stats g_stats{};
 
 int fail(int code, const std::string& msg) {
     g_last_error = msg;
@@ -575,6 +716,8 @@ void v2g_default_options(v2g_options* o) {
     o->mu_update_frequency = 500;
     o->device = 0;
     o->record_trace = 0;
+    o->profile = 0;
+    o->adaptive_projection = 0;
 }
 
 const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
@@ -598,6 +741,7 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         o.cg_maxiter = opt->cg_maxiter;
         o.tau = opt->tau_parameter;
         o.mu_update_frequency = opt->mu_update_frequency;
+        o.adaptive_projection = opt->adaptive_projection != 0;
         if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)
             return v2g::fail(V2G_ERR_ARG, "iteration limits must be positive");
         auto h = std::make_unique<v2g_handle>();
@@ -605,6 +749,7 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         P.opt = o;
         P.device = opt->device;
         P.record_trace = opt->record_trace != 0;
+        P.profile = opt->profile != 0;
         std::vector<int> z(nirrep, 0);
         auto arr = [&](const int* a) { return a ? std::vector<int>(a, a + nirrep) : z; };
         P.sp.frzcpi = arr(frzcpi);
@@ -747,36 +892,101 @@ int v2g_solve_batch(v2g_handle** hs, int count, v2g_result* res) {
     return v2g::guarded([&]() -> int {
         if (!hs || !res || count < 1) return v2g::fail(V2G_ERR_ARG, "bad batch arguments");
         v2g::require_device();
+        const int device = hs[0] ? hs[0]->P.device : 0;
+        CK(cudaSetDevice(device));
+        cudaEvent_t t0, t1, t2, t3;
+        CK(cudaEventCreate(&t0));
+        CK(cudaEventCreate(&t1));
+        CK(cudaEventCreate(&t2));
+        CK(cudaEventCreate(&t3));
+        CK(cudaEventRecord(t0, 0));
         // group handles by layout (shared tables), at most 256 per group
         std::map<v2g::DeviceTables*, std::vector<int>> groups;
         for (int i = 0; i < count; i++) {
             if (!hs[i]) return v2g::fail(V2G_ERR_ARG, "null handle in batch");
             if (!hs[i]->P.have_c) return v2g::fail(V2G_ERR_ARG, "v2g_set_hamiltonian was not called");
+            if (hs[i]->P.device != device) return v2g::fail(V2G_ERR_ARG, "all handles of a batch use one device");
             groups[&hs[i]->P.tables()].push_back(i);
         }
-        int worst = V2G_OK;
+        std::vector<std::unique_ptr<v2g::GroupRun>> runs;
+        std::vector<std::vector<int>> members;
         for (auto& kv : groups) {
             const auto& idx = kv.second;
-            for (size_t s = 0; s < idx.size(); s += 256) {
+            for (size_t s0 = 0; s0 < idx.size(); s0 += 256) {
                 std::vector<Problem*> probs;
                 std::vector<int> which;
-                for (size_t k = s; k < idx.size() && k < s + 256; k++) {
+                for (size_t k = s0; k < idx.size() && k < s0 + 256; k++) {
                     probs.push_back(&hs[idx[k]]->P);
                     which.push_back(idx[k]);
                 }
-                v2g::GroupRun g(*kv.first, probs);
-                std::vector<v2g_result> r;
-                g.solve(r);
-                CK(cudaGetLastError());
-                for (size_t k = 0; k < which.size(); k++) {
-                    res[which[k]] = r[k];
-                    if (r[k].status != V2G_OK && worst == V2G_OK) worst = r[k].status;
-                }
+                runs.push_back(std::make_unique<v2g::GroupRun>(*kv.first, probs));
+                members.push_back(which);
             }
         }
+        CK(cudaDeviceSynchronize());
+        CK(cudaEventRecord(t1, 0));
+        const long launches0 = v2g::g_kernel_launches.load();
+        // every layout group runs its own lock-step loop on its own stream
+        std::vector<std::vector<v2g_result>> out(runs.size());
+        std::vector<std::string> errs(runs.size());
+        std::vector<std::thread> th;
+        for (size_t g = 0; g < runs.size(); g++)
+            th.emplace_back([&, g]() {
+                try {
+                    CK(cudaSetDevice(device));
+                    runs[g]->solve(out[g]);
+                } catch (const std::exception& e) {
+                    errs[g] = e.what();
+                }
+            });
+        for (auto& t : th) t.join();
+        for (auto& e : errs)
+            if (!e.empty()) throw v2g::CudaError(e);
+        CK(cudaDeviceSynchronize());
+        CK(cudaEventRecord(t2, 0));
+        const long launches1 = v2g::g_kernel_launches.load();
+        for (auto& r : runs) r->download_state();
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(t3, 0));
+        CK(cudaEventSynchronize(t3));
+        float ms_dev = 0, ms_e2e = 0;
+        CK(cudaEventElapsedTime(&ms_dev, t1, t2));
+        CK(cudaEventElapsedTime(&ms_e2e, t0, t3));
+        v2g_batch_stats st{};
+        st.device_seconds = ms_dev * 1e-3;
+        st.e2e_seconds = ms_e2e * 1e-3;
+        st.kernel_launches = launches1 - launches0;
+        st.groups = (long)runs.size();
+        for (auto& r : runs) {
+            st.map_seconds += r->map_seconds();
+            st.map_launches += r->map_launches();
+            st.map_bytes += r->map_bytes();
+            st.h2d_bytes += r->h2d_bytes();
+            st.d2h_bytes += r->d2h_bytes();
+            st.refine_sweeps += r->oa_sweeps();
+            st.jacobi_sweeps += r->jacobi_sweeps();
+            st.jacobi_blocks += r->jacobi_blocks();
+        }
+        v2g::g_stats = st;
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        cudaEventDestroy(t2);
+        cudaEventDestroy(t3);
+        int worst = V2G_OK;
+        for (size_t g = 0; g < runs.size(); g++)
+            for (size_t k = 0; k < members[g].size(); k++) {
+                res[members[g][k]] = out[g][k];
+                if (out[g][k].status != V2G_OK && worst == V2G_OK) worst = out[g][k].status;
+            }
         if (worst != V2G_OK) v2g::g_last_error = "at least one instance did not converge";
         return worst;
     });
+}
+
+int v2g_last_batch_stats(v2g_batch_stats* out) {
+    if (!out) return V2G_ERR_ARG;
+    *out = v2g::g_stats;
+    return V2G_OK;
 }
 
 int v2g_solve(v2g_handle* h, v2g_result* res) { return v2g_solve_batch(&h, 1, res); }

@@ -142,7 +142,7 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
 
 constexpr double kJacobiRotEps = 1e-15;
 constexpr int kJacobiSweeps = 20;
-constexpr int kPairSweeps = 3;
+constexpr int kPairSweeps = 1;
 
 __global__ void __launch_bounds__(kJThreads) small_project_kernel(const BlockTask* __restrict__ tasks, int B,
                                                                   const double* __restrict__ aty,
@@ -441,6 +441,55 @@ __global__ void __launch_bounds__(256) bj_update_w_kernel(const BlockTask* __res
     }
 }
 
+// W tiles first (blockIdx.x < nwt), then V tiles: one launch per round.
+__global__ void __launch_bounds__(256) bj_update_wv_kernel(const BlockTask* __restrict__ tasks,
+                                                           const WTileTask* __restrict__ wt, int nwt,
+                                                           const VTileTask* __restrict__ vt, int round,
+                                                           double* Ww, double* Vw, const double* __restrict__ Qbuf,
+                                                           const int* __restrict__ bmask) {
+    extern __shared__ double sm[];
+    double* T = sm;
+    double* Qs = sm + kJ * kLd;
+    if ((int)blockIdx.x < nwt) {
+        const WTileTask w = wt[blockIdx.x];
+        if (bmask && !bmask[w.task]) return;
+        const BlockTask t = tasks[w.task];
+        const int r = round % (t.nb - 1);
+        int I1, J1, I2, J2;
+        rr_pair(t.nb, r, w.k1, I1, J1);
+        rr_pair(t.nb, r, w.k2, I2, J2);
+        double* base = Ww + t.woff;
+        for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
+            const int a = l / 64, bq = l % 64;
+            T[a * kLd + bq] = base[(int64_t)pair_idx(I1, J1, a) * t.np + pair_idx(I2, J2, bq)];
+        }
+        __syncthreads();
+        tile_rotate(T, Qs, Qbuf + t.qoff + (int64_t)w.k1 * 4096, Qbuf + t.qoff + (int64_t)w.k2 * 4096, true);
+        for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
+            const int a = l / 64, bq = l % 64;
+            base[(int64_t)pair_idx(I1, J1, a) * t.np + pair_idx(I2, J2, bq)] = T[a * kLd + bq];
+        }
+        return;
+    }
+    const VTileTask v = vt[blockIdx.x - nwt];
+    if (bmask && !bmask[v.task]) return;
+    const BlockTask t = tasks[v.task];
+    int I, J;
+    rr_pair(t.nb, round % (t.nb - 1), v.k, I, J);
+    double* base = Vw + t.woff;
+    const int r0 = v.chunk * 64;
+    for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
+        const int a = l / 64, bq = l % 64;
+        T[a * kLd + bq] = base[(int64_t)(r0 + a) * t.np + pair_idx(I, J, bq)];
+    }
+    __syncthreads();
+    tile_rotate(T, Qs, nullptr, Qbuf + t.qoff + (int64_t)v.k * 4096, false);
+    for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
+        const int a = l / 64, bq = l % 64;
+        base[(int64_t)(r0 + a) * t.np + pair_idx(I, J, bq)] = T[a * kLd + bq];
+    }
+}
+
 __global__ void __launch_bounds__(256) bj_update_v_kernel(const BlockTask* __restrict__ tasks,
                                                           const VTileTask* __restrict__ vt, int round, double* Vw,
                                                           const double* __restrict__ Qbuf,
@@ -467,21 +516,47 @@ __global__ void __launch_bounds__(256) bj_update_v_kernel(const BlockTask* __res
     }
 }
 
-__global__ void bj_check_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ Ww,
+// Convergence test of the block Jacobi, in two deterministic passes:
+// per padded row the off-diagonal and total squared sums, then per block.
+__global__ void bj_rowsum_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ Ww,
+                                 const int* __restrict__ bmask, double* __restrict__ rowsum) {
+    __shared__ double red[33];
+    const int task = blockIdx.y;
+    if (!bmask[task]) return;
+    const BlockTask t = tasks[task];
+    const int p = blockIdx.x;
+    if (p >= t.np) return;
+    const double* w = Ww + t.woff + (int64_t)p * t.np;
+    double off = 0.0, tot = 0.0;
+    for (int q = threadIdx.x; q < t.np; q += blockDim.x) {
+        const double a = w[q];
+        tot += a * a;
+        if (q != p) off += a * a;
+    }
+    off = block_sum(off, red);
+    tot = block_sum(tot, red);
+    if (threadIdx.x == 0) {
+        rowsum[2 * (t.doff + p)] = off;
+        rowsum[2 * (t.doff + p) + 1] = tot;
+    }
+}
+
+__global__ void bj_check_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ rowsum,
                                 const double* __restrict__ tols, const double* __restrict__ abs_tols,
-                                int* __restrict__ bmask) {
+                                const int* __restrict__ max_sweeps, int sweeps_done, int* __restrict__ bmask) {
     __shared__ double red[33];
     if (!bmask[blockIdx.x]) return;
+    if (max_sweeps && sweeps_done >= max_sweeps[blockIdx.x]) {
+        if (threadIdx.x == 0) bmask[blockIdx.x] = 0;
+        return;
+    }
     const double tol = tols[blockIdx.x];
     const double atol = abs_tols ? abs_tols[blockIdx.x] : 0.0;
     const BlockTask t = tasks[blockIdx.x];
-    const double* w = Ww + t.woff;
     double off = 0.0, tot = 0.0;
-    const int64_t nn = (int64_t)t.np * t.np;
-    for (int64_t i = threadIdx.x; i < nn; i += blockDim.x) {
-        const double a = w[i];
-        tot += a * a;
-        if (i / t.np != i % t.np) off += a * a;
+    for (int p = threadIdx.x; p < t.np; p += blockDim.x) {
+        off += rowsum[2 * (t.doff + p)];
+        tot += rowsum[2 * (t.doff + p) + 1];
     }
     off = block_sum(off, red);
     tot = block_sum(tot, red);
@@ -539,20 +614,30 @@ __global__ void lam_from_diag_kernel(const BlockTask* __restrict__ tasks, const 
 // the error left after the update is of order emax^2.
 
 constexpr double kHard = 0.1;
+constexpr double kFroMax = 0.2;
 
 __global__ void oa_lambda_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ S,
                                  const double* __restrict__ G, const int* __restrict__ bmask,
-                                 double* __restrict__ lam, double* __restrict__ scale) {
+                                 double* __restrict__ lam, double* __restrict__ scale, int* __restrict__ restart) {
     __shared__ double red[33];
+    __shared__ int bad;
     if (bmask && !bmask[blockIdx.x]) return;
     const BlockTask t = tasks[blockIdx.x];
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
     double mx = 0.0;
     for (int i = threadIdx.x; i < t.np; i += blockDim.x) {
         const int64_t d = t.woff + (int64_t)i * t.np + i;
         const double l = (i < t.n) ? S[d] / G[d] : 0.0;
         lam[t.doff + i] = l;
         mx = fmax(mx, fabs(l));
+        // eigenvectors drifted far from orthonormal, or values broke down
+        // (the refinement itself corrects deviations of order ||E||^2; only a
+        // large drift means a step went wrong)
+        if (i < t.n && (!isfinite(l) || !(fabs(G[d] - 1.0) <= 0.25))) bad = 1;
     }
+    __syncthreads();
+    if (threadIdx.x == 0 && bad) restart[blockIdx.x] = 1;
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
     __syncthreads();
@@ -609,7 +694,9 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
                                  const double* __restrict__ G, const double* __restrict__ lam,
                                  const double* __restrict__ scale, const int* __restrict__ partner,
                                  const int* __restrict__ bmask, double* __restrict__ M,
-                                 unsigned long long* __restrict__ emax, int* __restrict__ hard) {
+                                 unsigned long long* __restrict__ emax, int* __restrict__ hard,
+                                 double* __restrict__ erow) {
+    __shared__ double red[33];
     const int task = blockIdx.y;
     if (bmask && !bmask[task]) return;
     const BlockTask t = tasks[task];
@@ -618,7 +705,7 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
     const double negligible = 1e-15 * scale[task];
     const double li = lam[t.doff + i];
     const int pi = (i < t.n) ? partner[t.doff + i] : -1;
-    double emx = 0.0;
+    double emx = 0.0, esq = 0.0;
     int hd = 0;
     // exact rotation of an isolated pair (i, pi)
     double rc = 1.0, rs = 0.0;
@@ -659,10 +746,13 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
                 e = num / gap;
             }
             emx = fmax(emx, fabs(e));
+            esq += e * e;
             m = e;
         }
         M[w] = m;
     }
+    esq = block_sum(esq, red);
+    if (threadIdx.x == 0) erow[t.doff + i] = esq;
     for (int o = 16; o > 0; o >>= 1) {
         emx = fmax(emx, __shfl_down_sync(0xffffffffu, emx, o));
         hd |= __shfl_down_sync(0xffffffffu, hd, o);
@@ -675,6 +765,18 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
 
 // After an analysis: upd = ref & !hard (apply V <- V M), jac |= ref & hard,
 // ref = upd & (emax > tol) (another sweep needed); counts ref into n_ref.
+__global__ void oa_fro_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ erow,
+                              const int* __restrict__ bmask, int* __restrict__ hard) {
+    __shared__ double red[33];
+    if (bmask && !bmask[blockIdx.x]) return;
+    const BlockTask t = tasks[blockIdx.x];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < t.n; i += blockDim.x) s += erow[t.doff + i];
+    s = block_sum(s, red);
+    // a first-order step is only trusted while ||E||_F stays small
+    if (threadIdx.x == 0 && !(s <= kFroMax * kFroMax)) hard[blockIdx.x] = 1;
+}
+
 __global__ void oa_masks_kernel(int ntasks, const unsigned long long* __restrict__ emax,
                                 const int* __restrict__ hard, const double* __restrict__ tols,
                                 const double* __restrict__ abs_tols, const double* __restrict__ scale,
@@ -704,6 +806,25 @@ __global__ void oa_masks_kernel(int ntasks, const unsigned long long* __restrict
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += s[w];
         *n_ref = tot;
     }
+}
+
+// C <- upper triangle of C mirrored to the lower one (tile granularity: the
+// GEMM computed tiles ti <= tj only)
+__global__ void mirror_kernel(const BlockTask* __restrict__ tasks, double* __restrict__ C,
+                              const int* __restrict__ bmask) {
+    if (bmask && !bmask[blockIdx.y]) return;
+    const BlockTask t = tasks[blockIdx.y];
+    const int p = blockIdx.x;
+    if (p >= t.np) return;
+    double* c = C + t.woff;
+    // row p, columns q < 64 * (p / 64): lower tiles
+    const int qend = (p / 64) * 64;
+    for (int q = threadIdx.x; q < qend; q += blockDim.x) c[(int64_t)p * t.np + q] = c[(int64_t)q * t.np + p];
+}
+
+__global__ void uncap_kernel(int n, const int* __restrict__ sel, int* __restrict__ max_sweeps) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (sel[i]) max_sweeps[i] = 1 << 20;
 }
 
 __global__ void merge_mask_kernel(int n, const int* __restrict__ src, int* __restrict__ dst) {
@@ -760,6 +881,7 @@ void set_smem_attrs() {
     cudaFuncSetAttribute(bj_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
     cudaFuncSetAttribute(bj_update_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
     cudaFuncSetAttribute(bj_update_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
+    cudaFuncSetAttribute(bj_update_wv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
     done = true;
 }
 
@@ -810,6 +932,14 @@ void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, in
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
+void launch_bj_update_wv(const BlockTask* tasks, const WTileTask* wt, int nwt, const VTileTask* vt, int nvt, int round,
+                         double* Ww, double* Vw, const double* Qbuf, const int* bmask, cudaStream_t s) {
+    if (nwt + nvt == 0) return;
+    set_smem_attrs();
+    bj_update_wv_kernel<<<nwt + nvt, 256, kJacobiSmem, s>>>(tasks, wt, nwt, vt, round, Ww, Vw, Qbuf, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
 void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, int round, double* Vw,
                         const double* Qbuf, const int* bmask, cudaStream_t s) {
     if (nvt == 0) return;
@@ -818,10 +948,13 @@ void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, in
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-void launch_bj_check(const BlockTask* tasks, int ntasks, const double* Ww, const double* tol, const double* abs_tol,
-                     int* bmask, int* n_open, cudaStream_t s) {
+void launch_bj_check(const BlockTask* tasks, int ntasks, int max_np, const double* Ww, const double* tol,
+                     const double* abs_tol, const int* max_sweeps, int sweeps_done, double* rowsum, int* bmask,
+                     int* n_open, cudaStream_t s) {
     if (ntasks == 0) return;
-    bj_check_kernel<<<ntasks, 256, 0, s>>>(tasks, Ww, tol, abs_tol, bmask);
+    bj_rowsum_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, Ww, bmask, rowsum);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    bj_check_kernel<<<ntasks, 256, 0, s>>>(tasks, rowsum, tol, abs_tol, max_sweeps, sweeps_done, bmask);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     count_open_kernel<<<1, 1024, 0, s>>>(ntasks, bmask, n_open);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
@@ -843,14 +976,16 @@ void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, 
 
 void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
                        const int* bmask, double* lam, double* scale, int* partner, double* M,
-                       unsigned long long* emax, int* hard, cudaStream_t s) {
+                       unsigned long long* emax, int* hard, double* erow, int* restart, cudaStream_t s) {
     if (ntasks == 0) return;
-    oa_lambda_kernel<<<ntasks, 256, 0, s>>>(tasks, S, G, bmask, lam, scale);
+    oa_lambda_kernel<<<ntasks, 256, 0, s>>>(tasks, S, G, bmask, lam, scale, restart);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     oa_pairs_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, bmask, partner, hard);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     oa_update_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, partner, bmask, M, emax,
-                                                           hard);
+                                                           hard, erow);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    oa_fro_kernel<<<ntasks, 256, 0, s>>>(tasks, erow, bmask, hard);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
@@ -866,6 +1001,18 @@ void launch_copy_blocks(const BlockTask* tasks, int ntasks, int max_np, const do
                         const int* bmask, cudaStream_t s) {
     if (ntasks == 0) return;
     copy_blocks_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, src, dst, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_mirror(const BlockTask* tasks, int ntasks, int max_np, double* C, const int* bmask, cudaStream_t s) {
+    if (ntasks == 0) return;
+    mirror_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, C, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_uncap(int n, const int* sel, int* max_sweeps, cudaStream_t s) {
+    if (n == 0) return;
+    uncap_kernel<<<1, 1024, 0, s>>>(n, sel, max_sweeps);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

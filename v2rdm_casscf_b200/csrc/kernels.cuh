@@ -19,7 +19,7 @@ extern std::atomic<long> g_kernel_launches;
 
 struct DevCsr {
     int64_t nrows = 0;
-    const int64_t* rowptr = nullptr;
+    const int32_t* rowptr = nullptr;  // tables stay below 2^31 entries (checked when built)
     const int32_t* col = nullptr;
     const double* val = nullptr;
 };
@@ -120,12 +120,16 @@ void launch_bj_solve(const BlockTask* tasks, const PairTask* pt, int npt, int ro
                      const int* bmask, cudaStream_t s);
 void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, int round, double* Ww,
                         const double* Qbuf, const int* bmask, cudaStream_t s);
+void launch_bj_update_wv(const BlockTask* tasks, const WTileTask* wt, int nwt, const VTileTask* vt, int nvt, int round,
+                         double* Ww, double* Vw, const double* Qbuf, const int* bmask, cudaStream_t s);
 void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, int round, double* Vw,
                         const double* Qbuf, const int* bmask, cudaStream_t s);
 // Per-block off-diagonal and total Frobenius norms of W; sets bmask[t] = 0
-// for blocks whose off-diagonal norm is below max(tol[t] * total, abs_tol[t]).
-void launch_bj_check(const BlockTask* tasks, int ntasks, const double* Ww, const double* tol, const double* abs_tol,
-                     int* bmask, int* n_open, cudaStream_t s);
+// for blocks whose off-diagonal norm is below max(tol[t] * total, abs_tol[t])
+// or that have done max_sweeps[t] sweeps.
+void launch_bj_check(const BlockTask* tasks, int ntasks, int max_np, const double* Ww, const double* tol,
+                     const double* abs_tol, const int* max_sweeps, int sweeps_done, double* rowsum, int* bmask,
+                     int* n_open, cudaStream_t s);
 // dx = max(lam, 0) / mu and dz = max(-lam, 0) (per block, length np; zero on padding)
 void launch_pos_weights(const BlockTask* tasks, int ntasks, const double* lam, const double* mu, const int* bmask,
                         double* dx, double* dz, cudaStream_t s);
@@ -137,15 +141,22 @@ void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, 
 // and hard[t] is set for blocks needing the Jacobi fallback (an index
 // strongly coupled to more than one other; isolated strongly coupled pairs
 // are rotated exactly).  partner needs one int per padded row.
+// Blocks whose eigenvectors lost orthonormality (|g_ii - 1| > 0.25) or whose
+// values broke down get restart[t] = 1; blocks whose first-order step has
+// ||E||_F > 0.2 are marked hard.  erow holds one double per padded row.
 void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
                        const int* bmask, double* lam, double* scale, int* partner, double* M,
-                       unsigned long long* emax, int* hard, cudaStream_t s);
+                       unsigned long long* emax, int* hard, double* erow, int* restart, cudaStream_t s);
 void launch_oa_masks(int ntasks, const unsigned long long* emax, const int* hard, const double* tol,
                      const double* abs_tol, const double* scale, int* ref, int* upd, int* jac, int* n_ref,
                      cudaStream_t s);
 void launch_copy_blocks(const BlockTask* tasks, int ntasks, int max_np, const double* src, double* dst,
                         const int* bmask, cudaStream_t s);
 void launch_count(int n, const int* mask, int* out, cudaStream_t s);
+// symmetric GEMM results: copy the upper tiles onto the lower ones
+void launch_mirror(const BlockTask* tasks, int ntasks, int max_np, double* C, const int* bmask, cudaStream_t s);
+// max_sweeps[i] = unlimited where sel[i]
+void launch_uncap(int n, const int* sel, int* max_sweeps, cudaStream_t s);
 // dst[i] |= src[i]
 void launch_merge_mask(int n, const int* src, int* dst, cudaStream_t s);
 // x = X and z = Z (unpadded, interleaved)

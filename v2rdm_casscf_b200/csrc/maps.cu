@@ -65,7 +65,12 @@ __device__ __forceinline__ void block_partial(double v, int B, double* __restric
 
 // out[r,b] = coef[b] * (sum_k val[k] in[col[k],b] - sub[r]) + add[r,b];
 // with dotv, also partial[., b] of sum_r dotv[r,b] * out[r,b].
-__global__ void spmv_kernel(int64_t nrows, int B, const int64_t* __restrict__ rowptr,
+// A row's (col, val) entries are loaded in batches of kUnroll before the
+// gathers, so the gathers of one row are in flight together instead of
+// waiting on each other; the summation order is still k = k0, k0 + 1, ...
+constexpr int kUnroll = 4;
+
+__global__ void spmv_kernel(int64_t nrows, int B, const int32_t* __restrict__ rowptr,
                             const int32_t* __restrict__ col, const double* __restrict__ val,
                             const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ sub,
                             const double* __restrict__ coef, const double* __restrict__ add,
@@ -78,8 +83,22 @@ __global__ void spmv_kernel(int64_t nrows, int B, const int64_t* __restrict__ ro
         const double cf = coef ? coef[b] : 1.0;
         for (int64_t r = ch.first; r < ch.nrows; r += ch.stride) {
             double s = 0.0;
-            const int64_t k1 = rowptr[r + 1];
-            for (int64_t k = rowptr[r]; k < k1; k++) s += val[k] * in[(int64_t)col[k] * B + b];
+            const int k0 = rowptr[r], k1 = rowptr[r + 1];
+            for (int k = k0; k < k1; k += kUnroll) {
+                int c[kUnroll];
+                double v[kUnroll], g[kUnroll];
+#pragma unroll
+                for (int u = 0; u < kUnroll; u++) {
+                    const bool ok = k + u < k1;
+                    c[u] = ok ? col[k + u] : 0;
+                    v[u] = ok ? val[k + u] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kUnroll; u++) g[u] = (k + u < k1) ? in[(int64_t)c[u] * B + b] : 0.0;
+#pragma unroll
+                for (int u = 0; u < kUnroll; u++)
+                    if (k + u < k1) s += v[u] * g[u];
+            }
             const int64_t t = r * B + b;
             if (sub) s -= sub[r];
             if (coef) s *= cf;

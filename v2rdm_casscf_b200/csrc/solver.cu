@@ -77,7 +77,7 @@ struct DeviceTables {
     Layout L;
     int device = 0;
     Csr hA;  // kept on the host for adjoint checks and the nnz count
-    DevBuf<int64_t> A_rowptr, AT_rowptr;
+    DevBuf<int32_t> A_rowptr, AT_rowptr;
     DevBuf<int32_t> A_col, AT_col;
     DevBuf<double> A_val, AT_val;
     DevBuf<double> b;
@@ -112,11 +112,14 @@ std::shared_ptr<DeviceTables> get_tables(const Layout& L, int device) {
     if (!err.empty()) throw std::invalid_argument(err);
     Csr AT;
     transpose(T->hA, AT);
+    if (T->hA.nnz() >= (int64_t)INT32_MAX) throw std::invalid_argument("constraint table exceeds 2^31 entries");
     CK(cudaSetDevice(device));
-    T->A_rowptr.upload(T->hA.rowptr.data(), T->hA.rowptr.size());
+    std::vector<int32_t> rp32(T->hA.rowptr.begin(), T->hA.rowptr.end());
+    T->A_rowptr.upload(rp32.data(), rp32.size());
     T->A_col.upload(T->hA.col.data(), T->hA.col.size());
     T->A_val.upload(T->hA.val.data(), T->hA.val.size());
-    T->AT_rowptr.upload(AT.rowptr.data(), AT.rowptr.size());
+    rp32.assign(AT.rowptr.begin(), AT.rowptr.end());
+    T->AT_rowptr.upload(rp32.data(), rp32.size());
     T->AT_col.upload(AT.col.data(), AT.col.size());
     T->AT_val.upload(AT.val.data(), AT.val.size());
     build_b(L, T->hb);
@@ -177,9 +180,9 @@ class GroupRun {
         coef_.alloc(B_);
         mask_.alloc(B_);
         cs_.alloc(B_);
-        nact_.alloc(4);
+        nact_.alloc(8);  // counters: CG, Jacobi, refinement, fallback, restart
         CK(cudaMallocHost(&hscal_, sizeof(double) * 4 * B_));
-        CK(cudaMallocHost(&hnact_, sizeof(int) * 4));
+        CK(cudaMallocHost(&hnact_, sizeof(int) * 8));
         build_projection_plan();
         upload_state();
         for (auto* p : P_) profile_ = profile_ || p->profile;
@@ -252,8 +255,10 @@ class GroupRun {
             refine();
         }
         launch_pos_weights(large_d_.p, nlarge_, lam_.p, mu_.p, bact_.p, dw_.p, dz_.p, s_);
-        launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, V_.p, true, dw_.p, Tm_.p, bact_.p, s_);
-        launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, V_.p, true, dz_.p, M_.p, bact_.p, s_);
+        launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, false, V_.p, true, dw_.p, Tm_.p, bact_.p, s_);
+        launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, false, V_.p, true, dz_.p, M_.p, bact_.p, s_);
+        launch_mirror(large_d_.p, nlarge_, max_np_, Tm_.p, bact_.p, s_);
+        launch_mirror(large_d_.p, nlarge_, max_np_, M_.p, bact_.p, s_);
         launch_write_xz(large_d_.p, nlarge_, max_n_, B_, Tm_.p, M_.p, mask_.p, x_.p, z_.p, s_);
         warm_ = true;
     }
@@ -261,18 +266,22 @@ class GroupRun {
     // Ogita-Aishima sweeps from the previous eigenvectors; blocks with a hard
     // pair or without convergence after kMaxOa sweeps go to block Jacobi.
     void refine() {
-        constexpr int kMaxOa = 6;
+        constexpr int kMaxOa = 4;
         CK(cudaMemcpyAsync(bref_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
         CK(cudaMemsetAsync(bjac_.p, 0, nlarge_ * sizeof(int), s_));
+        CK(cudaMemsetAsync(restart_.p, 0, nlarge_ * sizeof(int), s_));
         int nref = 1;
         for (int sweep = 0; sweep < kMaxOa && nref > 0; sweep++) {
+            // S = V^T (U V) and G = V^T V are symmetric: upper tiles, then mirrored
             launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bref_.p, s_);
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bref_.p, s_);
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, V_.p, false, nullptr, G_.p, bref_.p, s_);
+            launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bref_.p, s_);
+            launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, true, V_.p, false, nullptr, G_.p, bref_.p, s_);
+            launch_mirror(large_d_.p, nlarge_, max_np_, W_.p, bref_.p, s_);
+            launch_mirror(large_d_.p, nlarge_, max_np_, G_.p, bref_.p, s_);
             CK(cudaMemsetAsync(emax_.p, 0, nlarge_ * sizeof(unsigned long long), s_));
             CK(cudaMemsetAsync(hard_.p, 0, nlarge_ * sizeof(int), s_));
             launch_oa_analyze(large_d_.p, nlarge_, max_np_, W_.p, G_.p, bref_.p, lam_.p, scale_.p, partner_.p,
-                              M_.p, emax_.p, hard_.p, s_);
+                              M_.p, emax_.p, hard_.p, erow_.p, restart_.p, s_);
             launch_oa_masks(nlarge_, emax_.p, hard_.p, otol_.p, atol_.p, scale_.p, bref_.p, bupd_.p, bjac_.p,
                             nact_.p + 2, s_);
             launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, M_.p, false, nullptr, Tm_.p, bupd_.p, s_);
@@ -287,13 +296,25 @@ class GroupRun {
         launch_count(nlarge_, bjac_.p, nact_.p + 3, s_);
         CK(cudaMemcpyAsync(hnact_ + 3, nact_.p + 3, sizeof(int), cudaMemcpyDeviceToHost, s_));
         CK(cudaStreamSynchronize(s_));
+        // blocks whose eigenvectors degraded restart cold (V = I, W = U) and
+        // converge fully; they leave the refinement and warm Jacobi sets
+        launch_count(nlarge_, restart_.p, nact_.p + 4, s_);
+        CK(cudaMemcpyAsync(hnact_ + 4, nact_.p + 4, sizeof(int), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
         if (hnact_[3] > 0) {
             jacobi_blocks_ += hnact_[3];
             // warm block Jacobi on W = V^T U V with the current V
             launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bjac_.p, s_);
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bjac_.p, s_);
-            block_jacobi(30);
+            launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bjac_.p, s_);
+            launch_mirror(large_d_.p, nlarge_, max_np_, W_.p, bjac_.p, s_);
         }
+        if (hnact_[4] > 0) {
+            restarts_ += hnact_[4];
+            launch_cold_start(large_d_.p, nlarge_, max_np_, U_.p, W_.p, V_.p, restart_.p, s_);
+            launch_merge_mask(nlarge_, restart_.p, bjac_.p, s_);
+            launch_uncap(nlarge_, restart_.p, msw_.p, s_);
+        }
+        if (hnact_[3] > 0 || hnact_[4] > 0) block_jacobi(30);
     }
 
     // Block Jacobi on the blocks flagged in bjac_ until their relative
@@ -301,14 +322,15 @@ class GroupRun {
     void block_jacobi(int max_sweeps) {
         CK(cudaMemcpyAsync(bwork_.p, bjac_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
         for (int sweep = 0; sweep < max_sweeps; sweep++) {
-            launch_bj_check(large_d_.p, nlarge_, W_.p, jtol_.p, atol_.p, bwork_.p, nact_.p + 1, s_);
+            launch_bj_check(large_d_.p, nlarge_, max_np_, W_.p, jtol_.p, atol_.p, cap_ ? msw_.p : nullptr, sweep,
+                            rowsum_.p, bwork_.p, nact_.p + 1, s_);
             CK(cudaMemcpyAsync(hnact_ + 1, nact_.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s_));
             CK(cudaStreamSynchronize(s_));
             if (hnact_[1] == 0) break;
             for (int g = 0; g < max_rounds_; g++) {
                 launch_bj_solve(large_d_.p, pairs_.p, npairs_, g, W_.p, Q_.p, bwork_.p, s_);
-                launch_bj_update_w(large_d_.p, wtiles_.p, nwtiles_, g, W_.p, Q_.p, bwork_.p, s_);
-                launch_bj_update_v(large_d_.p, vtiles_.p, nvtiles_, g, V_.p, Q_.p, bwork_.p, s_);
+                launch_bj_update_wv(large_d_.p, wtiles_.p, nwtiles_, vtiles_.p, nvtiles_, g, W_.p, V_.p, Q_.p,
+                                    bwork_.p, s_);
             }
             sweeps_total_++;
         }
@@ -537,6 +559,18 @@ class GroupRun {
             const int b = hlarge_[t].inst;
             if (!rho.empty() && rho[b] > 0.0) at[t] = rho[b] / std::sqrt((double)nblk[b]);
         }
+        // a fallback block of an instance still far from the solution takes one
+        // warm sweep per outer iteration; the next iteration continues from it
+        std::vector<int> ms(nlarge_, 1 << 20);
+        cap_ = false;
+        for (int t = 0; t < nlarge_; t++) {
+            const int b = hlarge_[t].inst;
+            if (!rho.empty() && rho[b] >= 1e-4) {
+                ms[t] = 1;
+                cap_ = true;
+            }
+        }
+        CK(cudaMemcpyAsync(msw_.p, ms.data(), nlarge_ * sizeof(int), cudaMemcpyHostToDevice, s_));
         CK(cudaMemcpyAsync(jtol_.p, jt.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
         CK(cudaMemcpyAsync(otol_.p, ot.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
         CK(cudaMemcpyAsync(atol_.p, at.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
@@ -596,7 +630,11 @@ class GroupRun {
         jtol_.alloc(nlarge_);
         otol_.alloc(nlarge_);
         atol_.alloc(nlarge_);
+        msw_.alloc(nlarge_);
         lam_.alloc(doff);
+        erow_.alloc(doff);
+        restart_.alloc(nlarge_);
+        rowsum_.alloc(2 * doff);
         partner_.alloc(doff);
         scale_.alloc(nlarge_);
         emax_.alloc(nlarge_);
@@ -606,7 +644,7 @@ class GroupRun {
         bref_.alloc(nlarge_);
         bupd_.alloc(nlarge_);
         bjac_.alloc(nlarge_);
-        std::vector<GemmTile> gt;
+        std::vector<GemmTile> gt, st;
         std::vector<PairTask> pt;
         std::vector<WTileTask> wt;
         std::vector<VTileTask> vt;
@@ -617,7 +655,10 @@ class GroupRun {
             max_n_ = std::max(max_n_, t.n);
             max_rounds_ = std::max(max_rounds_, t.nb - 1);
             for (int i = 0; i < nt; i++)
-                for (int j = 0; j < nt; j++) gt.push_back({ti, i, j});
+                for (int j = 0; j < nt; j++) {
+                    gt.push_back({ti, i, j});
+                    if (i <= j) st.push_back({ti, i, j});
+                }
             for (int k = 0; k < npair; k++) pt.push_back({ti, k});
             for (int k1 = 0; k1 < npair; k1++)
                 for (int k2 = 0; k2 < npair; k2++) wt.push_back({ti, k1, k2});
@@ -625,6 +666,8 @@ class GroupRun {
                 for (int k = 0; k < npair; k++) vt.push_back({ti, ch, k});
         }
         gtiles_.upload(gt.data(), gt.size());
+        stiles_.upload(st.data(), st.size());
+        nstiles_ = (int)st.size();
         pairs_.upload(pt.data(), pt.size());
         wtiles_.upload(wt.data(), wt.size());
         vtiles_.upload(vt.data(), vt.size());
@@ -648,15 +691,17 @@ class GroupRun {
     std::vector<BlockTask> hlarge_;
     DevBuf<BlockTask> small_d_, large_d_;
     int nsmall_ = 0, nlarge_ = 0, max_np_ = 0, max_n_ = 0, max_rounds_ = 0;
-    DevBuf<double> U_, W_, V_, Tm_, G_, M_, Q_, dw_, dz_, lam_, scale_, jtol_, otol_, atol_;
+    DevBuf<double> U_, W_, V_, Tm_, G_, M_, Q_, dw_, dz_, lam_, scale_, jtol_, otol_, atol_, rowsum_, erow_;
     DevBuf<unsigned long long> emax_;
-    DevBuf<int> hard_, bact_, bwork_, bref_, bupd_, bjac_, partner_;
+    DevBuf<int> hard_, bact_, bwork_, bref_, bupd_, bjac_, partner_, msw_, restart_;
+    long restarts_ = 0;
+    bool cap_ = false;
     long oa_sweeps_ = 0, jacobi_blocks_ = 0;
-    DevBuf<GemmTile> gtiles_;
+    DevBuf<GemmTile> gtiles_, stiles_;
     DevBuf<PairTask> pairs_;
     DevBuf<WTileTask> wtiles_;
     DevBuf<VTileTask> vtiles_;
-    int ngtiles_ = 0, npairs_ = 0, nwtiles_ = 0, nvtiles_ = 0;
+    int ngtiles_ = 0, nstiles_ = 0, npairs_ = 0, nwtiles_ = 0, nvtiles_ = 0;
     bool warm_ = false;
     long sweeps_total_ = 0;
     // profile mode

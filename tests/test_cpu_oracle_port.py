@@ -1,0 +1,60 @@
+"""The numpy restatement in oracle/port.py against the reference's own outputs
+(golden fixtures from the compiled reference) and against the product's
+constraint table (CPU only)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import port
+from tests.helpers import GOLDEN, csr_of, load
+
+
+@pytest.mark.parametrize("name", ["c1_n4_dqg", "c1_n6_dqg", "c1_n5_triplet_dqg", "c1_n5_dqg_nosz", "c1_n4_d"])
+def test_port_maps_match_reference(name):
+    g = load(os.path.join(GOLDEN, f"maps_{name}.npz"))
+    docc, socc = g["doccpi"], g["soccpi"]
+    na, nb = int(docc.sum() + socc.sum()), int(docc.sum())
+    L = port.Layout(int(g["amopi"][0]), na, nb, int(socc.sum()) + 1, str(g["positivity"]),
+                    bool(g["constrain_spin"]), bool(g["constrain_sz"]))
+    A = port.build_A(L)
+    assert A.shape == (int(g["ncon"]), int(g["dimx"]))
+    assert L.dims == g["block_dims"].tolist()
+    assert np.abs(A @ g["u"] - g["Au"]).max() <= 1e-13 * np.abs(g["Au"]).max()
+    assert np.abs(A.T @ g["w"] - g["ATw"]).max() <= 1e-13 * np.abs(g["ATw"]).max()
+    assert np.array_equal(port.build_b(L, A.shape[0]), g["b"])
+
+
+def test_port_guess_matches_reference_start():
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    L = port.Layout(4, 2, 2)
+    A = port.build_A(L)
+    x, y, z = port.random_guess(L.dimx, A.shape[0])
+    # the reference's first iteration line starts from this state: check its
+    # primal energy against the trace is not possible without c; check the
+    # guess range and determinism instead
+    x2, y2, z2 = port.random_guess(L.dimx, A.shape[0])
+    assert np.array_equal(x, x2) and x.min() >= -2.0 and x.max() <= 0.0
+
+
+def test_port_solve_matches_reference():
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    a = synthetic(4, int(g["seed"]))
+    L = port.Layout(4, a.na, a.nb)
+    A = port.build_A(L)
+    b = port.build_b(L, A.shape[0])
+    c = port.build_c(L, a.h, a.eri())
+    x, y, z = port.random_guess(L.dimx, A.shape[0])
+    out = port.solve(L, A, b, c, x, y, z, float(g["r_conv"]), float(g["e_conv"]))
+    assert out["converged"]
+    assert abs(out["e_primal"] - float(g["e_primal"])) <= 1e-6
+
+
+def test_port_agrees_with_product_table(v2g):
+    L = port.Layout(5, 3, 2, 2)
+    A = port.build_A(L)
+    s = v2g.V2RDMSolver([5], 3, 2, 2)
+    P = csr_of(s)
+    assert (A - P).count_nonzero() == 0 or abs(A - P).max() <= 1e-15

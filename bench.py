@@ -9,6 +9,12 @@ all solved in one batched call of the C ABI (v2g_solve_batch).  One step = one
 full batched solve.  Inputs are far larger than L2 (the primal/dual vectors of
 the batch take several GB), so no L2 flush is needed between steps.
 
+  step      one complete batched solve, from the reference's start to every
+            instance passing the stopping test (the metric is a time to
+            solution).  Warm-up steps make the same batched call capped at
+            --warmup-outer outer iterations: they run every kernel, table
+            build and allocation of the step without repeating a
+            many-minute solve.
   value     device seconds of the batched solve, inputs resident in HBM
             (CUDA events around the iteration phase, max over ranks)
   e2e       the same solve through the public C ABI from host buffers,
@@ -132,12 +138,16 @@ def run_gpu(args):
     dev = local
     all_spaces = workload(args.workload, args.count)
     mine = list(range(rank, len(all_spaces), world))
-    opts = dict(OPTIONS)
-    if args.max_outer:
-        opts["MAXITER"] = args.max_outer
-    solvers = [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
-                                               projection=args.projection)
-               for i in mine]
+    def make(maxiter):
+        opts = dict(OPTIONS)
+        if maxiter:
+            opts["MAXITER"] = maxiter
+        return [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
+                                                projection=args.projection, cg_tolerance_factor=args.cg_factor)
+                for i in mine]
+
+    solvers = make(args.max_outer)
+    warm_solvers = make(args.warmup_outer) if args.warmup else []
     # the random start of the reference depends only on the layout: compute once per size
     starts = {}
     for s in solvers:
@@ -145,19 +155,20 @@ def run_gpu(args):
         if key not in starts:
             s.guess()
             starts[key] = s.get_state()
-    def reset():
-        for s in solvers:
+    def reset(group):
+        for s in group:
             x, y, z, mu = starts[(s.dimx, s.nconstraints)]
             s.set_state(x, y, z, mu)
 
-    def step():
-        reset()
-        res = V.solve_batch(solvers)
+    def step(group=None):
+        group = solvers if group is None else group
+        reset(group)
+        res = V.solve_batch(group)
         st = V.last_batch_stats()
         return res, st
 
     for _ in range(args.warmup):
-        step()
+        step(warm_solvers)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -195,8 +206,12 @@ def run_gpu(args):
         oiters = {}
         for i, r in zip(mine, results):
             oiters.setdefault(int(all_spaces[i].n), []).append(int(r["oiter"]))
+    # Roofline of the dominant kernel, timed alone: inside the solve every
+    # layout group runs on its own stream, so per-kernel events there also
+    # cover other groups' kernels.  The largest group's maps are applied to
+    # interleaved vectors of its own size on one stream, CUDA events around them.
     pk, pk_kind = peaks()
-    achieved = (map_b / map_s / 1e9) if map_s > 0 else None
+    achieved, map_detail = roofline_pass(V, solvers, all_spaces, mine, dev, torch)
     out = {
         "metric": METRIC,
         "value": value,
@@ -216,6 +231,10 @@ def run_gpu(args):
             "instances": args.count,
             "precision": "FP64 (maps, CG, projection)",
             "projection": args.projection,
+            "cg_tolerance_factor": args.cg_factor,
+            "mode": "plain FP64 (reference algorithm)" if (args.projection == "exact" and args.cg_factor == 0.01)
+                    else "FP64 with adaptive projection and CG tolerance",
+            "warmup_steps": f"{args.warmup} batched calls capped at {args.warmup_outer} outer iterations",
             "l2": "inputs larger than L2 (no flush needed)",
             "parallelism": f"instances dealt to {world} rank(s), no exchange",
             "max_outer": args.max_outer or None,
@@ -223,8 +242,10 @@ def run_gpu(args):
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {
-            "kernel": "spmv_kernel (A / A^T gather inside CG)",
+            "kernel": "ell_kernel + long_kernel (A and A^T gathers of the CG), largest layout group, timed alone",
             "bound": "hbm",
+            "detail": map_detail,
+            "in_solve_event_timing_gbs": (map_b / map_s / 1e9) if map_s > 0 else None,
             "achieved": achieved,
             "peak": pk,
             "peak_kind": pk_kind,
@@ -253,6 +274,44 @@ def run_gpu(args):
                        "outer_iterations": [int(r["oiter"]) for r in results],
                        "n": [int(a.n) for a in all_spaces]}, open(ITER_FILE, "w"))
         print(json.dumps(out))
+
+
+def roofline_pass(V, solvers, spaces, mine, dev, torch, reps=20):
+    """Algorithmic GB/s of A and A^T for the largest group (bytes 8*(rows+cols) per vector)."""
+    by_n = {}
+    for k, i in enumerate(mine):
+        by_n.setdefault(spaces[i].n, []).append(solvers[k])
+    n = max(by_n)
+    grp = by_n[n]
+    B = len(grp)
+    s = grp[0]
+    nx, nc = s.dimx, s.nconstraints
+    g = torch.Generator(device=f"cuda:{dev}").manual_seed(0)
+    x = torch.randn(nx * B, dtype=torch.float64, device=f"cuda:{dev}", generator=g)
+    y = torch.randn(nc * B, dtype=torch.float64, device=f"cuda:{dev}", generator=g)
+    ox = torch.empty_like(x)
+    oy = torch.empty_like(y)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    total_b, total_t = 0.0, 0.0
+    for name, tr, src, dst in (("A", False, x, oy), ("AT", True, y, ox)):
+        for _ in range(3):
+            s.map_batched_device(B, src.data_ptr(), dst.data_ptr(), stream.cuda_stream, transpose=tr)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(reps):
+            s.map_batched_device(B, src.data_ptr(), dst.data_ptr(), stream.cuda_stream, transpose=tr)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        nbytes = 8.0 * (nx + nc) * B
+        out[name] = {"us_per_launch": t * 1e6, "GBps": nbytes / t / 1e9}
+        total_b += nbytes
+        total_t += t
+    out["group"] = f"n={n}, {B} instances interleaved"
+    out["bytes_per_launch"] = 8.0 * (nx + nc) * B
+    return total_b / total_t / 1e9, out
 
 
 def ref_time_per_iteration(space, iters, threads):
@@ -352,11 +411,17 @@ def main():
     ap.add_argument("--count", type=int, default=256)
     ap.add_argument("--max-outer", type=int, default=0, help="cap outer iterations (experiments only)")
     ap.add_argument("--projection", default="adaptive", choices=["exact", "adaptive"])
+    ap.add_argument("--cg-factor", type=float, default=0.1,
+                    help="CG tolerance factor (0.01 = the reference's rule)")
+    ap.add_argument("--plain", action="store_true", help="reference algorithm: exact projection, CG factor 0.01")
+    ap.add_argument("--warmup-outer", type=int, default=3, help="outer iterations per warm-up step")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-sample", type=lambda s: [int(v) for v in s.split(",")], default=[8, 12, 16, 20])
     ap.add_argument("--no-clocks", dest="clocks", action="store_false")
     ap.add_argument("--save-iterations", action="store_true")
     args = ap.parse_args()
+    if args.plain:
+        args.projection, args.cg_factor = "exact", 0.01
     if args.impl == "reference":
         run_reference(args)
     else:

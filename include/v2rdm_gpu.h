@@ -64,6 +64,10 @@ typedef struct v2g_options {
                                    residual is below 0.01 min(eps(p), eps(d)), the CG tolerance
                                    rule (x, z stay PSD); 0: every projection converged, as the
                                    plugin (0) */
+    double cg_tolerance_factor; /* CG stops at factor * min(eps(p), eps(d)) after the first outer
+                                   iteration; 0.01 is the plugin's rule (v2rdm_solver.cc:1797-1805),
+                                   and values up to 0.1 trade fewer CG iterations for a few more
+                                   outer ones (0.01) */
 } v2g_options;
 
 typedef struct v2g_result {
@@ -119,6 +123,12 @@ int v2g_apply_A(v2g_handle* h, const double* u, double* out);
 int v2g_apply_AT(v2g_handle* h, const double* u, double* out);
 int v2g_apply_A_device(v2g_handle* h, const double* d_u, double* d_out);
 int v2g_apply_AT_device(v2g_handle* h, const double* d_u, double* d_out);
+
+/* The maps applied to nvec vectors at once, stored instance-interleaved on
+ * the device (element e of vector v at [e * nvec + v], 1 <= nvec <= 256), on
+ * the given CUDA stream (NULL: the legacy default stream).  Asynchronous. */
+int v2g_apply_A_batched_device(v2g_handle* h, int nvec, const double* d_u, double* d_out, void* stream);
+int v2g_apply_AT_batched_device(v2g_handle* h, int nvec, const double* d_u, double* d_out, void* stream);
 
 /* One projection step on the handle's state, as Update_xz: with
  * U = A^T y - c + mu x per block, x = U+/mu and z = -U-. */

@@ -39,10 +39,11 @@ MAP_CASES = {
 }
 
 SOLVE_CASES = {
-    # name: (n, seed, r_conv, e_conv)
-    "synthetic_n4_s0": (4, 0, 1e-6, 1e-7),
-    "synthetic_n4_s1": (4, 1, 1e-6, 1e-7),
-    "synthetic_n5_s2": (5, 2, 1e-6, 1e-7),
+    # name: (n, seed, r_conv, e_conv, electrons)
+    "synthetic_n4_s0": (4, 0, 1e-6, 1e-7, None),
+    "synthetic_n4_s1": (4, 1, 1e-6, 1e-7, None),
+    "synthetic_n5_s2": (5, 2, 1e-6, 1e-7, None),      # singlet, N = 4
+    "synthetic_n5_s2_doublet": (5, 2, 1e-6, 1e-7, 5),  # doublet, N = 5
 }
 
 
@@ -94,8 +95,8 @@ def xz():
 
 
 def solve(name, spec):
-    n, seed, rc, ec = spec
-    a = synthetic(n, seed)
+    n, seed, rc, ec, electrons = spec
+    a = synthetic(n, seed, electrons=electrons)
     r = RefSolver([n], [a.nb], soccpi=[a.na - a.nb], multiplicity=a.multiplicity, positivity="DQG",
                   r_convergence=rc, e_convergence=ec)
     r.set_integrals(a.oei_packed, a.qmo, a.nq)
@@ -103,6 +104,7 @@ def solve(name, spec):
     r.build_constraints()
     out = r.solve(trace_cap=100000)
     np.savez_compressed(os.path.join(HERE, f"solve_{name}.npz"), n=n, seed=seed, r_conv=rc, e_conv=ec,
+                        electrons=a.na + a.nb,
                         e_primal=out["e_primal"], e_dual=out["e_dual"], ep=out["ep"], ed=out["ed"],
                         oiter=out["oiter"], iiter=out["iiter"], converged=out["converged"], trace=out["trace"],
                         x=r.get("x"), y=r.get("y"), z=r.get("z"))

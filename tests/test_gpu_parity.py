@@ -58,14 +58,14 @@ def _solve_golden(v2g, name):
     from v2rdm_casscf_b200.hamiltonian import synthetic
 
     g = load(os.path.join(GOLDEN, f"solve_{name}.npz"))
-    a = synthetic(int(g["n"]), int(g["seed"]))
+    a = synthetic(int(g["n"]), int(g["seed"]), electrons=int(g["electrons"]))
     s = v2g.V2RDMSolver.from_active_space(
         a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])), record_trace=True)
     s.guess()
     return g, s
 
 
-@pytest.mark.parametrize("name", ["synthetic_n4_s0", "synthetic_n4_s1", "synthetic_n5_s2"])
+@pytest.mark.parametrize("name", ["synthetic_n4_s0", "synthetic_n4_s1", "synthetic_n5_s2", "synthetic_n5_s2_doublet"])
 def test_solve_matches_reference(v2g, name):
     # Converged energies agree; individual iterations do not have to, since CG
     # on A A^T from the random start amplifies rounding (a sparse vs dense
@@ -108,7 +108,7 @@ def test_batch_equals_individual_solves(v2g):
 def test_solve_matches_oracle_fresh_seed(v2g, ref):
     from v2rdm_casscf_b200.hamiltonian import synthetic
 
-    a2 = synthetic(5, 11)  # doublet (5e,5o)
+    a2 = synthetic(5, 11, electrons=5)  # doublet (5e,5o)
     opts = dict(R_CONVERGENCE=1e-6, E_CONVERGENCE=1e-7)
     r = ref.RefSolver([5], [2], soccpi=[1], multiplicity=2, positivity="DQG", r_convergence=1e-6,
                       e_convergence=1e-7)
@@ -123,14 +123,14 @@ def test_solve_matches_oracle_fresh_seed(v2g, ref):
     assert abs(e - out["e_primal"]) <= 1e-6
 
 
-@pytest.mark.parametrize("name", ["synthetic_n4_s1", "synthetic_n5_s2"])
+@pytest.mark.parametrize("name", ["synthetic_n4_s1", "synthetic_n5_s2", "synthetic_n5_s2_doublet"])
 def test_adaptive_projection_reaches_the_same_energy(v2g, name):
     # loose eigendecompositions far from the solution, exact ones near it:
     # same converged energy as the reference within the parity tolerance
     from v2rdm_casscf_b200.hamiltonian import synthetic
 
     g = load(os.path.join(GOLDEN, f"solve_{name}.npz"))
-    a = synthetic(int(g["n"]), int(g["seed"]))
+    a = synthetic(int(g["n"]), int(g["seed"]), electrons=int(g["electrons"]))
     s = v2g.V2RDMSolver.from_active_space(
         a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])), projection="adaptive")
     s.guess()
@@ -154,3 +154,18 @@ def test_adaptive_projection_with_large_blocks(v2g):
     e2 = s2.compute_energy()
     assert s1.result["status"] == 0 and s2.result["status"] == 0
     assert abs(e1 - e2) <= 1e-6
+
+
+def test_cg_tolerance_factor_reaches_the_same_energy(v2g):
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n5_s2.npz"))
+    a = synthetic(int(g["n"]), int(g["seed"]), electrons=int(g["electrons"]))
+    s = v2g.V2RDMSolver.from_active_space(
+        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])), projection="adaptive",
+        cg_tolerance_factor=0.1)
+    s.guess()
+    e = s.compute_energy()
+    assert s.result["status"] == 0
+    assert abs(e - float(g["e_primal"])) <= 1e-6
+    assert s.result["iiter"] < int(g["iiter"])

@@ -33,7 +33,7 @@ EXPORTS = [
     "v2g_nblocks", "v2g_block_dims", "v2g_set_hamiltonian", "v2g_get_c", "v2g_get_b", "v2g_efzc",
     "v2g_guess_random", "v2g_set_state", "v2g_get_state", "v2g_apply_A", "v2g_apply_AT", "v2g_apply_A_device",
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
-    "v2g_trace", "v2g_last_batch_stats",
+    "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
 ]
 
 
@@ -53,6 +53,7 @@ class Options(ctypes.Structure):
         ("record_trace", ctypes.c_int),
         ("profile", ctypes.c_int),
         ("adaptive_projection", ctypes.c_int),
+        ("cg_tolerance_factor", ctypes.c_double),
     ]
 
 
@@ -140,6 +141,8 @@ def lib():
         L.v2g_trace.restype = L_
         L.v2g_trace.argtypes = [P, DP, L_]
         L.v2g_last_batch_stats.argtypes = [ctypes.POINTER(BatchStats)]
+        for f in ("v2g_apply_A_batched_device", "v2g_apply_AT_batched_device"):
+            getattr(L, f).argtypes = [P, I, P, P, P]
         _lib = L
     return _lib
 
@@ -187,12 +190,13 @@ class V2RDMSolver:
     option names.  ``projection="adaptive"`` lets Update_xz accept an
     eigendecomposition whose residual is below 0.01 min(eps(p), eps(d)) (the
     CG tolerance rule); the default "exact" converges every projection, as
-    the plugin does.
+    the plugin does.  ``cg_tolerance_factor`` replaces the 0.01 of the CG
+    tolerance rule 0.01 min(eps(p), eps(d)).
     """
 
     def __init__(self, active, nalpha, nbeta, multiplicity=1, frozen_docc=None, restricted_docc=None,
                  restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False,
-                 profile=False, projection="exact"):
+                 profile=False, projection="exact", cg_tolerance_factor=0.01):
         L = lib()
         opts = dict(DEFAULT_OPTIONS)
         for k, v in (options or {}).items():
@@ -220,6 +224,7 @@ class V2RDMSolver:
         if projection not in ("exact", "adaptive"):
             raise ValueError("projection is 'exact' or 'adaptive'")
         o.adaptive_projection = int(projection == "adaptive")
+        o.cg_tolerance_factor = float(cg_tolerance_factor)
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)
@@ -318,6 +323,12 @@ class V2RDMSolver:
         val = np.zeros(nnz)
         _check(L.v2g_export_A(self.h, rowptr.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), _ip(col), _dp(val)))
         return rowptr, col, val
+
+    def map_batched_device(self, nvec, d_in, d_out, stream=None, transpose=False):
+        """A (or A^T) on nvec instance-interleaved device vectors (raw pointers)."""
+        f = lib().v2g_apply_AT_batched_device if transpose else lib().v2g_apply_A_batched_device
+        _check(f(self.h, int(nvec), ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                 ctypes.c_void_p(stream) if stream else None))
 
     def update_xz(self, mu):
         _check(lib().v2g_update_xz(self.h, float(mu)))

@@ -648,23 +648,23 @@ __global__ void oa_lambda_kernel(const BlockTask* __restrict__ tasks, const doub
     }
 }
 
-// One pass per row: partner[i] = the single j that is strongly coupled to i
-// (|num| > kHard |gap|, not negligible), -1 for none, -2 for several.
+// One pass per row: partner[i] = the j most strongly coupled to i among the
+// pairs the first-order step cannot handle (|num| > kHard |gap|, not
+// negligible), ranked by |num| / |gap| with ties to the smaller j; -1 if none.
+// Mutual partners form a matching that the update rotates exactly.
 __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ S,
                                 const double* __restrict__ G, const double* __restrict__ lam,
                                 const double* __restrict__ scale, const int* __restrict__ bmask,
                                 int* __restrict__ partner, int* __restrict__ hard) {
-    __shared__ int cnt, who;
+    __shared__ double sr[256];
+    __shared__ int sj[256];
     const int task = blockIdx.y;
     if (bmask && !bmask[task]) return;
     const BlockTask t = tasks[task];
     const int i = blockIdx.x;
     if (i >= t.np) return;
-    if (threadIdx.x == 0) {
-        cnt = 0;
-        who = -1;
-    }
-    __syncthreads();
+    double best = -1.0;
+    int bj = -1;
     if (i < t.n) {
         const double negligible = 1e-15 * scale[task];
         const double li = lam[t.doff + i];
@@ -672,19 +672,32 @@ __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const doubl
             if (j == i) continue;
             const int64_t w = t.woff + (int64_t)i * t.np + j;
             const double lj = lam[t.doff + j];
-            const double num = S[w] - lj * G[w];
-            if (fabs(num) > negligible && !(fabs(num) <= kHard * fabs(lj - li))) {
-                atomicAdd(&cnt, 1);
-                who = j;
+            const double num = fabs(S[w] - lj * G[w]);
+            const double gap = fabs(lj - li);
+            if (num > negligible && !(num <= kHard * gap)) {
+                const double ratio = gap > 0.0 ? num / gap : DBL_MAX;
+                if (ratio > best) {
+                    best = ratio;
+                    bj = j;
+                }
             }
         }
     }
+    sr[threadIdx.x] = best;
+    sj[threadIdx.x] = bj;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const int pj = cnt == 0 ? -1 : (cnt == 1 ? who : -2);
-        partner[t.doff + i] = pj;
-        if (pj == -2) atomicOr(hard + task, 1);
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            const double r2 = sr[threadIdx.x + w];
+            const int j2 = sj[threadIdx.x + w];
+            if (r2 > sr[threadIdx.x] || (r2 == sr[threadIdx.x] && j2 >= 0 && (sj[threadIdx.x] < 0 || j2 < sj[threadIdx.x]))) {
+                sr[threadIdx.x] = r2;
+                sj[threadIdx.x] = j2;
+            }
+        }
+        __syncthreads();
     }
+    if (threadIdx.x == 0) partner[t.doff + i] = sj[0];
 }
 
 // M = I + E.  Isolated strongly coupled pairs (partner of each other) get
@@ -706,9 +719,11 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
     const double li = lam[t.doff + i];
     const int pi = (i < t.n) ? partner[t.doff + i] : -1;
     double emx = 0.0, esq = 0.0;
-    int hd = 0;
-    // exact rotation of an isolated pair (i, pi)
-    double rc = 1.0, rs = 0.0;
+    int hd = 0;  // hard flags now come from oa_fro_kernel only
+    // exact rotation of a mutual pair (i, pi); a row whose strongest partner
+    // is taken waits for a later sweep (its hard pairs get E = 0 now)
+    double rc = 1.0, rs = 0.0, pend = 0.0;
+    bool rot = false, pending = false;
     if (pi >= 0 && partner[t.doff + pi] == i) {
         const int p = i < pi ? i : pi, q = i < pi ? pi : i;
         const double app = lam[t.doff + p], aqq = lam[t.doff + q];
@@ -718,9 +733,12 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
         const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
         rc = 1.0 / sqrt(1.0 + tt * tt);
         rs = tt * rc;
+        rot = true;
         emx = fabs(rs);
     } else if (pi >= 0) {
-        hd = 1;  // one-sided strong coupling: not an isolated pair
+        pending = true;
+        const int64_t w = t.woff + (int64_t)i * t.np + pi;
+        pend = fabs(S[w] - lam[t.doff + pi] * G[w]);
     }
     for (int j = threadIdx.x; j < t.np; j += blockDim.x) {
         const int64_t w = t.woff + (int64_t)i * t.np + j;
@@ -728,8 +746,8 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
         if (i >= t.n || j >= t.n) {
             m = (i == j) ? 1.0 : 0.0;
         } else if (i == j) {
-            m = (pi >= 0) ? rc : 1.0 + 0.5 * (1.0 - G[w]);
-        } else if (j == pi) {
+            m = rot ? rc : 1.0 + 0.5 * (1.0 - G[w]);
+        } else if (rot && j == pi) {
             // J_pp = c, J_pq = s, J_qp = -s, J_qq = c with p < q
             m = (i < j) ? rs : -rs;
         } else {
@@ -740,8 +758,9 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
             if (fabs(num) <= negligible) {
                 e = -0.5 * G[w];
             } else if (!(fabs(num) <= kHard * fabs(gap))) {
-                hd = 1;  // cannot happen for a consistent partner table
-                e = 0.0;
+                e = 0.0;  // strongly coupled: rotated in this or a later sweep
+                pending = true;
+                pend = fmax(pend, fabs(num));
             } else {
                 e = num / gap;
             }
@@ -753,6 +772,10 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
     }
     esq = block_sum(esq, red);
     if (threadIdx.x == 0) erow[t.doff + i] = esq;
+    // a pair left for a later sweep leaves a residual of its coupling; expressed
+    // on the emax scale (residual ~ emax^2 scale) so the block's tolerance
+    // decides whether another sweep is needed
+    if (pending) emx = fmax(emx, scale[task] > 0.0 ? sqrt(pend / scale[task]) : 1.0);
     for (int o = 16; o > 0; o >>= 1) {
         emx = fmax(emx, __shfl_down_sync(0xffffffffu, emx, o));
         hd |= __shfl_down_sync(0xffffffffu, hd, o);

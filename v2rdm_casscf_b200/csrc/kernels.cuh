@@ -17,20 +17,36 @@ namespace v2g {
 // Number of kernels the launchers below have issued (all threads, all devices).
 extern std::atomic<long> g_kernel_launches;
 
-struct DevCsr {
-    int64_t nrows = 0;
-    const int32_t* rowptr = nullptr;  // tables stay below 2^31 entries (checked when built)
-    const int32_t* col = nullptr;
-    const double* val = nullptr;
+// A sparse map (A or A^T) in bucketed ELL form: rows are grouped by length
+// into buckets of fixed width (1, 2, 4, 8, 16, 32 slots, padding marked by
+// col = -1), stored slot-major so that a warp reads its table entries
+// coalesced and needs no row-pointer lookup; rows longer than 32 entries
+// (traces, contractions) are kept as CSR and reduced by a whole CTA each.
+constexpr int kMaxBuckets = 6;
+struct DevMap {
+    int64_t nrows = 0;  // output length
+    int nb = 0;
+    int width[kMaxBuckets] = {};
+    int64_t nslots[kMaxBuckets] = {};
+    int64_t row_off[kMaxBuckets] = {};  // into rows
+    int64_t ent_off[kMaxBuckets] = {};  // into cols / vals
+    const int32_t* rows = nullptr;
+    const int32_t* cols = nullptr;
+    const double* vals = nullptr;
+    int nlong = 0;
+    const int32_t* long_rows = nullptr;
+    const int32_t* long_ptr = nullptr;
+    const int32_t* long_col = nullptr;
+    const double* long_val = nullptr;
 };
 
 // out[r,b] = coef[b] * (sum_k val[k] in[col[k],b] - sub[r]) + add[r,b]
 // (each of sub, coef, add optional); instances with mask[b] == 0 are skipped.
-void launch_spmv(const DevCsr& A, int B, const double* in, double* out, const double* sub, const double* coef,
+void launch_spmv(const DevMap& A, int B, const double* in, double* out, const double* sub, const double* coef,
                  const double* add, const int* mask, cudaStream_t s);
 
 // out = A in, and dot_out[b] = sum_r dotv[r,b] out[r,b] (deterministic).
-void launch_spmv_dot(const DevCsr& A, int B, const double* in, double* out, const double* dotv, const int* mask,
+void launch_spmv_dot(const DevMap& A, int B, const double* in, double* out, const double* dotv, const int* mask,
                      double* partial, double* dot_out, cudaStream_t s);
 
 // Per-instance reductions over interleaved vectors of n elements.

@@ -39,6 +39,9 @@ struct Options {
     // 0.01 min(eps_p, eps_d) (the CG tolerance rule); off = every projection
     // converged, as the reference's Update_xz.
     bool adaptive_projection = false;
+    // CG tolerance = cg_tol_factor * min(eps_p, eps_d) after the first
+    // iteration (0.01 in the reference, v2rdm_solver.cc:1797-1805).
+    double cg_tol_factor = 0.01;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for

@@ -63,51 +63,103 @@ __device__ __forceinline__ void block_partial(double v, int B, double* __restric
     }
 }
 
-// out[r,b] = coef[b] * (sum_k val[k] in[col[k],b] - sub[r]) + add[r,b];
-// with dotv, also partial[., b] of sum_r dotv[r,b] * out[r,b].
-// A row's (col, val) entries are loaded in batches of kUnroll before the
-// gathers, so the gathers of one row are in flight together instead of
-// waiting on each other; the summation order is still k = k0, k0 + 1, ...
-constexpr int kUnroll = 4;
+// Per-row epilogue shared by the map kernels.
+struct Epi {
+    const double* sub;
+    const double* coef;
+    const double* add;
+    const double* dotv;
+    double* out;
+};
+__device__ __forceinline__ double epilogue(const Epi& e, int64_t r, int B, int b, double s) {
+    const int64_t t = r * B + b;
+    if (e.sub) s -= e.sub[r];
+    if (e.coef) s *= e.coef[b];
+    if (e.add) s += e.add[t];
+    e.out[t] = s;
+    return e.dotv ? e.dotv[t] * s : 0.0;
+}
 
-__global__ void spmv_kernel(int64_t nrows, int B, const int32_t* __restrict__ rowptr,
-                            const int32_t* __restrict__ col, const double* __restrict__ val,
-                            const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ sub,
-                            const double* __restrict__ coef, const double* __restrict__ add,
-                            const int* __restrict__ mask, const double* __restrict__ dotv,
-                            double* __restrict__ partial) {
-    const Chunk ch = chunk_of(nrows, B);
+// Bucketed-ELL part.  Blocks [blk[i], blk[i+1]) serve bucket i; inside a
+// bucket the slots are dealt like rows in chunk_of (fixed instance per thread).
+template <int W>
+__device__ __forceinline__ double ell_rows(const DevMap& M, int bi, int64_t first_blk, int64_t nblk, int B,
+                                           const double* __restrict__ in, const Epi& e, int b, int rsub, int rpp) {
+    const int64_t ns = M.nslots[bi];
+    const int32_t* rows = M.rows + M.row_off[bi];
+    const int32_t* cols = M.cols + M.ent_off[bi];
+    const double* vals = M.vals + M.ent_off[bi];
     double acc = 0.0;
-    if (ch.live && !(mask && !mask[ch.b])) {
-        const int b = ch.b;
-        const double cf = coef ? coef[b] : 1.0;
-        for (int64_t r = ch.first; r < ch.nrows; r += ch.stride) {
-            double s = 0.0;
-            const int k0 = rowptr[r], k1 = rowptr[r + 1];
-            for (int k = k0; k < k1; k += kUnroll) {
-                int c[kUnroll];
-                double v[kUnroll], g[kUnroll];
+    for (int64_t i = (blockIdx.x - first_blk) * rpp + rsub; i < ns; i += nblk * rpp) {
+        int c[W];
+        double v[W];
 #pragma unroll
-                for (int u = 0; u < kUnroll; u++) {
-                    const bool ok = k + u < k1;
-                    c[u] = ok ? col[k + u] : 0;
-                    v[u] = ok ? val[k + u] : 0.0;
-                }
+        for (int k = 0; k < W; k++) {
+            c[k] = cols[k * ns + i];
+            v[k] = vals[k * ns + i];
+        }
+        double g[W];
 #pragma unroll
-                for (int u = 0; u < kUnroll; u++) g[u] = (k + u < k1) ? in[(int64_t)c[u] * B + b] : 0.0;
+        for (int k = 0; k < W; k++) g[k] = (c[k] >= 0) ? in[(int64_t)c[k] * B + b] : 0.0;
+        double s = 0.0;
 #pragma unroll
-                for (int u = 0; u < kUnroll; u++)
-                    if (k + u < k1) s += v[u] * g[u];
-            }
-            const int64_t t = r * B + b;
-            if (sub) s -= sub[r];
-            if (coef) s *= cf;
-            if (add) s += add[t];
-            out[t] = s;
-            if (dotv) acc += dotv[t] * s;
+        for (int k = 0; k < W; k++)
+            if (c[k] >= 0) s += v[k] * g[k];
+        acc += epilogue(e, rows[i], B, b, s);
+    }
+    return acc;
+}
+
+struct Blocks {
+    int start[kMaxBuckets + 1];
+};
+
+__global__ void ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in, Epi e,
+                           const int* __restrict__ mask, double* __restrict__ partial) {
+    int bi = 0;
+    while (bi + 1 < M.nb && (int)blockIdx.x >= bl.start[bi + 1]) bi++;
+    const int rpp = blockDim.x / B;
+    const int b = threadIdx.x % B;
+    const int rsub = threadIdx.x / B;
+    const bool live = threadIdx.x < rpp * B && !(mask && !mask[b]);
+    double acc = 0.0;
+    if (live) {
+        const int64_t f = bl.start[bi], nblk = bl.start[bi + 1] - bl.start[bi];
+        switch (M.width[bi]) {
+            case 1: acc = ell_rows<1>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
+            case 2: acc = ell_rows<2>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
+            case 4: acc = ell_rows<4>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
+            case 8: acc = ell_rows<8>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
+            case 16: acc = ell_rows<16>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
+            default: acc = ell_rows<32>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
         }
     }
     if (partial) block_partial(acc, B, partial);
+}
+
+// Long rows: one CTA per row; thread t sums entries k = t / B, t / B + T / B,
+// ... for instance t % B, then a fixed-order reduction per instance.
+__global__ void long_kernel(DevMap M, int B, const double* __restrict__ in, Epi e, const int* __restrict__ mask,
+                            double* __restrict__ partial, int partial_base) {
+    __shared__ double sh[kThreads];
+    const int lanes = blockDim.x / B;
+    const int b = threadIdx.x % B;
+    const int l = threadIdx.x / B;
+    const int r = M.long_rows[blockIdx.x];
+    const int k0 = M.long_ptr[blockIdx.x], k1 = M.long_ptr[blockIdx.x + 1];
+    double s = 0.0;
+    if (threadIdx.x < lanes * B)
+        for (int k = k0 + l; k < k1; k += lanes) s += M.long_val[k] * in[(int64_t)M.long_col[k] * B + b];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    double acc = 0.0;
+    if (threadIdx.x < B) {
+        double t = 0.0;
+        for (int q = 0; q < lanes; q++) t += sh[threadIdx.x + q * B];
+        if (!(mask && !mask[threadIdx.x])) acc = epilogue(e, r, B, threadIdx.x, t);
+    }
+    __syncthreads();
+    if (partial) block_partial(threadIdx.x < B ? acc : 0.0, B, partial + (int64_t)partial_base * B);
 }
 
 // Stage 1: block g reduces a contiguous chunk of elements for every instance;
@@ -287,20 +339,49 @@ static int spmv_grid(int64_t nrows, int B) {
     return (int)(g < 1 ? 1 : g);
 }
 
-void launch_spmv(const DevCsr& A, int B, const double* in, double* out, const double* sub, const double* coef,
+// Blocks per ELL bucket, proportional to its slots, at most kSpmvBlocks in all.
+static Blocks map_blocks(const DevMap& M, int B) {
+    Blocks bl{};
+    const int64_t rpp = kThreads / B;
+    int64_t tot = 0;
+    for (int i = 0; i < M.nb; i++) tot += (M.nslots[i] + rpp - 1) / rpp;
+    const double scale = tot > kSpmvBlocks ? (double)kSpmvBlocks / (double)tot : 1.0;
+    int acc = 0;
+    for (int i = 0; i < M.nb; i++) {
+        bl.start[i] = acc;
+        int64_t g = (int64_t)(((M.nslots[i] + rpp - 1) / rpp) * scale);
+        if (g < 1) g = 1;
+        acc += (int)g;
+    }
+    bl.start[M.nb] = acc;
+    return bl;
+}
+
+static int run_map(const DevMap& M, int B, const double* in, double* out, const double* sub, const double* coef,
+                   const double* add, const int* mask, const double* dotv, double* partial, cudaStream_t s) {
+    Epi e{sub, coef, add, dotv, out};
+    const Blocks bl = map_blocks(M, B);
+    if (M.nb > 0) {
+        ell_kernel<<<bl.start[M.nb], kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+        g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    }
+    if (M.nlong > 0) {
+        long_kernel<<<M.nlong, kThreads, 0, s>>>(M, B, in, e, mask, partial, bl.start[M.nb]);
+        g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    }
+    return bl.start[M.nb] + M.nlong;  // partial blocks written
+}
+
+void launch_spmv(const DevMap& A, int B, const double* in, double* out, const double* sub, const double* coef,
                  const double* add, const int* mask, cudaStream_t s) {
-    spmv_kernel<<<spmv_grid(A.nrows, B), kThreads, 0, s>>>(A.nrows, B, A.rowptr, A.col, A.val, in, out, sub, coef,
-                                                           add, mask, nullptr, nullptr);
+    run_map(A, B, in, out, sub, coef, add, mask, nullptr, nullptr, s);
 }
 
 int64_t reduce_partial_size(int B) { return (int64_t)kSpmvBlocks * B; }
 
-void launch_spmv_dot(const DevCsr& A, int B, const double* in, double* out, const double* dotv, const int* mask,
+void launch_spmv_dot(const DevMap& A, int B, const double* in, double* out, const double* dotv, const int* mask,
                      double* partial, double* dot_out, cudaStream_t s) {
-    const int g = spmv_grid(A.nrows, B);
-    spmv_kernel<<<g, kThreads, 0, s>>>(A.nrows, B, A.rowptr, A.col, A.val, in, out, nullptr, nullptr, nullptr,
-                                       mask, dotv, partial);
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    const int g = run_map(A, B, in, out, nullptr, nullptr, nullptr, mask, dotv, partial, s);
     reduce_stage2<<<B, kThreads, 0, s>>>(g, B, partial, dot_out);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }

@@ -72,18 +72,87 @@ struct DevBuf {
     }
 };
 
+// One map (A or A^T) on the device in the bucketed-ELL form of kernels.cuh.
+struct MapTable {
+    DevBuf<int32_t> rows, cols, long_rows, long_ptr, long_col;
+    DevBuf<double> vals, long_val;
+    DevMap dm;
+
+    void build(const Csr& M) {
+        static const int widths[kMaxBuckets] = {1, 2, 4, 8, 16, 32};
+        std::vector<std::vector<int32_t>> brow(kMaxBuckets);
+        std::vector<int32_t> lrows, lptr(1, 0), lcol;
+        std::vector<double> lval;
+        for (int64_t r = 0; r < M.nrows; r++) {
+            const int64_t len = M.rowptr[r + 1] - M.rowptr[r];
+            int w = 0;
+            while (w < kMaxBuckets && widths[w] < len) w++;
+            if (w < kMaxBuckets) {
+                brow[w].push_back((int32_t)r);
+            } else {
+                lrows.push_back((int32_t)r);
+                for (int64_t k = M.rowptr[r]; k < M.rowptr[r + 1]; k++) {
+                    lcol.push_back(M.col[k]);
+                    lval.push_back(M.val[k]);
+                }
+                lptr.push_back((int32_t)lcol.size());
+            }
+        }
+        std::vector<int32_t> hrows, hcols;
+        std::vector<double> hvals;
+        dm = DevMap{};
+        dm.nrows = M.nrows;
+        for (int w = 0; w < kMaxBuckets; w++) {
+            if (brow[w].empty()) continue;
+            const int W = widths[w];
+            const int64_t ns = (int64_t)brow[w].size();
+            const int bi = dm.nb++;
+            dm.width[bi] = W;
+            dm.nslots[bi] = ns;
+            dm.row_off[bi] = (int64_t)hrows.size();
+            dm.ent_off[bi] = (int64_t)hcols.size();
+            hrows.insert(hrows.end(), brow[w].begin(), brow[w].end());
+            const size_t base = hcols.size();
+            hcols.resize(base + (size_t)W * ns, -1);
+            hvals.resize(base + (size_t)W * ns, 0.0);
+            for (int64_t i = 0; i < ns; i++) {
+                const int64_t r = brow[w][i];
+                int k = 0;
+                for (int64_t e = M.rowptr[r]; e < M.rowptr[r + 1]; e++, k++) {
+                    hcols[base + (size_t)k * ns + i] = M.col[e];
+                    hvals[base + (size_t)k * ns + i] = M.val[e];
+                }
+            }
+        }
+        rows.upload(hrows.data(), hrows.size());
+        cols.upload(hcols.data(), hcols.size());
+        vals.upload(hvals.data(), hvals.size());
+        long_rows.upload(lrows.data(), lrows.size());
+        long_ptr.upload(lptr.data(), lptr.size());
+        long_col.upload(lcol.data(), lcol.size());
+        long_val.upload(lval.data(), lval.size());
+        dm.rows = rows.p;
+        dm.cols = cols.p;
+        dm.vals = vals.p;
+        dm.nlong = (int)lrows.size();
+        dm.long_rows = long_rows.p;
+        dm.long_ptr = long_ptr.p;
+        dm.long_col = long_col.p;
+        dm.long_val = long_val.p;
+    }
+};
+
 // Index tables and b for one layout, shared by every instance with it.
 struct DeviceTables {
     Layout L;
     int device = 0;
-    Csr hA;  // kept on the host for adjoint checks and the nnz count
-    DevBuf<int32_t> A_rowptr, AT_rowptr;
-    DevBuf<int32_t> A_col, AT_col;
-    DevBuf<double> A_val, AT_val;
+    Csr hA;  // kept on the host for v2g_export_A
+    MapTable mA, mAT;
     DevBuf<double> b;
     std::vector<double> hb;
-    DevCsr A() const { return DevCsr{L.ncon, A_rowptr.p, A_col.p, A_val.p}; }
-    DevCsr AT() const { return DevCsr{L.dimx, AT_rowptr.p, AT_col.p, AT_val.p}; }
+    const DevMap& A() const { return mA.dm; }
+    const DevMap& AT() const { return mAT.dm; }
+    int max_long() const { return std::max(mA.dm.nlong, mAT.dm.nlong); }
 };
 
 std::string layout_key(const Layout& L, int device) {
@@ -114,14 +183,8 @@ std::shared_ptr<DeviceTables> get_tables(const Layout& L, int device) {
     transpose(T->hA, AT);
     if (T->hA.nnz() >= (int64_t)INT32_MAX) throw std::invalid_argument("constraint table exceeds 2^31 entries");
     CK(cudaSetDevice(device));
-    std::vector<int32_t> rp32(T->hA.rowptr.begin(), T->hA.rowptr.end());
-    T->A_rowptr.upload(rp32.data(), rp32.size());
-    T->A_col.upload(T->hA.col.data(), T->hA.col.size());
-    T->A_val.upload(T->hA.val.data(), T->hA.val.size());
-    rp32.assign(AT.rowptr.begin(), AT.rowptr.end());
-    T->AT_rowptr.upload(rp32.data(), rp32.size());
-    T->AT_col.upload(AT.col.data(), AT.col.size());
-    T->AT_val.upload(AT.val.data(), AT.val.size());
+    T->mA.build(T->hA);
+    T->mAT.build(AT);
     build_b(L, T->hb);
     T->b.upload(T->hb.data(), T->hb.size());
     g_cache[key] = T;
@@ -174,7 +237,7 @@ class GroupRun {
         r_.alloc(C);
         p_.alloc(C);
         ap_.alloc(C);
-        partial_.alloc(reduce_partial_size(B_));
+        partial_.alloc(reduce_partial_size(B_) + (int64_t)(T.max_long() + 8) * B_);
         red_.alloc(4 * B_);
         mu_.alloc(B_);
         coef_.alloc(B_);
@@ -266,7 +329,7 @@ class GroupRun {
     // Ogita-Aishima sweeps from the previous eigenvectors; blocks with a hard
     // pair or without convergence after kMaxOa sweeps go to block Jacobi.
     void refine() {
-        constexpr int kMaxOa = 4;
+        constexpr int kMaxOa = 6;
         CK(cudaMemcpyAsync(bref_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
         CK(cudaMemsetAsync(bjac_.p, 0, nlarge_ * sizeof(int), s_));
         CK(cudaMemsetAsync(restart_.p, 0, nlarge_ * sizeof(int), s_));
@@ -392,7 +455,7 @@ class GroupRun {
                 if (oiter[b] == 0)
                     tol = 0.01;
                 else
-                    tol = (ep[b] > ed[b]) ? 0.01 * ed[b] : 0.01 * ep[b];
+                    tol = (ep[b] > ed[b]) ? o.cg_tol_factor * ed[b] : o.cg_tol_factor * ep[b];
                 if (tol < o.cg_convergence) tol = o.cg_convergence;
                 cs[b] = CgScalars{};
                 cs[b].tol = tol;
@@ -493,7 +556,7 @@ class GroupRun {
   private:
     // CG map launch with optional CUDA-event timing (profile mode).
     // With dotv, also red_[b] = sum dotv[., b] * out[., b].
-    void map_launch(const DevCsr& M, const double* in, double* out, const double* dotv = nullptr,
+    void map_launch(const DevMap& M, const double* in, double* out, const double* dotv = nullptr,
                     const int* mask = nullptr) {
         auto go = [&]() {
             if (dotv)
@@ -763,6 +826,7 @@ void v2g_default_options(v2g_options* o) {
     o->record_trace = 0;
     o->profile = 0;
     o->adaptive_projection = 0;
+    o->cg_tolerance_factor = 0.01;
 }
 
 const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
@@ -787,6 +851,9 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         o.tau = opt->tau_parameter;
         o.mu_update_frequency = opt->mu_update_frequency;
         o.adaptive_projection = opt->adaptive_projection != 0;
+        o.cg_tol_factor = opt->cg_tolerance_factor;
+        if (!(o.cg_tol_factor > 0.0 && o.cg_tol_factor < 1.0))
+            return v2g::fail(V2G_ERR_ARG, "cg_tolerance_factor must be in (0, 1)");
         if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)
             return v2g::fail(V2G_ERR_ARG, "iteration limits must be positive");
         auto h = std::make_unique<v2g_handle>();
@@ -897,7 +964,7 @@ static int apply_map(v2g_handle* h, const double* u, double* out, bool transpose
         v2g::DeviceTables& T = P.tables();
         CK(cudaSetDevice(T.device));
         const int64_t nin = transpose ? P.L.ncon : P.L.dimx, nout = transpose ? P.L.dimx : P.L.ncon;
-        v2g::DevCsr M = transpose ? T.AT() : T.A();
+        const v2g::DevMap& M = transpose ? T.AT() : T.A();
         if (device_ptrs) {
             v2g::launch_spmv(M, 1, u, out, nullptr, nullptr, nullptr, nullptr, 0);
             CK(cudaGetLastError());
@@ -917,6 +984,26 @@ int v2g_apply_A(v2g_handle* h, const double* u, double* out) { return apply_map(
 int v2g_apply_AT(v2g_handle* h, const double* u, double* out) { return apply_map(h, u, out, true, false); }
 int v2g_apply_A_device(v2g_handle* h, const double* u, double* out) { return apply_map(h, u, out, false, true); }
 int v2g_apply_AT_device(v2g_handle* h, const double* u, double* out) { return apply_map(h, u, out, true, true); }
+
+static int apply_batched(v2g_handle* h, int nvec, const double* u, double* out, void* stream, bool transpose) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !u || !out || nvec < 1 || nvec > 256) return v2g::fail(V2G_ERR_ARG, "bad batched map arguments");
+        v2g::require_device();
+        v2g::DeviceTables& T = h->P.tables();
+        CK(cudaSetDevice(T.device));
+        v2g::launch_spmv(transpose ? T.AT() : T.A(), nvec, u, out, nullptr, nullptr, nullptr, nullptr,
+                         (cudaStream_t)stream);
+        CK(cudaGetLastError());
+        return V2G_OK;
+    });
+}
+
+int v2g_apply_A_batched_device(v2g_handle* h, int nvec, const double* u, double* out, void* stream) {
+    return apply_batched(h, nvec, u, out, stream, false);
+}
+int v2g_apply_AT_batched_device(v2g_handle* h, int nvec, const double* u, double* out, void* stream) {
+    return apply_batched(h, nvec, u, out, stream, true);
+}
 
 int v2g_update_xz(v2g_handle* h, double mu) {
     return v2g::guarded([&]() -> int {

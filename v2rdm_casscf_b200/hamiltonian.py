@@ -6,7 +6,8 @@ integrals ``Qmo[Q * ntri + INDEX(p, q)]`` with ``ntri = nmo (nmo + 1) / 2``
 (tei.cc:321).  This module builds such inputs for the workloads the solver is
 measured on:
 
-* ``synthetic(n, seed)``: the seeded active space of the batched workload.
+* ``synthetic(n, seed)``: the seeded active space of the batched workload
+  (singlet; N = n electrons, N = n - 1 for odd n).
   h is symmetric with diagonal ~ U(-2.0, -0.5) Eh and off-diagonal
   ~ N(0, 0.1^2); g_pqrs = sum_Q L^Q_pq L^Q_rs with 3n symmetric Cholesky
   vectors whose entries are ~ N(0, 0.25^2), so the ERI tensor is PSD with
@@ -77,8 +78,13 @@ class ActiveSpace:
         return self.na - self.nb + 1
 
 
-def synthetic(n, seed, nq=None):
-    """Seeded synthetic singlet active space (n orbitals, n electrons)."""
+def synthetic(n, seed, nq=None, electrons=None):
+    """Seeded synthetic singlet active space of n orbitals.
+
+    The batched workload asks for N = n electrons in a singlet; an odd n cannot
+    hold a singlet with n electrons, so odd n get N = n - 1 (still a singlet,
+    half filling rounded down).  ``electrons`` overrides N (high-spin for odd N).
+    """
     nq = 3 * n if nq is None else nq
     rng_h = np.random.Generator(np.random.Philox(key=[seed, 0]))
     rng_l = np.random.Generator(np.random.Philox(key=[seed, 1]))
@@ -89,7 +95,8 @@ def synthetic(n, seed, nq=None):
     L = rng_l.normal(0.0, 0.25, size=(nq, n, n))
     L = np.tril(L)
     L = L + np.transpose(np.tril(L, -1), (0, 2, 1))
-    return ActiveSpace(h, L, n - n // 2, n // 2, 0.0, name=f"synthetic(n={n},seed={seed})")
+    N = (n - n % 2) if electrons is None else int(electrons)
+    return ActiveSpace(h, L, N - N // 2, N // 2, 0.0, name=f"synthetic(n={n},seed={seed},N={N})")
 
 
 def batch_sizes(count=256, nmin=8, nmax=20, seed=2024):

@@ -134,6 +134,22 @@ int v2g_apply_AT_batched_device(v2g_handle* h, int nvec, const double* d_u, doub
  * U = A^T y - c + mu x per block, x = U+/mu and z = -U-. */
 int v2g_update_xz(v2g_handle* h, double mu);
 
+/* The projection step of v2g_update_xz on caller-owned device vectors,
+ * allocating no device memory.  No counterpart in the reference: it is for
+ * host programs that cannot call cudaMalloc while they run (a pool allocator
+ * that owns all device memory, a fixed device-memory budget).  Inputs c and y
+ * and the in/out x (dimx, dimx and nconstraints doubles, device memory);
+ * output z (dimx).  Limits: every block of dimension <= 64 and dimx <= 65536,
+ * else V2G_ERR_ARG; the handle's device tables must exist (v2g_update_xz, a
+ * map call or a solve builds them).  Scratch is a static device array of
+ * about 0.5 MiB that every GPU loading the library holds until exit; the
+ * first call on a device looks up its address, so make that call before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU
+ * (other streams or host threads) race.  Asynchronous on the given stream
+ * (NULL: the legacy default stream). */
+int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const double* d_y, double* d_x, double* d_z,
+                          void* stream);
+
 /* The full BPSDP solve from the handle's current state. */
 int v2g_solve(v2g_handle* h, v2g_result* res);
 

@@ -1,0 +1,57 @@
+"""The allocation-free projection entry point (v2g_update_xz_noalloc) against
+v2g_update_xz, through the C ABI, on consecutive calls that share its static
+scratch.  Same tolerance as the projection tests: 1e-10 relative."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _expected(s, x, y, z, mu):
+    s.set_state(x, y, z, mu)
+    s.update_xz(mu)  # existing entry point; also puts the maps on the device
+    x1, _, z1, _ = s.get_state()
+    return x1, z1
+
+
+def test_noalloc_projection_matches_update_xz(v2g):
+    import torch
+
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    dev = torch.device("cuda:0")
+    # two calls on one layout, then a larger layout: the scratch keeps the
+    # previous call's contents, which must not leak into the next result
+    cases = [(4, 3, 0.7), (4, 5, 1.3), (5, 4, 0.9)]
+    solvers = {}
+    for n, seed, mu in cases:
+        if n not in solvers:
+            solvers[n] = v2g.V2RDMSolver.from_active_space(synthetic(n, seed))
+        s = solvers[n]
+        rng = np.random.default_rng(seed)
+        x = rng.uniform(-2.0, 0.0, s.dimx)
+        y = rng.uniform(-2.0, 0.0, s.nconstraints)
+        z = rng.uniform(-2.0, 0.0, s.dimx)
+        x_ref, z_ref = _expected(s, x, y, z, mu)
+
+        d_c = torch.from_numpy(s.c).to(dev)
+        d_y = torch.from_numpy(y).to(dev)
+        d_x = torch.from_numpy(x).to(dev)
+        d_z = torch.full((s.dimx,), float("nan"), dtype=torch.float64, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        s.update_xz_noalloc(mu, d_c.data_ptr(), d_y.data_ptr(), d_x.data_ptr(), d_z.data_ptr(),
+                            stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        x_out, z_out = d_x.cpu().numpy(), d_z.cpu().numpy()
+        scale = max(np.abs(x_ref).max(), np.abs(z_ref).max())
+        assert np.isfinite(x_out).all() and np.isfinite(z_out).all()
+        assert np.abs(x_out - x_ref).max() <= 1e-10 * scale
+        assert np.abs(z_out - z_ref).max() <= 1e-10 * scale
+
+
+def test_noalloc_rejects_large_blocks(v2g):
+    s = v2g.V2RDMSolver([6], 3, 3)  # G2aa block of 72
+    rng = np.random.default_rng(0)
+    s.ATu(rng.standard_normal(s.nconstraints))  # builds the device tables
+    with pytest.raises(v2g.V2GError, match="exceeds the maximum of 64"):
+        s.update_xz_noalloc(1.0, 1, 1, 1, 1)

@@ -34,6 +34,7 @@ EXPORTS = [
     "v2g_guess_random", "v2g_set_state", "v2g_get_state", "v2g_apply_A", "v2g_apply_AT", "v2g_apply_A_device",
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
+    "v2g_update_xz_noalloc",
 ]
 
 
@@ -135,6 +136,7 @@ def lib():
         for f in ("v2g_apply_A_device", "v2g_apply_AT_device"):
             getattr(L, f).argtypes = [P, P, P]
         L.v2g_update_xz.argtypes = [P, D]
+        L.v2g_update_xz_noalloc.argtypes = [P, D, P, P, P, P, P]
         L.v2g_solve.argtypes = [P, ctypes.POINTER(Result)]
         L.v2g_solve_batch.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(Result)]
         L.v2g_export_A.argtypes = [P, LP, IP, DP]
@@ -332,6 +334,13 @@ class V2RDMSolver:
 
     def update_xz(self, mu):
         _check(lib().v2g_update_xz(self.h, float(mu)))
+
+    def update_xz_noalloc(self, mu, d_c, d_y, d_x, d_z, stream=None):
+        """Update_xz on caller-owned device vectors (raw pointers), allocating no
+        device memory; for callers that cannot allocate (blocks <= 64 only)."""
+        _check(lib().v2g_update_xz_noalloc(self.h, float(mu), ctypes.c_void_p(d_c), ctypes.c_void_p(d_y),
+                                           ctypes.c_void_p(d_x), ctypes.c_void_p(d_z),
+                                           ctypes.c_void_p(stream) if stream else None))
 
     # -- solve ------------------------------------------------------------------
     def compute_energy(self):

@@ -1143,6 +1143,104 @@ int v2g_export_A(v2g_handle* h, long* rowptr, int* col, double* val) {
     });
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Projection step that allocates no device memory.
+//
+// Some host programs cannot call cudaMalloc while they run: codes that hand
+// all device memory to their own pool allocator at start-up and forbid other
+// allocations, programs that run under a fixed device-memory budget, and
+// callers that must not take the implicit device synchronisation a
+// cudaMalloc/cudaFree can cause.  v2g_update_xz_noalloc serves them for
+// layouts whose blocks all take the shared-memory eigensolver (dimension
+// <= 64).  Its scratch, the A^T y intermediate, the block task list and mu,
+// lives in the file-scope array below: every GPU that loads this library
+// holds it until the process exits, and every call shares it.
+namespace {
+
+constexpr int kNoAllocMaxTasks = 256;          // blocks per call
+constexpr int64_t kNoAllocMaxDimx = 65536;     // primal length per call
+constexpr size_t kNoAllocMuBytes = 256;
+constexpr size_t kNoAllocTaskBytes = (kNoAllocMaxTasks * sizeof(v2g::BlockTask) + 255) / 256 * 256;
+constexpr size_t kNoAllocBytes = kNoAllocMuBytes + kNoAllocTaskBytes + kNoAllocMaxDimx * sizeof(double);
+constexpr int kNoAllocMaxDevices = 64;
+
+// In host code this name only stands for the symbol; its device address
+// comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the first call on a device does this set-up).
+unsigned char* noalloc_scratch(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) throw std::invalid_argument("device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) throw v2g::CudaError(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_addr[device] = p;
+    }
+    return static_cast<unsigned char*>(g_noalloc_addr[device]);
+}
+
+}  // namespace
+
+extern "C" {
+
+int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const double* d_y, double* d_x, double* d_z,
+                          void* stream) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !(mu > 0.0) || !d_c || !d_y || !d_x || !d_z) return v2g::fail(V2G_ERR_ARG, "bad argument");
+        v2g::require_device();
+        Problem& P = h->P;
+        if (!P.T)
+            return v2g::fail(V2G_ERR_ARG,
+                             "v2g_update_xz_noalloc: the handle's constraint tables are not on the device yet "
+                             "(v2g_update_xz, a map call or a solve builds them)");
+        v2g::DeviceTables& T = *P.T;
+        const v2g::Layout& L = T.L;
+        if (L.dimx > kNoAllocMaxDimx)
+            return v2g::fail(V2G_ERR_ARG, "v2g_update_xz_noalloc: dimx " + std::to_string(L.dimx) +
+                                              " exceeds the maximum of " + std::to_string(kNoAllocMaxDimx));
+        v2g::BlockTask tasks[kNoAllocMaxTasks];
+        int nt = 0;
+        for (size_t k = 0; k < L.block_dims.size(); k++) {
+            const int n = L.block_dims[k];
+            if (n == 0) continue;
+            if (n > 64)
+                return v2g::fail(V2G_ERR_ARG, "v2g_update_xz_noalloc: block of dimension " + std::to_string(n) +
+                                                  " exceeds the maximum of 64 (use v2g_update_xz)");
+            if (nt == kNoAllocMaxTasks)
+                return v2g::fail(V2G_ERR_ARG, "v2g_update_xz_noalloc: more than " +
+                                                  std::to_string(kNoAllocMaxTasks) + " blocks");
+            v2g::BlockTask t{};
+            t.xoff = L.block_off[k];
+            t.n = n;
+            t.inst = 0;
+            tasks[nt++] = t;
+        }
+        CK(cudaSetDevice(T.device));
+        unsigned char* base = noalloc_scratch(T.device);
+        double* s_mu = reinterpret_cast<double*>(base);
+        v2g::BlockTask* s_tasks = reinterpret_cast<v2g::BlockTask*>(base + kNoAllocMuBytes);
+        double* s_aty = reinterpret_cast<double*>(base + kNoAllocMuBytes + kNoAllocTaskBytes);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        // mu and the task list are rewritten by every call; A^T y is cleared
+        // first, so nothing of an earlier call's contents is read.
+        CK(cudaMemcpyAsync(s_mu, &mu, sizeof(double), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(s_tasks, tasks, nt * sizeof(v2g::BlockTask), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(s_aty, 0, L.dimx * sizeof(double), s));
+        v2g::launch_spmv(T.AT(), 1, d_y, s_aty, nullptr, nullptr, nullptr, nullptr, s);
+        v2g::launch_small_project(s_tasks, nt, 1, s_aty, d_c, d_x, d_z, s_mu, nullptr, s);
+        CK(cudaGetLastError());
+        return V2G_OK;
+    });
+}
+
 long v2g_trace(const v2g_handle* h, double* rows, long cap) {
     if (!h) return -1;
     const auto& t = h->P.trace;

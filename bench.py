@@ -3,7 +3,7 @@
 boundary-point SDP solve of a batch of active spaces on B200.
 
 Workload (default "batch256"): 256 seeded synthetic active spaces, n ~ U{8..20}
-orbitals with N = n electrons (singlet for even n, doublet for odd n), C1, DQG
+orbitals, singlets with N = n electrons (N = n - 1 for odd n), C1, DQG
 with CONSTRAIN_SPIN, each started from the reference's random guess (srand(0)),
 all solved in one batched call of the C ABI (v2g_solve_batch).  One step = one
 full batched solve.  Inputs are far larger than L2 (the primal/dual vectors of
@@ -226,7 +226,7 @@ def run_gpu(args):
         "dtype": "f64",
         "data": "synthetic (seeded Philox active spaces; no public dataset involved)",
         "config": {
-            "workload": f"{args.workload}: {args.count} synthetic active spaces n~U{{8..20}}, N=n, C1, DQG, "
+            "workload": f"{args.workload}: {args.count} synthetic active spaces n~U{{8..20}}, singlet N=n (n-1 for odd n), C1, DQG, "
                         "CONSTRAIN_SPIN, E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6, random start (srand(0))",
             "instances": args.count,
             "precision": "FP64 (maps, CG, projection)",

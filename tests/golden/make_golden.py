@@ -36,14 +36,19 @@ MAP_CASES = {
     "c1_n5_dqg_nosz": ([5], [2], [1], "DQG", True, False),
     "c2v_dqg": ([2, 1, 1, 2], [1, 0, 0, 1], [0, 0, 0, 0], "DQG", True, True),
     "c1_n4_d": ([4], [2], [0], "D", True, True),
+    "c1_n4_dqgt1": ([4], [2], [0], "DQGT1", True, True),
+    "c1_n4_dqgt2": ([4], [2], [0], "DQGT2", True, True),
+    "c2_n4_doublet_dqgt": ([2, 2], [1, 0], [1, 0], "DQGT1T2", True, True),
 }
 
 SOLVE_CASES = {
-    # name: (n, seed, r_conv, e_conv, electrons)
+    # name: (n, seed, r_conv, e_conv, electrons[, positivity])
     "synthetic_n4_s0": (4, 0, 1e-6, 1e-7, None),
     "synthetic_n4_s1": (4, 1, 1e-6, 1e-7, None),
     "synthetic_n5_s2": (5, 2, 1e-6, 1e-7, None),      # singlet, N = 4
     "synthetic_n5_s2_doublet": (5, 2, 1e-6, 1e-7, 5),  # doublet, N = 5
+    "synthetic_n4_s0_dqgt2": (4, 0, 1e-6, 1e-7, None, "DQGT2"),
+    "synthetic_n4_s1_dqgt1": (4, 1, 1e-6, 1e-7, None, "DQGT1"),
 }
 
 
@@ -95,16 +100,17 @@ def xz():
 
 
 def solve(name, spec):
-    n, seed, rc, ec, electrons = spec
+    n, seed, rc, ec, electrons = spec[:5]
+    pos = spec[5] if len(spec) > 5 else "DQG"
     a = synthetic(n, seed, electrons=electrons)
-    r = RefSolver([n], [a.nb], soccpi=[a.na - a.nb], multiplicity=a.multiplicity, positivity="DQG",
+    r = RefSolver([n], [a.nb], soccpi=[a.na - a.nb], multiplicity=a.multiplicity, positivity=pos,
                   r_convergence=rc, e_convergence=ec)
     r.set_integrals(a.oei_packed, a.qmo, a.nq)
     r.guess()
     r.build_constraints()
     out = r.solve(trace_cap=100000)
     np.savez_compressed(os.path.join(HERE, f"solve_{name}.npz"), n=n, seed=seed, r_conv=rc, e_conv=ec,
-                        electrons=a.na + a.nb,
+                        electrons=a.na + a.nb, positivity=pos,
                         e_primal=out["e_primal"], e_dual=out["e_dual"], ep=out["ep"], ed=out["ed"],
                         oiter=out["oiter"], iiter=out["iiter"], converged=out["converged"], trace=out["trace"],
                         x=r.get("x"), y=r.get("y"), z=r.get("z"))

@@ -69,6 +69,7 @@ def test_oracle_reproduces_golden(ref):
 
 @pytest.mark.parametrize("spec", [
     ([7], 3, 3, 1, "DQG"), ([6], 3, 2, 2, "DQG"), ([3, 3], 3, 3, 1, "DQG"), ([2, 2, 2, 1], 3, 3, 1, "DQ"),
+    ([4], 2, 2, 1, "DQGT1"), ([5], 3, 2, 2, "DQGT1T2"), ([3, 2], 3, 2, 2, "DQGT2"), ([2, 2, 1, 1], 3, 3, 1, "DQGT"),
 ])
 def test_constraint_table_matches_oracle(v2g, ref, spec):
     amopi, na, nb, mult, pos = spec

@@ -59,13 +59,16 @@ def _solve_golden(v2g, name):
 
     g = load(os.path.join(GOLDEN, f"solve_{name}.npz"))
     a = synthetic(int(g["n"]), int(g["seed"]), electrons=int(g["electrons"]))
+    pos = str(g["positivity"]) if "positivity" in g else "DQG"
     s = v2g.V2RDMSolver.from_active_space(
-        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])), record_trace=True)
+        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]), POSITIVITY=pos),
+        record_trace=True)
     s.guess()
     return g, s
 
 
-@pytest.mark.parametrize("name", ["synthetic_n4_s0", "synthetic_n4_s1", "synthetic_n5_s2", "synthetic_n5_s2_doublet"])
+@pytest.mark.parametrize("name", ["synthetic_n4_s0", "synthetic_n4_s1", "synthetic_n5_s2", "synthetic_n5_s2_doublet",
+                                  "synthetic_n4_s1_dqgt1"])
 def test_solve_matches_reference(v2g, name):
     # Converged energies agree; individual iterations do not have to, since CG
     # on A A^T from the random start amplifies rounding (a sparse vs dense

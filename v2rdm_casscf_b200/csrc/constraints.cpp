@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <stdexcept>
 
 namespace v2g {
 
@@ -367,6 +368,200 @@ void rows_g2(const Layout& L, RowSink& S) {
     }
 }
 
+// Element (r, c) of a geminal-indexed family in irrep h; throws when an
+// index does not exist, which would mean a wrong restatement.
+struct Gem {
+    const Layout& L;
+    int64_t at(Fam f, int h, int64_t dim, int r, int c) const {
+        if (r < 0 || c < 0) throw std::logic_error("constraint row refers to a missing geminal");
+        return gem(L, f, h, dim, r, c);
+    }
+    int hp(int p, int q) const { return L.sym_pair(L.symmetry[p], L.symmetry[q]); }
+    // D2ab-type (ab geminals), D2aa-type (aa geminals), G2 2g x 2g
+    int64_t ab(Fam f, int p, int q, int r, int s) const {
+        const int h = hp(p, q);
+        return at(f, h, L.gems_ab[h], L.ab(h, p, q), L.ab(h, r, s));
+    }
+    int64_t aa(Fam f, int p, int q, int r, int s) const {
+        const int h = hp(p, q);
+        return at(f, h, L.gems_aa[h], L.aa(h, p, q), L.aa(h, r, s));
+    }
+    int64_t g2(bool beta, int p, int q, int r, int s) const {
+        const int h = hp(p, q), g = L.gems_ab[h], o = beta ? g : 0;
+        if (L.ab(h, p, q) < 0 || L.ab(h, r, s) < 0) throw std::logic_error("constraint row refers to a missing geminal");
+        return at(F_G2AA, h, 2 * g, L.ab(h, p, q) + o, L.ab(h, r, s) + o);
+    }
+};
+
+// Sign of the antisymmetric pair (p,q) stored as its p > q geminal.
+inline int pair_sign(int p, int q) { return p > q ? -1 : 1; }
+
+// t1.cc:433-811 (T1_constraints_Au).  Row order aab, bba, aaa, bbb; every
+// row is -T1(ijk,lmn) plus Q2 / D2 / G2 / D1 terms selected by coincident
+// indices.
+void rows_t1(const Layout& L, RowSink& S) {
+    const Gem G{L};
+    for (int beta = 0; beta < 2; beta++) {
+        const Fam ft = beta ? F_T1BBA : F_T1AAB, fq = beta ? F_Q2BB : F_Q2AA, fg = beta ? F_G2AB : F_G2BA;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int nt = L.trip_aab[h];
+            for (int I = 0; I < nt; I++) {
+                const int i = L.bas_aab[h][I][0], j = L.bas_aab[h][I][1], k = L.bas_aab[h][I][2];
+                for (int J = 0; J < nt; J++) {
+                    const int l = L.bas_aab[h][J][0], m = L.bas_aab[h][J][1], n = L.bas_aab[h][J][2];
+                    S.add(G.at(ft, h, nt, I, J), -1.0);
+                    if (k == n) S.add(G.aa(fq, i, j, l, m), 1.0);
+                    if (!beta) {
+                        if (j == l) S.add(G.ab(F_D2AB, m, n, i, k), -1.0);
+                        if (l == i) S.add(G.ab(F_D2AB, m, n, j, k), 1.0);
+                    } else {
+                        if (j == l) S.add(G.ab(F_D2AB, n, m, k, i), -1.0);
+                        if (l == i) S.add(G.ab(F_D2AB, n, m, k, j), 1.0);
+                    }
+                    if (j == m) S.add(G.ab(fg, n, i, k, l), -1.0);
+                    if (i == m) S.add(G.ab(fg, n, j, k, l), 1.0);
+                    S.end();
+                }
+            }
+        }
+    }
+    for (int beta = 0; beta < 2; beta++) {
+        const Fam ft = beta ? F_T1BBB : F_T1AAA, fq = beta ? F_Q2BB : F_Q2AA, fd = beta ? F_D2BB : F_D2AA,
+                  f1 = beta ? F_D1B : F_D1A;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int nt = L.trip_aaa[h];
+            for (int I = 0; I < nt; I++) {
+                const int i = L.bas_aaa[h][I][0], j = L.bas_aaa[h][I][1], k = L.bas_aaa[h][I][2];
+                for (int J = 0; J < nt; J++) {
+                    const int l = L.bas_aaa[h][J][0], m = L.bas_aaa[h][J][1], n = L.bas_aaa[h][J][2];
+                    S.add(G.at(ft, h, nt, I, J), -1.0);
+                    if (k == n) S.add(G.aa(fq, i, j, l, m), 1.0);
+                    if (j == n && G.hp(i, k) == G.hp(l, m)) S.add(G.aa(fq, i, k, l, m), -1.0);
+                    if (i == n && G.hp(j, k) == G.hp(l, m)) S.add(G.aa(fq, j, k, l, m), 1.0);
+                    if (l == k && G.hp(j, i) == G.hp(n, m)) S.add(G.aa(fd, n, m, j, i), 1.0);
+                    if (j == l) S.add(G.aa(fd, n, m, k, i), -1.0);
+                    if (l == i) S.add(G.aa(fd, n, m, k, j), 1.0);
+                    if (k == m) {
+                        if (j == l) S.add(d1(L, f1, n, i), -1.0);
+                        S.add(G.g2(beta, n, i, j, l), 1.0);
+                    }
+                    if (j == m) {
+                        if (k == l) S.add(d1(L, f1, n, i), 1.0);
+                        S.add(G.g2(beta, n, i, k, l), -1.0);
+                    }
+                    if (i == m) {
+                        if (k == l) S.add(d1(L, f1, n, j), -1.0);
+                        S.add(G.g2(beta, n, j, k, l), 1.0);
+                    }
+                    S.end();
+                }
+            }
+        }
+    }
+}
+
+// t2.cc:1251-1862 (T2_constraints_Au_slow, the form the reference calls).
+// Row order aab, bba, then the two (aab + aba)-dimensional blocks aaa/abb
+// and bbb/baa, each walked row by row over its four sub-blocks.
+void rows_t2(const Layout& L, RowSink& S) {
+    const Gem G{L};
+    for (int beta = 0; beta < 2; beta++) {
+        const Fam ft = beta ? F_T2BBA : F_T2AAB, fd = beta ? F_D2BB : F_D2AA, f1 = beta ? F_D1A : F_D1B;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int nt = L.trip_aab[h];
+            for (int I = 0; I < nt; I++) {
+                const int i = L.bas_aab[h][I][0], j = L.bas_aab[h][I][1], k = L.bas_aab[h][I][2];
+                for (int J = 0; J < nt; J++) {
+                    const int l = L.bas_aab[h][J][0], m = L.bas_aab[h][J][1], n = L.bas_aab[h][J][2];
+                    S.add(G.at(ft, h, nt, I, J), -1.0);
+                    if (k == n) S.add(G.aa(fd, i, j, l, m), 1.0);
+                    if (j == m && i == l) S.add(d1(L, f1, n, k), 1.0);
+                    if (j == l && i == m) S.add(d1(L, f1, n, k), -1.0);
+                    if (!beta) {
+                        if (i == l) S.add(G.ab(F_D2AB, j, n, m, k), -1.0);
+                        if (j == l) S.add(G.ab(F_D2AB, i, n, m, k), 1.0);
+                        if (i == m) S.add(G.ab(F_D2AB, j, n, l, k), 1.0);
+                        if (j == m) S.add(G.ab(F_D2AB, i, n, l, k), -1.0);
+                    } else {
+                        if (i == l) S.add(G.ab(F_D2AB, n, j, k, m), -1.0);
+                        if (j == l) S.add(G.ab(F_D2AB, n, i, k, m), 1.0);
+                        if (i == m) S.add(G.ab(F_D2AB, n, j, k, l), 1.0);
+                        if (j == m) S.add(G.ab(F_D2AB, n, i, k, l), -1.0);
+                    }
+                    S.end();
+                }
+            }
+        }
+    }
+    for (int beta = 0; beta < 2; beta++) {
+        // beta = 0: aaa/abb block (same-spin D2aa, D1a; mixed D2ab, D2bb)
+        // beta = 1: bbb/baa block (same-spin D2bb, D1b; mixed D2ab, D2aa)
+        const Fam ft = beta ? F_T2BBB : F_T2AAA;
+        const Fam fs = beta ? F_D2BB : F_D2AA, fo = beta ? F_D2AA : F_D2BB;
+        const Fam f1s = beta ? F_D1B : F_D1A, f1o = beta ? F_D1A : F_D1B;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int na = L.trip_aab[h], nt = L.trip_aab[h] + L.trip_aba[h];
+            for (int I = 0; I < nt; I++) {
+                const bool ri = I >= na;
+                const auto& tI = ri ? L.bas_aba[h][I - na] : L.bas_aab[h][I];
+                const int i = tI[0], j = tI[1], k = tI[2];
+                for (int J = 0; J < nt; J++) {
+                    const bool cj = J >= na;
+                    const auto& tJ = cj ? L.bas_aba[h][J - na] : L.bas_aab[h][J];
+                    const int l = tJ[0], m = tJ[1], n = tJ[2];
+                    S.add(G.at(ft, h, nt, I, J), -1.0);
+                    if (!ri && !cj) {
+                        // same-spin triplets
+                        if (k == n) S.add(G.aa(fs, i, j, l, m), 1.0);
+                        if (j == m && i == l) S.add(d1(L, f1s, n, k), 1.0);
+                        if (j == l && i == m) S.add(d1(L, f1s, n, k), -1.0);
+                        if (i == l && n != j && k != m)
+                            S.add(G.aa(fs, n, j, k, m), -(double)(pair_sign(n, j) * pair_sign(k, m)));
+                        if (j == l && n != i && k != m)
+                            S.add(G.aa(fs, n, i, k, m), (double)(pair_sign(n, i) * pair_sign(k, m)));
+                        if (i == m && n != j && k != l)
+                            S.add(G.aa(fs, n, j, k, l), (double)(pair_sign(n, j) * pair_sign(k, l)));
+                        if (j == m && n != i && k != l)
+                            S.add(G.aa(fs, n, i, k, l), -(double)(pair_sign(n, i) * pair_sign(k, l)));
+                    } else if (!ri && cj) {
+                        if (!beta) {
+                            if (i == l) S.add(G.ab(F_D2AB, j, n, k, m), 1.0);
+                            if (j == l) S.add(G.ab(F_D2AB, i, n, k, m), -1.0);
+                        } else {
+                            if (i == l) S.add(G.ab(F_D2AB, n, j, m, k), 1.0);
+                            if (j == l) S.add(G.ab(F_D2AB, n, i, m, k), -1.0);
+                        }
+                    } else if (ri && !cj) {
+                        if (!beta) {
+                            if (i == l) S.add(G.ab(F_D2AB, n, j, m, k), 1.0);
+                            if (i == m) S.add(G.ab(F_D2AB, n, j, l, k), -1.0);
+                        } else {
+                            if (i == l) S.add(G.ab(F_D2AB, j, n, k, m), 1.0);
+                            if (i == m) S.add(G.ab(F_D2AB, j, n, k, l), -1.0);
+                        }
+                    } else {
+                        // mixed-spin triplets on both sides
+                        if (!beta) {
+                            if (k == n) S.add(G.ab(F_D2AB, i, j, l, m), 1.0);
+                        } else {
+                            if (k == n) S.add(G.ab(F_D2AB, j, i, m, l), 1.0);
+                        }
+                        if (j == m && i == l) S.add(d1(L, f1o, n, k), 1.0);
+                        if (i == l && n != j && k != m)
+                            S.add(G.aa(fo, n, j, k, m), -(double)(pair_sign(n, j) * pair_sign(k, m)));
+                        if (!beta) {
+                            if (j == m) S.add(G.ab(F_D2AB, i, n, l, k), -1.0);
+                        } else {
+                            if (j == m) S.add(G.ab(F_D2AB, n, i, k, l), -1.0);
+                        }
+                    }
+                    S.end();
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 
 std::string build_A(const Layout& L, Csr& A) {
@@ -376,8 +571,8 @@ std::string build_A(const Layout& L, Csr& A) {
     if (L.opt.constrain_spin) rows_spin(L, S);
     if (L.opt.constrain_q2) rows_q2(L, S);
     if (L.opt.constrain_g2) rows_g2(L, S);
-    if (L.opt.constrain_t1) return "T1 constraints are not built yet";
-    if (L.opt.constrain_t2) return "T2 constraints are not built yet";
+    if (L.opt.constrain_t1) rows_t1(L, S);
+    if (L.opt.constrain_t2) rows_t2(L, S);
     A.nrows = S.rows();
     A.ncols = L.dimx;
     if (A.nrows != L.ncon) return "internal error: constraint row count mismatch";

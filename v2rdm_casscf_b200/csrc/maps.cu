@@ -80,61 +80,130 @@ __device__ __forceinline__ double epilogue(const Epi& e, int64_t r, int B, int b
     return e.dotv ? e.dotv[t] * s : 0.0;
 }
 
-// Bucketed-ELL part.  Blocks [blk[i], blk[i+1]) serve bucket i; inside a
-// bucket the slots are dealt like rows in chunk_of (fixed instance per thread).
-template <int W>
-__device__ __forceinline__ double ell_rows(const DevMap& M, int bi, int64_t first_blk, int64_t nblk, int B,
-                                           const double* __restrict__ in, const Epi& e, int b, int rsub, int rpp) {
+// Bucketed-ELL part.  One lane per row (slot index i of its bucket) and a
+// chunk of up to kChunk consecutive instances per thread: the table loads of a
+// warp are 32 consecutive slots (coalesced), and every thread keeps
+// W x (instances) independent gathers in flight.  The instances of a chunk are
+// adjacent in memory ([col * B + b0 .. b0 + cnt)), loaded as double2 when B is
+// even.  Per instance the entries are summed in slot order, so the result does
+// not depend on the chunking.
+constexpr int kChunk = 8;
+
+struct Blocks {
+    int start[kMaxBuckets + 1];  // first row tile of each bucket
+    int nchunk;                  // instance chunks per row tile
+};
+
+template <int W, bool VEC>
+__device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0, int64_t ntile, int B, int b0,
+                                         int cnt, unsigned act, const double* __restrict__ in, const Epi& e,
+                                         double (&dot)[kChunk]) {
+    constexpr int KB = W < 4 ? W : 4;
     const int64_t ns = M.nslots[bi];
     const int32_t* rows = M.rows + M.row_off[bi];
     const int32_t* cols = M.cols + M.ent_off[bi];
     const double* vals = M.vals + M.ent_off[bi];
-    double acc = 0.0;
-    for (int64_t i = (blockIdx.x - first_blk) * rpp + rsub; i < ns; i += nblk * rpp) {
-        int c[W];
-        double v[W];
+    for (int64_t i = tile0 * kThreads + threadIdx.x; i < ns; i += ntile * kThreads) {
+        double acc[kChunk];
 #pragma unroll
-        for (int k = 0; k < W; k++) {
-            c[k] = cols[k * ns + i];
-            v[k] = vals[k * ns + i];
+        for (int j = 0; j < kChunk; j++) acc[j] = 0.0;
+#pragma unroll
+        for (int k0 = 0; k0 < W; k0 += KB) {
+            int c[KB];
+            double v[KB];
+#pragma unroll
+            for (int k = 0; k < KB; k++) {
+                c[k] = __ldg(cols + (int64_t)(k0 + k) * ns + i);
+                v[k] = __ldg(vals + (int64_t)(k0 + k) * ns + i);
+            }
+#pragma unroll
+            for (int k = 0; k < KB; k++) {
+                if (c[k] < 0) continue;
+                const double* g = in + (int64_t)c[k] * B + b0;
+                if (VEC) {
+#pragma unroll
+                    for (int j = 0; j < kChunk; j += 2)
+                        if (j < cnt) {
+                            const double2 q = __ldg(reinterpret_cast<const double2*>(g + j));
+                            acc[j] += v[k] * q.x;
+                            acc[j + 1] += v[k] * q.y;
+                        }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < kChunk; j++)
+                        if (j < cnt) acc[j] += v[k] * __ldg(g + j);
+                }
+            }
         }
-        double g[W];
+        const int64_t r = rows[i];
 #pragma unroll
-        for (int k = 0; k < W; k++) g[k] = (c[k] >= 0) ? in[(int64_t)c[k] * B + b] : 0.0;
-        double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < W; k++)
-            if (c[k] >= 0) s += v[k] * g[k];
-        acc += epilogue(e, rows[i], B, b, s);
+        for (int j = 0; j < kChunk; j++)
+            if (j < cnt && ((act >> j) & 1u)) dot[j] += epilogue(e, r, B, b0 + j, acc[j]);
     }
-    return acc;
 }
 
-struct Blocks {
-    int start[kMaxBuckets + 1];
-};
+// Instances [b0, b0 + cnt) of chunk ch: balanced, and in pairs when B is even
+// (so that double2 loads stay 16-byte aligned).
+__device__ __forceinline__ void chunk_range(int B, int nchunk, int ch, int& b0, int& cnt) {
+    if ((B & 1) == 0) {
+        const int P = B / 2;
+        b0 = 2 * (int)(((int64_t)ch * P) / nchunk);
+        cnt = 2 * (int)(((int64_t)(ch + 1) * P) / nchunk) - b0;
+    } else {
+        b0 = (int)(((int64_t)ch * B) / nchunk);
+        cnt = (int)(((int64_t)(ch + 1) * B) / nchunk) - b0;
+    }
+}
 
-__global__ void ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in, Epi e,
-                           const int* __restrict__ mask, double* __restrict__ partial) {
+__global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in,
+                                                       Epi e, const int* __restrict__ mask,
+                                                       double* __restrict__ partial) {
+    const int tile = blockIdx.x / bl.nchunk;
+    const int ch = blockIdx.x % bl.nchunk;
     int bi = 0;
-    while (bi + 1 < M.nb && (int)blockIdx.x >= bl.start[bi + 1]) bi++;
-    const int rpp = blockDim.x / B;
-    const int b = threadIdx.x % B;
-    const int rsub = threadIdx.x / B;
-    const bool live = threadIdx.x < rpp * B && !(mask && !mask[b]);
-    double acc = 0.0;
-    if (live) {
-        const int64_t f = bl.start[bi], nblk = bl.start[bi + 1] - bl.start[bi];
-        switch (M.width[bi]) {
-            case 1: acc = ell_rows<1>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
-            case 2: acc = ell_rows<2>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
-            case 4: acc = ell_rows<4>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
-            case 8: acc = ell_rows<8>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
-            case 16: acc = ell_rows<16>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
-            default: acc = ell_rows<32>(M, bi, f, nblk, B, in, e, b, rsub, rpp); break;
+    while (bi + 1 < M.nb && tile >= bl.start[bi + 1]) bi++;
+    int b0, cnt;
+    chunk_range(B, bl.nchunk, ch, b0, cnt);
+    unsigned act = 0;
+    for (int j = 0; j < cnt; j++)
+        if (!mask || mask[b0 + j]) act |= 1u << j;
+    double dot[kChunk];
+#pragma unroll
+    for (int j = 0; j < kChunk; j++) dot[j] = 0.0;
+    if (act) {
+        const int64_t t0 = tile - bl.start[bi], nt = bl.start[bi + 1] - bl.start[bi];
+        const bool vec = (B & 1) == 0;
+        switch (M.width[bi] * 2 + (vec ? 1 : 0)) {
+            case 2: ell_rows<1, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 3: ell_rows<1, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 4: ell_rows<2, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 5: ell_rows<2, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 8: ell_rows<4, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 9: ell_rows<4, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 16: ell_rows<8, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 17: ell_rows<8, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 32: ell_rows<16, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 33: ell_rows<16, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 64: ell_rows<32, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            default: ell_rows<32, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
         }
     }
-    if (partial) block_partial(acc, B, partial);
+    if (!partial) return;
+    // per-instance block sums in a fixed order: warp shuffles, then warps
+    __shared__ double sh[kThreads / 32][kChunk];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < kChunk; j++) {
+        double v = dot[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[warp][j] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < cnt) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; w++) t += sh[w][threadIdx.x];
+        partial[(int64_t)tile * B + b0 + threadIdx.x] = t;
+    }
 }
 
 // Long rows: one CTA per row; thread t sums entries k = t / B, t / B + T / B,
@@ -339,17 +408,18 @@ static int spmv_grid(int64_t nrows, int B) {
     return (int)(g < 1 ? 1 : g);
 }
 
-// Blocks per ELL bucket, proportional to its slots, at most kSpmvBlocks in all.
+// Row tiles (kThreads slots each) per ELL bucket, proportional to its slots,
+// at most kSpmvBlocks tiles in all; every tile runs once per instance chunk.
 static Blocks map_blocks(const DevMap& M, int B) {
     Blocks bl{};
-    const int64_t rpp = kThreads / B;
+    bl.nchunk = (B + kChunk - 1) / kChunk;
     int64_t tot = 0;
-    for (int i = 0; i < M.nb; i++) tot += (M.nslots[i] + rpp - 1) / rpp;
+    for (int i = 0; i < M.nb; i++) tot += (M.nslots[i] + kThreads - 1) / kThreads;
     const double scale = tot > kSpmvBlocks ? (double)kSpmvBlocks / (double)tot : 1.0;
     int acc = 0;
     for (int i = 0; i < M.nb; i++) {
         bl.start[i] = acc;
-        int64_t g = (int64_t)(((M.nslots[i] + rpp - 1) / rpp) * scale);
+        int64_t g = (int64_t)(((M.nslots[i] + kThreads - 1) / kThreads) * scale);
         if (g < 1) g = 1;
         acc += (int)g;
     }
@@ -362,7 +432,7 @@ static int run_map(const DevMap& M, int B, const double* in, double* out, const 
     Epi e{sub, coef, add, dotv, out};
     const Blocks bl = map_blocks(M, B);
     if (M.nb > 0) {
-        ell_kernel<<<bl.start[M.nb], kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+        ell_kernel<<<bl.start[M.nb] * bl.nchunk, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
         g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     }
     if (M.nlong > 0) {

@@ -839,8 +839,6 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         v2g::Options o;
         if (!v2g::parse_positivity(opt->positivity ? opt->positivity : "", o))
             return v2g::fail(V2G_ERR_ARG, "unknown POSITIVITY");
-        if (o.constrain_t1 || o.constrain_t2)
-            return v2g::fail(V2G_ERR_UNSUPPORTED, "T1/T2 positivity is not built in this version");
         o.constrain_spin = opt->constrain_spin != 0;
         o.constrain_sz = opt->constrain_sz != 0;
         o.r_convergence = opt->r_convergence;

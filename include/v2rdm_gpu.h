@@ -150,6 +150,17 @@ int v2g_update_xz(v2g_handle* h, double mu);
 int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const double* d_y, double* d_x, double* d_z,
                           void* stream);
 
+/* The RDMs handed to the orbital optimiser, as PackSpatialDensity
+ * (v2rdm_solver.cc:3664-3773), from the handle's x: d1 = spin-summed 1-RDM,
+ * per irrep, packed lower triangle (d1_act_spatial_sym_); d2 = spin-free
+ * 2-RDM over spatial pairs, per irrep, packed lower triangle
+ * (d2_act_spatial_sym_).  active_energies (Pitzer order, one per active
+ * orbital) fix the numbering of the spatial pairs as the plugin's orbital
+ * energies do (basis.cc:626-652); NULL numbers them in Pitzer order.  The
+ * values equal the reference's bit for bit. */
+int v2g_spatial_density_dims(const v2g_handle* h, long* d1_dim, long* d2_dim);
+int v2g_pack_spatial_density(v2g_handle* h, const double* active_energies, double* d1, double* d2);
+
 /* The full BPSDP solve from the handle's current state. */
 int v2g_solve(v2g_handle* h, v2g_result* res);
 

@@ -16,6 +16,7 @@ Pieces taken from v2rdm_solver.cc, located by anchor lines and checked:
   * SymmetryPair / TotalSym                        (v2rdm_solver.cc:1677-1682)
   * Guess, BuildConstraints, bpsdp_Au/ATu(_slow), cg_Ax, Update_xz
                                                    (v2rdm_solver.cc:2386-3289)
+  * PackSpatialDensity, the RDM hand-off to focas  (v2rdm_solver.cc:3664-3773)
 
 Usage: gen_ref_sources.py <reference_dir> <out_file>
 """
@@ -55,6 +56,12 @@ def main():
     while not src[g1].startswith("}"):
         g1 -= 1
 
+    # PackSpatialDensity: up to the line before RotateOrbitals.
+    p0 = find_unique(src, "void v2RDMSolver::PackSpatialDensity() {")
+    p1 = find_unique(src, "void v2RDMSolver::RotateOrbitals(){")
+    while not src[p1].startswith("}"):
+        p1 -= 1
+
     def block(a, b):
         return "\n".join(src[a:b + 1])
 
@@ -87,6 +94,8 @@ def main():
         block(s0, s1),
         f"#line {g0 + 1} \"v2rdm_solver.cc\"",
         block(g0, g1),
+        f"#line {p0 + 1} \"v2rdm_solver.cc\"",
+        block(p0, p1),
         "}}",
         "// accessor so that the harness drives CG through the reference trampoline",
         "void* oracle_evaluate_Ap_ptr() { return (void*)&evaluate_Ap; }",

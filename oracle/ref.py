@@ -61,6 +61,10 @@ def lib():
         L.oref_update_xz.argtypes = [P, D]
         L.oref_solve.argtypes = [P, D, D, I, I, DP, DP, I]
         L.oref_set_threads.argtypes = [I]
+        L.oref_set_next_energies.argtypes = [DP, I]
+        L.oref_spatial_dims.restype = ctypes.c_long
+        L.oref_spatial_dims.argtypes = [P, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long)]
+        L.oref_pack_spatial.argtypes = [P, DP, DP]
         _lib = L
     return _lib
 
@@ -88,8 +92,11 @@ class RefSolver:
     def __init__(self, nmopi, doccpi, soccpi=None, frzcpi=None, rstcpi=None, rstvpi=None, frzvpi=None,
                  multiplicity=1, positivity="DQG", constrain_spin=True, constrain_sz=True,
                  r_convergence=1e-4, e_convergence=1e-4, cg_convergence=1e-9, maxiter=10000,
-                 cg_maxiter=10000):
+                 cg_maxiter=10000, energies=None):
         nirrep = len(nmopi)
+        if energies is not None:  # orbital energies, all orbitals in Pitzer order
+            e = np.ascontiguousarray(energies, dtype=np.float64)
+            lib().oref_set_next_energies(_dptr(e), int(e.size))
         z = [0] * nirrep
         arrs = [_iarr(v if v is not None else z) for v in
                 (nmopi, frzcpi, rstcpi, rstvpi, frzvpi, doccpi, soccpi)]
@@ -173,6 +180,14 @@ class RefSolver:
 
     def update_xz(self, mu):
         lib().oref_update_xz(self.h, float(mu))
+
+    def pack_spatial_density(self):
+        """(d1, d2) of PackSpatialDensity for the current x (v2rdm_solver.cc:3664-3773)."""
+        n1, n2 = ctypes.c_long(), ctypes.c_long()
+        lib().oref_spatial_dims(self.h, ctypes.byref(n1), ctypes.byref(n2))
+        d1, d2 = np.zeros(n1.value), np.zeros(n2.value)
+        lib().oref_pack_spatial(self.h, _dptr(d1), _dptr(d2))
+        return d1, d2
 
     def solve(self, tau=1.0, mu=1.0, mu_update_frequency=500, max_outer=0, trace_cap=0):
         res = np.zeros(16)

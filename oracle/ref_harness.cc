@@ -45,6 +45,8 @@ double v2RDMSolver::compute_energy() { return 0.0; }
 SharedMatrix v2RDMSolver::GetOEI() { throw PsiException("GetOEI is not available in the oracle", __FILE__, __LINE__); }
 void v2RDMSolver::GetTEIFromDisk() { throw PsiException("GetTEIFromDisk is not available in the oracle", __FILE__, __LINE__); }
 
+std::vector<double> g_next_eps;  // orbital energies for the next setup (Pitzer order)
+
 class OracleSolver : public v2RDMSolver {
   public:
     explicit OracleSolver(Options& o) : v2RDMSolver(SharedWavefunction(), o) {}
@@ -86,15 +88,19 @@ class OracleSolver : public v2RDMSolver {
             amopi_[h] = nmopi_[h] - frzcpi_[h] - rstcpi_[h] - rstvpi_[h] - frzvpi_[h];
             amo_ += amopi_[h];
         }
-        // Orbital energies only order orbitals inside BuildBasis; any strictly
-        // increasing sequence per irrep reproduces Pitzer order.
+        // Orbital energies only order orbitals inside BuildBasis (the energy
+        // order sets the numbering of the spatial pairs that PackSpatialDensity
+        // writes); default i + 0.001 h, or the values given to
+        // oref_set_next_energies (all orbitals, Pitzer order).
         epsilon_a_ = SharedVector(new Vector(nirrep_, (int*)nmopi_));
         epsilon_b_ = SharedVector(new Vector(nirrep_, (int*)nmopi_));
-        for (int h = 0; h < nirrep; h++)
-            for (int i = 0; i < nmopi[h]; i++) {
-                epsilon_a_->pointer(h)[i] = i + 0.001 * h;
-                epsilon_b_->pointer(h)[i] = i + 0.001 * h;
+        for (int h = 0, k = 0; h < nirrep; h++)
+            for (int i = 0; i < nmopi[h]; i++, k++) {
+                const double e = (k < (int)g_next_eps.size()) ? g_next_eps[k] : i + 0.001 * h;
+                epsilon_a_->pointer(h)[i] = e;
+                epsilon_b_->pointer(h)[i] = e;
             }
+        g_next_eps.clear();
         is_df_ = true;
         is_doci_ = false;
         doci_alpha_ = 1.0;
@@ -292,6 +298,30 @@ class OracleSolver : public v2RDMSolver {
     void do_Au(SharedVector out, SharedVector in) { bpsdp_Au(out, in); }
     void do_ATu(SharedVector out, SharedVector in) { bpsdp_ATu(out, in); }
     void do_guess() { Guess(); }
+    // Packed spatial densities of PackSpatialDensity (v2rdm_solver.cc:3664),
+    // sized as tei.cc:91-110 sizes them.
+    long d1_dim() const {
+        long n = 0;
+        for (int h = 0; h < nirrep_; h++) n += (long)amopi_[h] * (amopi_[h] + 1) / 2;
+        return n;
+    }
+    long d2_dim() const {
+        long n = 0;
+        for (int h = 0; h < nirrep_; h++) n += (long)gems_00[h] * (gems_00[h] + 1L) / 2L;
+        return n;
+    }
+    void do_pack(double* d1, double* d2) {
+        std::vector<double> a(d1_dim() + 1), b(d2_dim() + 1);
+        d1_act_spatial_sym_ = a.data();
+        d2_act_spatial_sym_ = b.data();
+        d1_act_spatial_dim_ = d1_dim();  // PackSpatialDensity clears d2 by this size
+        d2_act_spatial_dim_ = d2_dim();
+        PackSpatialDensity();
+        memcpy(d1, a.data(), sizeof(double) * d1_dim());
+        memcpy(d2, b.data(), sizeof(double) * d2_dim());
+        d1_act_spatial_sym_ = nullptr;
+        d2_act_spatial_sym_ = nullptr;
+    }
     void do_build_constraints() { BuildConstraints(); }
     double efzc() const { return efzc_; }
     int* symmetry_of_active() { return symmetry; }
@@ -316,6 +346,14 @@ thread_local std::string g_err;
 extern "C" {
 
 const char* oref_last_error() { return g_err.c_str(); }
+
+void oref_set_next_energies(const double* eps, int n) { psi::v2rdm_casscf::g_next_eps.assign(eps, eps + n); }
+long oref_spatial_dims(void* h, long* d1, long* d2) {
+    *d1 = ((Handle*)h)->s->d1_dim();
+    *d2 = ((Handle*)h)->s->d2_dim();
+    return 0;
+}
+void oref_pack_spatial(void* h, double* d1, double* d2) { ((Handle*)h)->s->do_pack(d1, d2); }
 
 void* oref_create(int nirrep, const int* nmopi, const int* frzcpi, const int* rstcpi, const int* rstvpi,
                   const int* frzvpi, const int* doccpi, const int* soccpi, int multiplicity, const char* positivity,

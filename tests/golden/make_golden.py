@@ -5,6 +5,7 @@ Runs the reference's own hot-path code, compiled from the reference tree into
 oracle/_ref/libv2rdm_ref.so (see oracle/Makefile), on seeded inputs and stores
 inputs and outputs as .npz files:
 
+  pack_<case>.npz   d1 and d2 of PackSpatialDensity for a seeded x
   maps_<case>.npz   A u and A^T w of bpsdp_Au / bpsdp_ATu for seeded u, w, plus
                     b (BuildConstraints) and the layout sizes
   c_<case>.npz      c and efzc of RepackIntegrals/FrozenCoreEnergy for seeded
@@ -39,6 +40,14 @@ MAP_CASES = {
     "c1_n4_dqgt1": ([4], [2], [0], "DQGT1", True, True),
     "c1_n4_dqgt2": ([4], [2], [0], "DQGT2", True, True),
     "c2_n4_doublet_dqgt": ([2, 2], [1, 0], [1, 0], "DQGT1T2", True, True),
+}
+
+PACK_CASES = {
+    # name: (amopi, doccpi, soccpi, orbital energies in Pitzer order or None)
+    "c1_n4": ([4], [2], [0], None),
+    "c1_n5_doublet": ([5], [2], [1], [0.5, 0.1, 0.3, 0.3, 0.2]),
+    "c2v_n6": ([2, 1, 1, 2], [1, 0, 0, 1], [0, 0, 0, 0], [0.3, 1.1, 0.2, 0.5, 0.1, 0.9]),
+    "c2_n5_doublet": ([3, 2], [1, 1], [1, 0], [0.2, 0.4, 0.9, 0.3, 0.35]),
 }
 
 SOLVE_CASES = {
@@ -99,6 +108,18 @@ def xz():
                             x_out=r.get("x"), z_out=r.get("z"))
 
 
+def pack(name, spec):
+    """PackSpatialDensity (v2rdm_solver.cc:3664-3773) of a seeded x."""
+    amopi, docc, socc, energies = spec
+    r = RefSolver(amopi, docc, soccpi=socc, multiplicity=sum(socc) + 1, energies=energies)
+    x = np.random.default_rng(7).standard_normal(r.dimx)
+    r.set("x", x)
+    d1, d2 = r.pack_spatial_density()
+    np.savez_compressed(os.path.join(HERE, f"pack_{name}.npz"), amopi=amopi, doccpi=docc, soccpi=socc,
+                        energies=np.array(energies if energies is not None else [], dtype=float),
+                        x=x, d1=d1, d2=d2)
+
+
 def solve(name, spec):
     n, seed, rc, ec, electrons = spec[:5]
     pos = spec[5] if len(spec) > 5 else "DQG"
@@ -120,6 +141,8 @@ if __name__ == "__main__":
     set_threads(int(os.environ.get("OMP_NUM_THREADS", "4")))
     for k, v in MAP_CASES.items():
         maps(k, v)
+    for k, v in PACK_CASES.items():
+        pack(k, v)
     cvec()
     xz()
     for k, v in SOLVE_CASES.items():

@@ -2,6 +2,7 @@
 layout, constraint table, b and c match the reference (golden fixtures made by
 tests/golden/make_golden.py from the reference's own code, and the compiled
 oracle when present)."""
+import ctypes
 import glob
 import os
 import re
@@ -102,3 +103,31 @@ def test_invalid_options_fail_loudly(v2g):
         v2g.V2RDMSolver([4], 2, 2, options=dict(MAXITER=0))
     with pytest.raises(KeyError):
         v2g.V2RDMSolver([4], 2, 2, options=dict(NOT_AN_OPTION=1))
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "pack_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_oracle_reproduces_spatial_density_golden(ref, path):
+    g = load(path)
+    e = g["energies"] if g["energies"].size else None
+    r = ref.RefSolver(g["amopi"].tolist(), g["doccpi"].tolist(), soccpi=g["soccpi"].tolist(),
+                      multiplicity=int(g["soccpi"].sum()) + 1, energies=e)
+    r.set("x", g["x"])
+    d1, d2 = r.pack_spatial_density()
+    assert np.array_equal(d1, g["d1"]) and np.array_equal(d2, g["d2"])
+
+
+def test_spatial_density_dims(v2g):
+    for amopi, na, nb in (([4], 2, 2), ([2, 1, 1, 2], 2, 2), ([3, 2], 3, 2)):
+        s = v2g.V2RDMSolver(amopi, na, nb, na - nb + 1)
+        n1, n2 = ctypes.c_long(), ctypes.c_long()
+        assert v2g.lib().v2g_spatial_density_dims(s.h, ctypes.byref(n1), ctypes.byref(n2)) == 0
+        n = sum(amopi)
+        assert n1.value == sum(a * (a + 1) // 2 for a in amopi)
+        # spatial pairs i >= j per irrep of the pair
+        sym = [h for h, a in enumerate(amopi) for _ in range(a)]
+        g00 = [0] * len(amopi)
+        for i in range(n):
+            for j in range(i + 1):
+                g00[sym[i] ^ sym[j]] += 1
+        assert n2.value == sum(g * (g + 1) // 2 for g in g00)

@@ -172,3 +172,19 @@ def test_cg_tolerance_factor_reaches_the_same_energy(v2g):
     assert s.result["status"] == 0
     assert abs(e - float(g["e_primal"])) <= 1e-6
     assert s.result["iiter"] < int(g["iiter"])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "pack_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_spatial_density_matches_reference(v2g, path):
+    # PackSpatialDensity: the same sums in the same order, so bit for bit
+    g = load(path)
+    amopi = g["amopi"].tolist()
+    na = int(g["doccpi"].sum() + g["soccpi"].sum())
+    nb = int(g["doccpi"].sum())
+    s = v2g.V2RDMSolver(amopi, na, nb, na - nb + 1)
+    s.set_state(g["x"], np.zeros(s.nconstraints), np.zeros(s.dimx), 1.0)
+    e = g["energies"] if g["energies"].size else None
+    d1, d2 = s.pack_spatial_density(e)
+    assert np.array_equal(d1, g["d1"])
+    assert np.array_equal(d2, g["d2"])

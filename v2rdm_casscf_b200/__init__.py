@@ -34,7 +34,7 @@ EXPORTS = [
     "v2g_guess_random", "v2g_set_state", "v2g_get_state", "v2g_apply_A", "v2g_apply_AT", "v2g_apply_A_device",
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
-    "v2g_update_xz_noalloc",
+    "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density",
 ]
 
 
@@ -137,6 +137,8 @@ def lib():
             getattr(L, f).argtypes = [P, P, P]
         L.v2g_update_xz.argtypes = [P, D]
         L.v2g_update_xz_noalloc.argtypes = [P, D, P, P, P, P, P]
+        L.v2g_spatial_density_dims.argtypes = [P, LP, LP]
+        L.v2g_pack_spatial_density.argtypes = [P, DP, DP, DP]
         L.v2g_solve.argtypes = [P, ctypes.POINTER(Result)]
         L.v2g_solve_batch.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(Result)]
         L.v2g_export_A.argtypes = [P, LP, IP, DP]
@@ -200,6 +202,7 @@ class V2RDMSolver:
                  restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False,
                  profile=False, projection="exact", cg_tolerance_factor=0.01):
         L = lib()
+        self.active = list(active)
         opts = dict(DEFAULT_OPTIONS)
         for k, v in (options or {}).items():
             k = k.upper()
@@ -334,6 +337,18 @@ class V2RDMSolver:
 
     def update_xz(self, mu):
         _check(lib().v2g_update_xz(self.h, float(mu)))
+
+    def pack_spatial_density(self, active_energies=None):
+        """(d1, d2) handed to focas, as PackSpatialDensity (v2rdm_solver.cc:3664-3773)."""
+        n1, n2 = ctypes.c_long(), ctypes.c_long()
+        _check(lib().v2g_spatial_density_dims(self.h, ctypes.byref(n1), ctypes.byref(n2)))
+        d1, d2 = np.zeros(n1.value), np.zeros(n2.value)
+        e = None
+        if active_energies is not None:
+            e = np.ascontiguousarray(active_energies, dtype=np.float64)
+            assert e.size == sum(self.active)
+        _check(lib().v2g_pack_spatial_density(self.h, _dp(e) if e is not None else None, _dp(d1), _dp(d2)))
+        return d1, d2
 
     def update_xz_noalloc(self, mu, d_c, d_y, d_x, d_z, stream=None):
         """Update_xz on caller-owned device vectors (raw pointers), allocating no

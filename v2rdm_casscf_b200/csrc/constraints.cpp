@@ -2,6 +2,7 @@
 #include "constraints.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <stdexcept>
 
@@ -740,6 +741,118 @@ std::string build_c(const Layout& L, const OrbitalSpaces& sp, const double* oei,
         }
     }
     return "";
+}
+
+void build_spatial_map(const Layout& L, const double* active_energies, Csr& P, int64_t& d1_dim, int64_t& d2_dim) {
+    const int n = L.amo, H = L.nirrep;
+    // active orbitals in energy order; ties keep Pitzer order (the reference
+    // takes the first strict minimum, basis.cc:211-238)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    if (active_energies)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return active_energies[a] < active_energies[b]; });
+    // spatial pairs (basis.cc:626-652)
+    std::vector<int> g00(H, 0);
+    std::vector<std::vector<int>> i00(H, std::vector<int>((size_t)n * n, -1));
+    for (int ie = 0; ie < n; ie++)
+        for (int je = 0; je <= ie; je++) {
+            const int i = order[ie], j = order[je];
+            const int h = L.sym_pair(L.symmetry[i], L.symmetry[j]);
+            i00[h][(size_t)i * n + j] = g00[h];
+            i00[h][(size_t)j * n + i] = g00[h];
+            g00[h]++;
+        }
+    auto tri = [](int64_t a, int64_t b) { return a > b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; };
+    std::vector<int64_t> off2(H + 1, 0), off1(H + 1, 0);
+    for (int h = 0; h < H; h++) {
+        off2[h + 1] = off2[h] + (int64_t)g00[h] * (g00[h] + 1) / 2;
+        off1[h + 1] = off1[h] + (int64_t)L.amopi[h] * (L.amopi[h] + 1) / 2;
+    }
+    d1_dim = off1[H];
+    d2_dim = off2[H];
+    // the last (h, ij, kl) of the reference's loop that writes each element
+    std::vector<int64_t> win((size_t)d2_dim, -1);
+    int64_t gmax = 1;
+    for (int h = 0; h < H; h++) gmax = std::max<int64_t>(gmax, L.gems_ab[h]);
+    for (int h = 0; h < H; h++)
+        for (int ij = 0; ij < L.gems_ab[h]; ij++) {
+            const int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+            for (int kl = 0; kl < L.gems_ab[h]; kl++) {
+                const int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                const int hik = L.sym_pair(L.symmetry[i], L.symmetry[k]);
+                const int ik = i00[hik][(size_t)i * n + k], jl = i00[hik][(size_t)j * n + l];
+                win[(size_t)(off2[hik] + tri(ik, jl))] = ((int64_t)h * gmax + ij) * gmax + kl;
+            }
+        }
+    P = Csr();
+    P.nrows = d1_dim + d2_dim;
+    P.ncols = L.dimx;
+    P.rowptr.assign(1, 0);
+    // d1: D1a(i,j) + D1b(i,j), i <= j, element INDEX(i,j) of irrep h
+    std::vector<std::array<int64_t, 2>> r1((size_t)d1_dim, {-1, -1});
+    for (int h = 0; h < H; h++)
+        for (int i = 0; i < L.amopi[h]; i++)
+            for (int j = i; j < L.amopi[h]; j++) {
+                const int64_t e = (int64_t)i * L.amopi[h] + j;
+                r1[(size_t)(off1[h] + tri(i, j))] = {L.off[F_D1A][h] + e, L.off[F_D1B][h] + e};
+            }
+    for (const auto& r : r1) {
+        for (int64_t c : r) {
+            P.col.push_back((int32_t)c);
+            P.val.push_back(1.0);
+        }
+        P.rowptr.push_back((int64_t)P.col.size());
+    }
+    // d2: the sixteen terms of v2rdm_solver.cc:3713-3742 in their order
+    auto ab = [&](int h, int p, int q) { return L.ab(h, p, q); };
+    auto aa = [&](int h, int p, int q) { return L.aa(h, p, q); };
+    for (int64_t id = 0; id < d2_dim; id++) {
+        const int64_t w = win[(size_t)id];
+        if (w >= 0) {
+            const int h = (int)(w / (gmax * gmax)), ij = (int)((w / gmax) % gmax), kl = (int)(w % gmax);
+            const int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+            const int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+            const int hik = L.sym_pair(L.symmetry[i], L.symmetry[k]);
+            const int hkj = L.sym_pair(L.symmetry[k], L.symmetry[j]);
+            const bool diag = i00[hik][(size_t)i * n + k] == i00[hik][(size_t)j * n + l];
+            const double half = diag ? 0.5 : 1.0;
+            const bool lj = l == j, ikq = i == k;
+            const int64_t gh = L.gems_ab[h], gk = L.gems_ab[hkj], ah = L.gems_aa[h], ak = L.gems_aa[hkj];
+            auto put = [&](int64_t col, double coef) {
+                P.col.push_back((int32_t)col);
+                P.val.push_back(coef);
+            };
+            const int64_t dab = L.off[F_D2AB][h], dabk = L.off[F_D2AB][hkj];
+            const int ijab = ab(h, i, j), jiab = ab(h, j, i), klab = ab(h, k, l), lkab = ab(h, l, k);
+            const int kjab = ab(hkj, k, j), ilab = ab(hkj, i, l), jkab = ab(hkj, j, k), liab = ab(hkj, l, i);
+            put(dab + ijab * gh + klab, half);
+            if (!lj) put(dabk + kjab * gk + ilab, half);
+            if (!ikq) put(dabk + ilab * gk + kjab, half);
+            if (!lj && !ikq) put(dab + klab * gh + ijab, half);
+            put(dab + jiab * gh + lkab, half);
+            if (!lj) put(dabk + jkab * gk + liab, half);
+            if (!ikq) put(dabk + liab * gk + jkab, half);
+            if (!lj && !ikq) put(dab + lkab * gh + jiab, half);
+            if (i != j && k != l) {
+                const double s = half * (i < j ? 1 : -1) * (k < l ? 1 : -1);
+                const int ijaa = aa(h, i, j), klaa = aa(h, k, l);
+                put(L.off[F_D2AA][h] + ijaa * ah + klaa, s);
+                if (!lj && !ikq) put(L.off[F_D2AA][h] + klaa * ah + ijaa, s);
+                put(L.off[F_D2BB][h] + ijaa * ah + klaa, s);
+                if (!lj && !ikq) put(L.off[F_D2BB][h] + klaa * ah + ijaa, s);
+            }
+            if (k != j && i != l) {
+                const double s = half * (k < j ? 1 : -1) * (i < l ? 1 : -1);
+                const int kjaa = aa(hkj, k, j), ilaa = aa(hkj, i, l);
+                if (!lj) put(L.off[F_D2AA][hkj] + kjaa * ak + ilaa, s);
+                if (!ikq) put(L.off[F_D2AA][hkj] + ilaa * ak + kjaa, s);
+                if (!lj) put(L.off[F_D2BB][hkj] + kjaa * ak + ilaa, s);
+                if (!ikq) put(L.off[F_D2BB][hkj] + ilaa * ak + kjaa, s);
+            }
+        }
+        P.rowptr.push_back((int64_t)P.col.size());
+    }
 }
 
 }  // namespace v2g

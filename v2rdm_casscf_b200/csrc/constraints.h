@@ -47,4 +47,14 @@ struct OrbitalSpaces {
 std::string build_c(const Layout& L, const OrbitalSpaces& sp, const double* oei_packed, const double* qmo, int nq,
                     std::vector<double>& c, double& efzc);
 
+// PackSpatialDensity (v2rdm_solver.cc:3664-3773) as a gather map P
+// ((d1_dim + d2_dim) x dimx): row r < d1_dim is element r of the packed
+// spin-summed 1-RDM, row d1_dim + r element r of the packed spin-free 2-RDM
+// handed to focas.  The spatial pairs are numbered in the energy order of the
+// active orbitals (basis.cc:626-652; energies in Pitzer order, NULL = Pitzer
+// order).  Each row lists its terms in the reference's summation order with
+// coefficients +-0.5 (+-1 for off-diagonal pairs, the reference's final
+// doubling), so an in-order FP64 sum reproduces the reference bit for bit.
+void build_spatial_map(const Layout& L, const double* active_energies, Csr& P, int64_t& d1_dim, int64_t& d2_dim);
+
 }  // namespace v2g

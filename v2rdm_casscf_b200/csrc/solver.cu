@@ -1003,6 +1003,49 @@ int v2g_apply_AT_batched_device(v2g_handle* h, int nvec, const double* u, double
     return apply_batched(h, nvec, u, out, stream, true);
 }
 
+int v2g_spatial_density_dims(const v2g_handle* h, long* d1_dim, long* d2_dim) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !d1_dim || !d2_dim) return v2g::fail(V2G_ERR_ARG, "null argument");
+        const v2g::Layout& L = h->P.L;
+        long n1 = 0, n2 = 0;
+        std::vector<int> g00(L.nirrep, 0);
+        for (int i = 0; i < L.amo; i++)
+            for (int j = 0; j <= i; j++) g00[L.sym_pair(L.symmetry[i], L.symmetry[j])]++;
+        for (int hh = 0; hh < L.nirrep; hh++) {
+            n1 += (long)L.amopi[hh] * (L.amopi[hh] + 1) / 2;
+            n2 += (long)g00[hh] * (g00[hh] + 1) / 2;
+        }
+        *d1_dim = n1;
+        *d2_dim = n2;
+        return V2G_OK;
+    });
+}
+
+int v2g_pack_spatial_density(v2g_handle* h, const double* active_energies, double* d1, double* d2) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !d1 || !d2) return v2g::fail(V2G_ERR_ARG, "null argument");
+        v2g::require_device();
+        Problem& P = h->P;
+        if ((int64_t)P.x.size() != P.L.dimx) return v2g::fail(V2G_ERR_ARG, "the handle has no primal state");
+        v2g::Csr M;
+        int64_t n1 = 0, n2 = 0;
+        v2g::build_spatial_map(P.L, active_energies, M, n1, n2);
+        CK(cudaSetDevice(P.device));
+        v2g::MapTable T;
+        T.build(M);
+        v2g::DevBuf<double> x, out;
+        x.upload(P.x.data(), P.x.size());
+        out.alloc((size_t)(n1 + n2));
+        v2g::launch_spmv(T.dm, 1, x.p, out.p, nullptr, nullptr, nullptr, nullptr, 0);
+        CK(cudaGetLastError());
+        std::vector<double> hout((size_t)(n1 + n2));
+        CK(cudaMemcpy(hout.data(), out.p, hout.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        std::copy(hout.begin(), hout.begin() + n1, d1);
+        std::copy(hout.begin() + n1, hout.end(), d2);
+        return V2G_OK;
+    });
+}
+
 int v2g_update_xz(v2g_handle* h, double mu) {
     return v2g::guarded([&]() -> int {
         if (!h || !(mu > 0.0)) return v2g::fail(V2G_ERR_ARG, "bad argument");

@@ -23,3 +23,25 @@ def make_solver(V, g, **kw):
 def csr_of(s):
     rp, col, val = s.A_csr()
     return sp.csr_matrix((val, col, rp), shape=(s.nconstraints, s.dimx))
+
+
+def fci_two_electron_singlet(a):
+    """Exact ground-state energy of a two-electron singlet in the active space
+    (dense diagonalisation over symmetric spatial pair functions), plus enuc.
+
+    For two electrons the D condition is exact, so a D-only v2RDM solve must
+    reach this energy: a check that does not go through the reference."""
+    n = a.n
+    h, g = a.h, a.eri()
+    eye = np.eye(n)
+    H = (np.einsum("ik,jl->ijkl", h, eye) + np.einsum("ik,jl->ijkl", eye, h)
+         + np.einsum("ikjl->ijkl", g)).reshape(n * n, n * n)
+    cols = []
+    for i in range(n):
+        for j in range(i, n):
+            v = np.zeros((n, n))
+            v[i, j] += 1.0
+            v[j, i] += 1.0
+            cols.append(v.ravel() / np.linalg.norm(v))
+    Q = np.array(cols).T
+    return float(np.linalg.eigvalsh(Q.T @ H @ Q)[0]) + a.enuc

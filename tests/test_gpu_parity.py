@@ -188,3 +188,16 @@ def test_spatial_density_matches_reference(v2g, path):
     d1, d2 = s.pack_spatial_density(e)
     assert np.array_equal(d1, g["d1"])
     assert np.array_equal(d2, g["d2"])
+
+
+@pytest.mark.parametrize("n,seed", [(3, 0), (4, 1), (5, 2)])
+def test_two_electron_d_equals_fci(v2g, n, seed):
+    # known answer independent of the reference: D is exact for two electrons
+    from tests.helpers import fci_two_electron_singlet
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a = synthetic(n, seed, electrons=2)
+    s = v2g.V2RDMSolver.from_active_space(a, options=dict(POSITIVITY="D", R_CONVERGENCE=1e-7, E_CONVERGENCE=1e-8))
+    s.guess()
+    e = s.compute_energy()
+    assert abs(e - fci_two_electron_singlet(a)) <= 1e-6

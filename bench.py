@@ -411,7 +411,7 @@ def main():
     ap.add_argument("--count", type=int, default=256)
     ap.add_argument("--max-outer", type=int, default=0, help="cap outer iterations (experiments only)")
     ap.add_argument("--projection", default="adaptive", choices=["exact", "adaptive"])
-    ap.add_argument("--cg-factor", type=float, default=0.1,
+    ap.add_argument("--cg-factor", type=float, default=0.01,
                     help="CG tolerance factor (0.01 = the reference's rule)")
     ap.add_argument("--plain", action="store_true", help="reference algorithm: exact projection, CG factor 0.01")
     ap.add_argument("--warmup-outer", type=int, default=3, help="outer iterations per warm-up step")

@@ -137,6 +137,24 @@ def solve(name, spec):
                         x=r.get("x"), y=r.get("y"), z=r.get("z"))
 
 
+def solve_hchain(name, natoms, spacing):
+    """Reference solve of an all-active H chain (STO-3G RHF orbitals, CD integrals)."""
+    from v2rdm_casscf_b200.hchain import hydrogen_chain
+
+    a = hydrogen_chain(natoms, spacing)
+    n = a.n
+    r = RefSolver([n], [a.nb], positivity="DQG", r_convergence=1e-6, e_convergence=1e-7)
+    r.set_integrals(a.oei_packed, a.qmo, a.nq, a.enuc)
+    r.guess()
+    r.build_constraints()
+    out = r.solve()
+    np.savez_compressed(os.path.join(HERE, f"solve_{name}.npz"), n=n, natoms=natoms, spacing=spacing,
+                        h=a.h, L=a.L, enuc=a.enuc, scf_energy=a.scf_energy, r_conv=1e-6, e_conv=1e-7,
+                        e_primal=out["e_primal"], e_dual=out["e_dual"], ep=out["ep"], ed=out["ed"],
+                        oiter=out["oiter"], iiter=out["iiter"], converged=out["converged"],
+                        t_total=out["t_total"])
+
+
 if __name__ == "__main__":
     set_threads(int(os.environ.get("OMP_NUM_THREADS", "4")))
     for k, v in MAP_CASES.items():
@@ -147,4 +165,5 @@ if __name__ == "__main__":
     xz()
     for k, v in SOLVE_CASES.items():
         solve(k, v)
+    solve_hchain("h10_chain", 10, 0.9)
     print("golden fixtures written to", HERE)

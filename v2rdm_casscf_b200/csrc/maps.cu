@@ -81,32 +81,34 @@ __device__ __forceinline__ double epilogue(const Epi& e, int64_t r, int B, int b
 }
 
 // Bucketed-ELL part.  One lane per row (slot index i of its bucket) and a
-// chunk of up to kChunk consecutive instances per thread: the table loads of a
+// chunk of up to CH consecutive instances per thread: the table loads of a
 // warp are 32 consecutive slots (coalesced), and every thread keeps
 // W x (instances) independent gathers in flight.  The instances of a chunk are
 // adjacent in memory ([col * B + b0 .. b0 + cnt)), loaded as double2 when B is
 // even.  Per instance the entries are summed in slot order, so the result does
-// not depend on the chunking.
-constexpr int kChunk = 8;
+// not depend on the chunking.  CH = 4 (80 registers, three CTAs per SM) was
+// the fastest of 2, 4 and 8 at n = 12..20 with 8..20 instances (B200); single
+// instances use CH = 2 (64 registers).
+constexpr int kSlotBatch = 4;  // slots whose gathers are issued together
 
 struct Blocks {
     int start[kMaxBuckets + 1];  // first row tile of each bucket
     int nchunk;                  // instance chunks per row tile
 };
 
-template <int W, bool VEC>
+template <int W, bool VEC, int CH>
 __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0, int64_t ntile, int B, int b0,
                                          int cnt, unsigned act, const double* __restrict__ in, const Epi& e,
-                                         double (&dot)[kChunk]) {
-    constexpr int KB = W < 4 ? W : 4;
+                                         double (&dot)[CH]) {
+    constexpr int KB = W < kSlotBatch ? W : kSlotBatch;
     const int64_t ns = M.nslots[bi];
     const int32_t* rows = M.rows + M.row_off[bi];
     const int32_t* cols = M.cols + M.ent_off[bi];
     const double* vals = M.vals + M.ent_off[bi];
     for (int64_t i = tile0 * kThreads + threadIdx.x; i < ns; i += ntile * kThreads) {
-        double acc[kChunk];
+        double acc[CH];
 #pragma unroll
-        for (int j = 0; j < kChunk; j++) acc[j] = 0.0;
+        for (int j = 0; j < CH; j++) acc[j] = 0.0;
 #pragma unroll
         for (int k0 = 0; k0 < W; k0 += KB) {
             int c[KB];
@@ -122,7 +124,7 @@ __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0,
                 const double* g = in + (int64_t)c[k] * B + b0;
                 if (VEC) {
 #pragma unroll
-                    for (int j = 0; j < kChunk; j += 2)
+                    for (int j = 0; j < CH; j += 2)
                         if (j < cnt) {
                             const double2 q = __ldg(reinterpret_cast<const double2*>(g + j));
                             acc[j] += v[k] * q.x;
@@ -130,14 +132,14 @@ __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0,
                         }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < kChunk; j++)
+                    for (int j = 0; j < CH; j++)
                         if (j < cnt) acc[j] += v[k] * __ldg(g + j);
                 }
             }
         }
         const int64_t r = rows[i];
 #pragma unroll
-        for (int j = 0; j < kChunk; j++)
+        for (int j = 0; j < CH; j++)
             if (j < cnt && ((act >> j) & 1u)) dot[j] += epilogue(e, r, B, b0 + j, acc[j]);
     }
 }
@@ -155,6 +157,7 @@ __device__ __forceinline__ void chunk_range(int B, int nchunk, int ch, int& b0, 
     }
 }
 
+template <int CH>
 __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in,
                                                        Epi e, const int* __restrict__ mask,
                                                        double* __restrict__ partial) {
@@ -167,33 +170,33 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int 
     unsigned act = 0;
     for (int j = 0; j < cnt; j++)
         if (!mask || mask[b0 + j]) act |= 1u << j;
-    double dot[kChunk];
+    double dot[CH];
 #pragma unroll
-    for (int j = 0; j < kChunk; j++) dot[j] = 0.0;
+    for (int j = 0; j < CH; j++) dot[j] = 0.0;
     if (act) {
         const int64_t t0 = tile - bl.start[bi], nt = bl.start[bi + 1] - bl.start[bi];
         const bool vec = (B & 1) == 0;
         switch (M.width[bi] * 2 + (vec ? 1 : 0)) {
-            case 2: ell_rows<1, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 3: ell_rows<1, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 4: ell_rows<2, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 5: ell_rows<2, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 8: ell_rows<4, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 9: ell_rows<4, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 16: ell_rows<8, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 17: ell_rows<8, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 32: ell_rows<16, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 33: ell_rows<16, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 64: ell_rows<32, false>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            default: ell_rows<32, true>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 2: ell_rows<1, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 3: ell_rows<1, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 4: ell_rows<2, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 5: ell_rows<2, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 8: ell_rows<4, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 9: ell_rows<4, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 16: ell_rows<8, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 17: ell_rows<8, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 32: ell_rows<16, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 33: ell_rows<16, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 64: ell_rows<32, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            default: ell_rows<32, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
         }
     }
     if (!partial) return;
     // per-instance block sums in a fixed order: warp shuffles, then warps
-    __shared__ double sh[kThreads / 32][kChunk];
+    __shared__ double sh[kThreads / 32][CH];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int j = 0; j < kChunk; j++) {
+    for (int j = 0; j < CH; j++) {
         double v = dot[j];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) sh[warp][j] = v;
@@ -412,7 +415,8 @@ static int spmv_grid(int64_t nrows, int B) {
 // at most kSpmvBlocks tiles in all; every tile runs once per instance chunk.
 static Blocks map_blocks(const DevMap& M, int B) {
     Blocks bl{};
-    bl.nchunk = (B + kChunk - 1) / kChunk;
+    const int ch = B <= 2 ? 2 : 4;
+    bl.nchunk = (B + ch - 1) / ch;
     int64_t tot = 0;
     for (int i = 0; i < M.nb; i++) tot += (M.nslots[i] + kThreads - 1) / kThreads;
     const double scale = tot > kSpmvBlocks ? (double)kSpmvBlocks / (double)tot : 1.0;
@@ -432,7 +436,10 @@ static int run_map(const DevMap& M, int B, const double* in, double* out, const 
     Epi e{sub, coef, add, dotv, out};
     const Blocks bl = map_blocks(M, B);
     if (M.nb > 0) {
-        ell_kernel<<<bl.start[M.nb] * bl.nchunk, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+        if (B <= 2)
+            ell_kernel<2><<<bl.start[M.nb] * bl.nchunk, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+        else
+            ell_kernel<4><<<bl.start[M.nb] * bl.nchunk, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
         g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     }
     if (M.nlong > 0) {

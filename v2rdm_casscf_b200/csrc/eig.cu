@@ -340,8 +340,11 @@ __device__ __forceinline__ int pair_idx(int I, int J, int a) { return a < 32 ? I
 
 __global__ void __launch_bounds__(kJThreads) bj_solve_kernel(const BlockTask* __restrict__ tasks,
                                                              const PairTask* __restrict__ pt, int round, double* Ww,
-                                                             double* __restrict__ Qbuf, const int* __restrict__ bmask) {
+                                                             double* __restrict__ Qbuf, const int* __restrict__ bmask,
+                                                             const double* __restrict__ pthr,
+                                                             int* __restrict__ qskip) {
     extern __shared__ double sm[];
+    __shared__ double red[33];
     double* S = sm;
     double* Q = sm + kJ * kLd;
     const PairTask pk = pt[blockIdx.x];
@@ -355,6 +358,21 @@ __global__ void __launch_bounds__(kJThreads) bj_solve_kernel(const BlockTask* __
         S[a * kLd + bq] = w[(int64_t)pair_idx(I, J, a) * t.np + pair_idx(I, J, bq)];
     }
     __syncthreads();
+    // a pair problem already diagonal to the block's share of its tolerance
+    // is left alone: its rotation is the identity and the updates skip it
+    const int64_t qi = (t.qoff >> 12) + pk.k;
+    double off = 0.0;
+    for (int l = threadIdx.x; l < 64 * 64; l += blockDim.x)
+        if (l / 64 != l % 64) {
+            const double v = S[(l / 64) * kLd + (l % 64)];
+            off += v * v;
+        }
+    off = block_sum(off, red);
+    if (off <= pthr[pk.task]) {
+        if (threadIdx.x == 0) qskip[qi] = 1;
+        return;
+    }
+    if (threadIdx.x == 0) qskip[qi] = 0;
     // the outer block-Jacobi sweeps iterate anyway: a few inner sweeps suffice
     jacobi_smem(S, Q, 64, kPairSweeps, kJacobiRotEps);
     __syncthreads();
@@ -362,36 +380,36 @@ __global__ void __launch_bounds__(kJThreads) bj_solve_kernel(const BlockTask* __
     for (int l = threadIdx.x; l < 64 * 64; l += blockDim.x) qo[l] = Q[(l / 64) * kLd + (l % 64)];
 }
 
-// out(64x64, smem ld kLd) = opL(L) * M * R, where L and R are 64x64 row-major
-// in global memory; used for W tile = Q1^T T Q2 and V tile = T Q.
-__device__ void tile_rotate(double* T, double* Qs, const double* Q1g, const double* Q2g, bool left) {
-    // T <- T * Q2
-    for (int l = threadIdx.x; l < 4096; l += blockDim.x) Qs[(l / 64) * kLd + l % 64] = Q2g[l];
-    __syncthreads();
+// T (64x64, smem ld kLd) <- Q1^T T Q2, where Q1 and Q2 are 64x64 row-major
+// in global memory and either may be null (identity); used for W tile =
+// Q1^T T Q2 and V tile = T Q.
+__device__ void tile_rotate(double* T, double* Qs, const double* Q1g, const double* Q2g) {
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double acc[4][4] = {};
-    for (int k = 0; k < 64; k++) {
-        double av[4], bv[4];
+    if (Q2g) {
+        // T <- T * Q2
+        for (int l = threadIdx.x; l < 4096; l += blockDim.x) Qs[(l / 64) * kLd + l % 64] = Q2g[l];
+        __syncthreads();
+        double acc[4][4] = {};
+        for (int k = 0; k < 64; k++) {
+            double av[4], bv[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) av[i] = T[(ty + 16 * i) * kLd + k];
+            for (int i = 0; i < 4; i++) av[i] = T[(ty + 16 * i) * kLd + k];
 #pragma unroll
-        for (int j = 0; j < 4; j++) bv[j] = Qs[k * kLd + tx + 16 * j];
+            for (int j = 0; j < 4; j++) bv[j] = Qs[k * kLd + tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] += av[i] * bv[j];
+        }
+        __syncthreads();
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] += av[i] * bv[j];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) T[(ty + 16 * i) * kLd + tx + 16 * j] = acc[i][j];
-    if (!left) {
+            for (int j = 0; j < 4; j++) T[(ty + 16 * i) * kLd + tx + 16 * j] = acc[i][j];
         __syncthreads();
-        return;
     }
+    if (!Q1g) return;
     // T <- Q1^T * T
-    __syncthreads();
     for (int l = threadIdx.x; l < 4096; l += blockDim.x) Qs[(l / 64) * kLd + l % 64] = Q1g[l];
     __syncthreads();
     double acc2[4][4] = {};
@@ -414,39 +432,13 @@ __device__ void tile_rotate(double* T, double* Qs, const double* Q1g, const doub
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) bj_update_w_kernel(const BlockTask* __restrict__ tasks,
-                                                          const WTileTask* __restrict__ wt, int round, double* Ww,
-                                                          const double* __restrict__ Qbuf,
-                                                          const int* __restrict__ bmask) {
-    extern __shared__ double sm[];
-    double* T = sm;
-    double* Qs = sm + kJ * kLd;
-    const WTileTask w = wt[blockIdx.x];
-    if (bmask && !bmask[w.task]) return;
-    const BlockTask t = tasks[w.task];
-    const int r = round % (t.nb - 1);
-    int I1, J1, I2, J2;
-    rr_pair(t.nb, r, w.k1, I1, J1);
-    rr_pair(t.nb, r, w.k2, I2, J2);
-    double* base = Ww + t.woff;
-    for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
-        const int a = l / 64, bq = l % 64;
-        T[a * kLd + bq] = base[(int64_t)pair_idx(I1, J1, a) * t.np + pair_idx(I2, J2, bq)];
-    }
-    __syncthreads();
-    tile_rotate(T, Qs, Qbuf + t.qoff + (int64_t)w.k1 * 4096, Qbuf + t.qoff + (int64_t)w.k2 * 4096, true);
-    for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
-        const int a = l / 64, bq = l % 64;
-        base[(int64_t)pair_idx(I1, J1, a) * t.np + pair_idx(I2, J2, bq)] = T[a * kLd + bq];
-    }
-}
-
 // W tiles first (blockIdx.x < nwt), then V tiles: one launch per round.
 __global__ void __launch_bounds__(256) bj_update_wv_kernel(const BlockTask* __restrict__ tasks,
                                                            const WTileTask* __restrict__ wt, int nwt,
                                                            const VTileTask* __restrict__ vt, int round,
                                                            double* Ww, double* Vw, const double* __restrict__ Qbuf,
-                                                           const int* __restrict__ bmask) {
+                                                           const int* __restrict__ bmask,
+                                                           const int* __restrict__ qskip) {
     extern __shared__ double sm[];
     double* T = sm;
     double* Qs = sm + kJ * kLd;
@@ -454,6 +446,8 @@ __global__ void __launch_bounds__(256) bj_update_wv_kernel(const BlockTask* __re
         const WTileTask w = wt[blockIdx.x];
         if (bmask && !bmask[w.task]) return;
         const BlockTask t = tasks[w.task];
+        const bool s1 = qskip[(t.qoff >> 12) + w.k1] != 0, s2 = qskip[(t.qoff >> 12) + w.k2] != 0;
+        if (s1 && s2) return;
         const int r = round % (t.nb - 1);
         int I1, J1, I2, J2;
         rr_pair(t.nb, r, w.k1, I1, J1);
@@ -464,7 +458,8 @@ __global__ void __launch_bounds__(256) bj_update_wv_kernel(const BlockTask* __re
             T[a * kLd + bq] = base[(int64_t)pair_idx(I1, J1, a) * t.np + pair_idx(I2, J2, bq)];
         }
         __syncthreads();
-        tile_rotate(T, Qs, Qbuf + t.qoff + (int64_t)w.k1 * 4096, Qbuf + t.qoff + (int64_t)w.k2 * 4096, true);
+        tile_rotate(T, Qs, s1 ? nullptr : Qbuf + t.qoff + (int64_t)w.k1 * 4096,
+                    s2 ? nullptr : Qbuf + t.qoff + (int64_t)w.k2 * 4096);
         for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
             const int a = l / 64, bq = l % 64;
             base[(int64_t)pair_idx(I1, J1, a) * t.np + pair_idx(I2, J2, bq)] = T[a * kLd + bq];
@@ -474,6 +469,7 @@ __global__ void __launch_bounds__(256) bj_update_wv_kernel(const BlockTask* __re
     const VTileTask v = vt[blockIdx.x - nwt];
     if (bmask && !bmask[v.task]) return;
     const BlockTask t = tasks[v.task];
+    if (qskip[(t.qoff >> 12) + v.k]) return;
     int I, J;
     rr_pair(t.nb, round % (t.nb - 1), v.k, I, J);
     double* base = Vw + t.woff;
@@ -483,33 +479,7 @@ __global__ void __launch_bounds__(256) bj_update_wv_kernel(const BlockTask* __re
         T[a * kLd + bq] = base[(int64_t)(r0 + a) * t.np + pair_idx(I, J, bq)];
     }
     __syncthreads();
-    tile_rotate(T, Qs, nullptr, Qbuf + t.qoff + (int64_t)v.k * 4096, false);
-    for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
-        const int a = l / 64, bq = l % 64;
-        base[(int64_t)(r0 + a) * t.np + pair_idx(I, J, bq)] = T[a * kLd + bq];
-    }
-}
-
-__global__ void __launch_bounds__(256) bj_update_v_kernel(const BlockTask* __restrict__ tasks,
-                                                          const VTileTask* __restrict__ vt, int round, double* Vw,
-                                                          const double* __restrict__ Qbuf,
-                                                          const int* __restrict__ bmask) {
-    extern __shared__ double sm[];
-    double* T = sm;
-    double* Qs = sm + kJ * kLd;
-    const VTileTask v = vt[blockIdx.x];
-    if (bmask && !bmask[v.task]) return;
-    const BlockTask t = tasks[v.task];
-    int I, J;
-    rr_pair(t.nb, round % (t.nb - 1), v.k, I, J);
-    double* base = Vw + t.woff;
-    const int r0 = v.chunk * 64;
-    for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
-        const int a = l / 64, bq = l % 64;
-        T[a * kLd + bq] = base[(int64_t)(r0 + a) * t.np + pair_idx(I, J, bq)];
-    }
-    __syncthreads();
-    tile_rotate(T, Qs, nullptr, Qbuf + t.qoff + (int64_t)v.k * 4096, false);
+    tile_rotate(T, Qs, nullptr, Qbuf + t.qoff + (int64_t)v.k * 4096);
     for (int l = threadIdx.x; l < 4096; l += blockDim.x) {
         const int a = l / 64, bq = l % 64;
         base[(int64_t)(r0 + a) * t.np + pair_idx(I, J, bq)] = T[a * kLd + bq];
@@ -543,7 +513,8 @@ __global__ void bj_rowsum_kernel(const BlockTask* __restrict__ tasks, const doub
 
 __global__ void bj_check_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ rowsum,
                                 const double* __restrict__ tols, const double* __restrict__ abs_tols,
-                                const int* __restrict__ max_sweeps, int sweeps_done, int* __restrict__ bmask) {
+                                const int* __restrict__ max_sweeps, int sweeps_done, int* __restrict__ bmask,
+                                double* __restrict__ pthr) {
     __shared__ double red[33];
     if (!bmask[blockIdx.x]) return;
     if (max_sweeps && sweeps_done >= max_sweeps[blockIdx.x]) {
@@ -560,7 +531,13 @@ __global__ void bj_check_kernel(const BlockTask* __restrict__ tasks, const doubl
     }
     off = block_sum(off, red);
     tot = block_sum(tot, red);
-    if (threadIdx.x == 0 && !(off > fmax(tol * tol * tot, atol * atol))) bmask[blockIdx.x] = 0;
+    const double lim = fmax(tol * tol * tot, atol * atol);
+    if (threadIdx.x == 0) {
+        if (!(off > lim)) bmask[blockIdx.x] = 0;
+        // per pair problem: the block's limit shared over the nb (nb - 1) / 2
+        // pair problems of a sweep
+        pthr[blockIdx.x] = lim / (0.5 * (double)t.nb * (double)(t.nb - 1));
+    }
 }
 
 __global__ void count_open_kernel(int n, const int* __restrict__ bmask, int* out) {
@@ -902,8 +879,6 @@ void set_smem_attrs() {
     if (done) return;
     cudaFuncSetAttribute(small_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
     cudaFuncSetAttribute(bj_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
-    cudaFuncSetAttribute(bj_update_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
-    cudaFuncSetAttribute(bj_update_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
     cudaFuncSetAttribute(bj_update_wv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
     done = true;
 }
@@ -940,44 +915,29 @@ void launch_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, cons
 }
 
 void launch_bj_solve(const BlockTask* tasks, const PairTask* pt, int npt, int round, double* Ww, double* Qbuf,
-                     const int* bmask, cudaStream_t s) {
+                     const int* bmask, const double* pthr, int* qskip, cudaStream_t s) {
     if (npt == 0) return;
     set_smem_attrs();
-    bj_solve_kernel<<<npt, kJThreads, kJacobiSmem, s>>>(tasks, pt, round, Ww, Qbuf, bmask);
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-}
-
-void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, int round, double* Ww,
-                        const double* Qbuf, const int* bmask, cudaStream_t s) {
-    if (nwt == 0) return;
-    set_smem_attrs();
-    bj_update_w_kernel<<<nwt, 256, kJacobiSmem, s>>>(tasks, wt, round, Ww, Qbuf, bmask);
+    bj_solve_kernel<<<npt, kJThreads, kJacobiSmem, s>>>(tasks, pt, round, Ww, Qbuf, bmask, pthr, qskip);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_bj_update_wv(const BlockTask* tasks, const WTileTask* wt, int nwt, const VTileTask* vt, int nvt, int round,
-                         double* Ww, double* Vw, const double* Qbuf, const int* bmask, cudaStream_t s) {
+                         double* Ww, double* Vw, const double* Qbuf, const int* bmask, const int* qskip,
+                         cudaStream_t s) {
     if (nwt + nvt == 0) return;
     set_smem_attrs();
-    bj_update_wv_kernel<<<nwt + nvt, 256, kJacobiSmem, s>>>(tasks, wt, nwt, vt, round, Ww, Vw, Qbuf, bmask);
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-}
-
-void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, int round, double* Vw,
-                        const double* Qbuf, const int* bmask, cudaStream_t s) {
-    if (nvt == 0) return;
-    set_smem_attrs();
-    bj_update_v_kernel<<<nvt, 256, kJacobiSmem, s>>>(tasks, vt, round, Vw, Qbuf, bmask);
+    bj_update_wv_kernel<<<nwt + nvt, 256, kJacobiSmem, s>>>(tasks, wt, nwt, vt, round, Ww, Vw, Qbuf, bmask, qskip);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_bj_check(const BlockTask* tasks, int ntasks, int max_np, const double* Ww, const double* tol,
                      const double* abs_tol, const int* max_sweeps, int sweeps_done, double* rowsum, int* bmask,
-                     int* n_open, cudaStream_t s) {
+                     double* pthr, int* n_open, cudaStream_t s) {
     if (ntasks == 0) return;
     bj_rowsum_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, Ww, bmask, rowsum);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    bj_check_kernel<<<ntasks, 256, 0, s>>>(tasks, rowsum, tol, abs_tol, max_sweeps, sweeps_done, bmask);
+    bj_check_kernel<<<ntasks, 256, 0, s>>>(tasks, rowsum, tol, abs_tol, max_sweeps, sweeps_done, bmask, pthr);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     count_open_kernel<<<1, 1024, 0, s>>>(ntasks, bmask, n_open);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);

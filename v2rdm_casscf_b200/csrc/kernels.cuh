@@ -132,20 +132,21 @@ struct WTileTask {
 struct VTileTask {
     int task, chunk, k;
 };
+// One round of the block Jacobi: each 64x64 pair problem is diagonalised
+// into Qbuf unless its off-diagonal norm^2 is at most pthr[task] (then
+// qskip marks its rotation as the identity and the update leaves it out).
 void launch_bj_solve(const BlockTask* tasks, const PairTask* pt, int npt, int round, double* Ww, double* Qbuf,
-                     const int* bmask, cudaStream_t s);
-void launch_bj_update_w(const BlockTask* tasks, const WTileTask* wt, int nwt, int round, double* Ww,
-                        const double* Qbuf, const int* bmask, cudaStream_t s);
+                     const int* bmask, const double* pthr, int* qskip, cudaStream_t s);
 void launch_bj_update_wv(const BlockTask* tasks, const WTileTask* wt, int nwt, const VTileTask* vt, int nvt, int round,
-                         double* Ww, double* Vw, const double* Qbuf, const int* bmask, cudaStream_t s);
-void launch_bj_update_v(const BlockTask* tasks, const VTileTask* vt, int nvt, int round, double* Vw,
-                        const double* Qbuf, const int* bmask, cudaStream_t s);
+                         double* Ww, double* Vw, const double* Qbuf, const int* bmask, const int* qskip,
+                         cudaStream_t s);
 // Per-block off-diagonal and total Frobenius norms of W; sets bmask[t] = 0
 // for blocks whose off-diagonal norm is below max(tol[t] * total, abs_tol[t])
-// or that have done max_sweeps[t] sweeps.
+// or that have done max_sweeps[t] sweeps, and pthr[t] = that limit squared
+// over the pair problems of a sweep.
 void launch_bj_check(const BlockTask* tasks, int ntasks, int max_np, const double* Ww, const double* tol,
                      const double* abs_tol, const int* max_sweeps, int sweeps_done, double* rowsum, int* bmask,
-                     int* n_open, cudaStream_t s);
+                     double* pthr, int* n_open, cudaStream_t s);
 // dx = max(lam, 0) / mu and dz = max(-lam, 0) (per block, length np; zero on padding)
 void launch_pos_weights(const BlockTask* tasks, int ntasks, const double* lam, const double* mu, const int* bmask,
                         double* dx, double* dz, cudaStream_t s);

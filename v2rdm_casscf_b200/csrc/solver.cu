@@ -386,14 +386,14 @@ class GroupRun {
         CK(cudaMemcpyAsync(bwork_.p, bjac_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
         for (int sweep = 0; sweep < max_sweeps; sweep++) {
             launch_bj_check(large_d_.p, nlarge_, max_np_, W_.p, jtol_.p, atol_.p, cap_ ? msw_.p : nullptr, sweep,
-                            rowsum_.p, bwork_.p, nact_.p + 1, s_);
+                            rowsum_.p, bwork_.p, pthr_.p, nact_.p + 1, s_);
             CK(cudaMemcpyAsync(hnact_ + 1, nact_.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s_));
             CK(cudaStreamSynchronize(s_));
             if (hnact_[1] == 0) break;
             for (int g = 0; g < max_rounds_; g++) {
-                launch_bj_solve(large_d_.p, pairs_.p, npairs_, g, W_.p, Q_.p, bwork_.p, s_);
+                launch_bj_solve(large_d_.p, pairs_.p, npairs_, g, W_.p, Q_.p, bwork_.p, pthr_.p, qskip_.p, s_);
                 launch_bj_update_wv(large_d_.p, wtiles_.p, nwtiles_, vtiles_.p, nvtiles_, g, W_.p, V_.p, Q_.p,
-                                    bwork_.p, s_);
+                                    bwork_.p, qskip_.p, s_);
             }
             sweeps_total_++;
         }
@@ -688,6 +688,8 @@ class GroupRun {
         G_.alloc(woff);
         M_.alloc(woff);
         Q_.alloc(qoff);
+        qskip_.alloc(qoff / 4096);
+        pthr_.alloc(nlarge_);
         dw_.alloc(doff);
         dz_.alloc(doff);
         jtol_.alloc(nlarge_);
@@ -756,7 +758,8 @@ class GroupRun {
     int nsmall_ = 0, nlarge_ = 0, max_np_ = 0, max_n_ = 0, max_rounds_ = 0;
     DevBuf<double> U_, W_, V_, Tm_, G_, M_, Q_, dw_, dz_, lam_, scale_, jtol_, otol_, atol_, rowsum_, erow_;
     DevBuf<unsigned long long> emax_;
-    DevBuf<int> hard_, bact_, bwork_, bref_, bupd_, bjac_, partner_, msw_, restart_;
+    DevBuf<int> hard_, bact_, bwork_, bref_, bupd_, bjac_, partner_, msw_, restart_, qskip_;
+    DevBuf<double> pthr_;
     long restarts_ = 0;
     bool cap_ = false;
     long oa_sweeps_ = 0, jacobi_blocks_ = 0;

@@ -56,7 +56,6 @@ SOLVE_CASES = {
     "synthetic_n4_s1": (4, 1, 1e-6, 1e-7, None),
     "synthetic_n5_s2": (5, 2, 1e-6, 1e-7, None),      # singlet, N = 4
     "synthetic_n5_s2_doublet": (5, 2, 1e-6, 1e-7, 5),  # doublet, N = 5
-    "synthetic_n4_s0_dqgt2": (4, 0, 1e-6, 1e-7, None, "DQGT2"),
     "synthetic_n4_s1_dqgt1": (4, 1, 1e-6, 1e-7, None, "DQGT1"),
 }
 

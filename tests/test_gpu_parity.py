@@ -201,3 +201,19 @@ def test_two_electron_d_equals_fci(v2g, n, seed):
     s.guess()
     e = s.compute_energy()
     assert abs(e - fci_two_electron_singlet(a)) <= 1e-6
+
+
+def test_h10_chain_matches_reference(v2g):
+    # the CPU-runnable workload: linear H10, 0.9 A, STO-3G RHF orbitals, all
+    # active, DQG; integrals stored with the reference's converged energy
+    from v2rdm_casscf_b200.hamiltonian import ActiveSpace
+
+    g = load(os.path.join(GOLDEN, "solve_h10_chain.npz"))
+    a = ActiveSpace(g["h"], g["L"], 5, 5, enuc=float(g["enuc"]))
+    s = v2g.V2RDMSolver.from_active_space(
+        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])))
+    s.guess()
+    e = s.compute_energy()
+    assert abs(e - float(g["e_primal"])) <= 1e-6
+    assert e < float(g["scf_energy"])  # a lower bound below the RHF energy
+    assert abs(s.result["oiter"] - int(g["oiter"])) <= 0.25 * int(g["oiter"])

@@ -139,7 +139,7 @@ def run_gpu(args):
     all_spaces = workload(args.workload, args.count)
     mine = list(range(rank, len(all_spaces), world))
     def make(maxiter):
-        opts = dict(OPTIONS)
+        opts = dict(OPTIONS, MU_UPDATE_FREQUENCY=args.mu_freq)
         if maxiter:
             opts["MAXITER"] = maxiter
         return [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
@@ -232,8 +232,10 @@ def run_gpu(args):
             "precision": "FP64 (maps, CG, projection)",
             "projection": args.projection,
             "cg_tolerance_factor": args.cg_factor,
-            "mode": "plain FP64 (reference algorithm)" if (args.projection == "exact" and args.cg_factor == 0.01)
-                    else "FP64 with adaptive projection and CG tolerance",
+            "mu_update_frequency": args.mu_freq,
+            "mode": "plain FP64 (reference algorithm and options)"
+                    if (args.projection == "exact" and args.cg_factor == 0.01 and args.mu_freq == 500)
+                    else "FP64 with adaptive projection" + (f", mu update every {args.mu_freq}" if args.mu_freq != 500 else ""),
             "warmup_steps": f"{args.warmup} batched calls capped at {args.warmup_outer} outer iterations",
             "l2": "inputs larger than L2 (no flush needed)",
             "parallelism": f"instances dealt to {world} rank(s), no exchange",
@@ -395,7 +397,9 @@ def run_reference(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": f"{args.workload}: {args.count} synthetic active spaces (see GPU arm)",
-                      "instances": args.count},
+                      "instances": args.count, "mu_update_frequency": args.mu_freq,
+                      "note": "reference CPU path (oracle/_ref) with the same options; time per outer iteration "
+                              "sampled, times the outer-iteration counts the GPU solve needed with those options"},
            "cpu_baseline": base,
            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -413,7 +417,10 @@ def main():
     ap.add_argument("--projection", default="adaptive", choices=["exact", "adaptive"])
     ap.add_argument("--cg-factor", type=float, default=0.01,
                     help="CG tolerance factor (0.01 = the reference's rule)")
-    ap.add_argument("--plain", action="store_true", help="reference algorithm: exact projection, CG factor 0.01")
+    ap.add_argument("--mu-update-frequency", dest="mu_freq", type=int, default=100,
+                    help="MU_UPDATE_FREQUENCY (the reference's default is 500)")
+    ap.add_argument("--plain", action="store_true",
+                    help="reference algorithm and options: exact projection, CG factor 0.01, mu update every 500")
     ap.add_argument("--warmup-outer", type=int, default=3, help="outer iterations per warm-up step")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-sample", type=lambda s: [int(v) for v in s.split(",")], default=[8, 12, 16, 20])
@@ -421,7 +428,7 @@ def main():
     ap.add_argument("--save-iterations", action="store_true")
     args = ap.parse_args()
     if args.plain:
-        args.projection, args.cg_factor = "exact", 0.01
+        args.projection, args.cg_factor, args.mu_freq = "exact", 0.01, 500
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -49,6 +49,18 @@ from v2rdm_casscf_b200.hamiltonian import batch_sizes, synthetic  # noqa: E402
 METRIC = "time-to-1e-6Eh v2RDM solve: mixed+warm-start vs plain FP64 GPU vs ref CPU"
 OPTIONS = dict(R_CONVERGENCE=1e-6, E_CONVERGENCE=1e-7)
 ITER_FILE = os.path.join(ROOT, "profiles", "batch256_outer_iterations.json")
+# DRAM bytes (read + write) per launch of the roofline launches, averaged over A and A^T,
+# from one ncu capture of exactly those launches (cold caches, as ncu replays them):
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:ell_kernel -c 46 --csv python bench.py --roofline-only
+# A: 437.8 MB read + 206.4 MB written; A^T: 518.5 MB + 235.4 MB (B200, 20 launches each).
+ROOFLINE_TRAFFIC = {
+    "n=20, 19 instances interleaved": {
+        "bytes_per_launch": 0.5 * ((437.8 + 206.4) + (518.5 + 235.4)) * 1e6,
+        "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same launches "
+                  "(python bench.py --roofline-only), mean of A and A^T",
+    },
+}
 
 
 def workload(name, count):
@@ -147,6 +159,14 @@ def run_gpu(args):
                 for i in mine]
 
     solvers = make(args.max_outer)
+    if args.roofline_only:
+        # the roofline launches alone (A and A^T of the largest group), for profilers
+        achieved, detail = roofline_pass(V, solvers, all_spaces, mine, dev, torch)
+        if rank == 0:
+            print(json.dumps({"roofline_only": True, "achieved_GBps": achieved, "detail": detail}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
     warm_solvers = make(args.warmup_outer) if args.warmup else []
     # the random start of the reference depends only on the layout: compute once per size
     starts = {}
@@ -253,10 +273,13 @@ def run_gpu(args):
             "peak_kind": pk_kind,
             "unit": "GB/s",
             "frac": (achieved / pk) if achieved else None,
-            "traffic": None,
+            "traffic": ROOFLINE_TRAFFIC.get(map_detail["group"], {}).get("bytes_per_launch"),
+            "traffic_source": ROOFLINE_TRAFFIC.get(map_detail["group"], {}).get("source"),
             "launches_timed": map_n,
         },
         "converged": int(sum(conv)),
+        "unconverged": [{"instance": int(mine[k]), "n": int(all_spaces[mine[k]].n), "status": int(r["status"]),
+                         "oiter": int(r["oiter"])} for k, r in enumerate(results) if r["status"] != 0],
         "wall_s": wall,
     }
     if clocks:
@@ -417,7 +440,7 @@ def main():
     ap.add_argument("--projection", default="adaptive", choices=["exact", "adaptive"])
     ap.add_argument("--cg-factor", type=float, default=0.01,
                     help="CG tolerance factor (0.01 = the reference's rule)")
-    ap.add_argument("--mu-update-frequency", dest="mu_freq", type=int, default=100,
+    ap.add_argument("--mu-update-frequency", dest="mu_freq", type=int, default=500,
                     help="MU_UPDATE_FREQUENCY (the reference's default is 500)")
     ap.add_argument("--plain", action="store_true",
                     help="reference algorithm and options: exact projection, CG factor 0.01, mu update every 500")
@@ -426,6 +449,8 @@ def main():
     ap.add_argument("--cpu-sample", type=lambda s: [int(v) for v in s.split(",")], default=[8, 12, 16, 20])
     ap.add_argument("--no-clocks", dest="clocks", action="store_false")
     ap.add_argument("--save-iterations", action="store_true")
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="run only the timed A / A^T launches of the roofline (for profiling)")
     args = ap.parse_args()
     if args.plain:
         args.projection, args.cg_factor, args.mu_freq = "exact", 0.01, 500

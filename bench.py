@@ -27,8 +27,9 @@ the batch take several GB), so no L2 flush is needed between steps.
             sample of sizes and extrapolated to the batch with the iteration
             counts of the same instances
 
-Multi-GPU (torchrun): instances are dealt round-robin to ranks (no exchange
-during the solve); value is the max over ranks.  `--impl reference` times the
+Multi-GPU (torchrun): instances are dealt to ranks by a longest-first bin-pack
+on a per-iteration cost model (v2rdm_casscf_b200/shard.py), with no exchange
+during the solve; value is the max over ranks.  `--impl reference` times the
 reference CPU path instead (rank 0 only).
 """
 import argparse
@@ -149,7 +150,10 @@ def run_gpu(args):
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(minutes=30))
     dev = local
     all_spaces = workload(args.workload, args.count)
-    mine = list(range(rank, len(all_spaces), world))
+    # instances dealt to ranks by a longest-first bin-pack on the modelled cost
+    from v2rdm_casscf_b200.shard import partition, workload_costs
+
+    mine = partition(workload_costs(all_spaces), world)[rank] if world > 1 else list(range(len(all_spaces)))
     def make(maxiter):
         opts = dict(OPTIONS, MU_UPDATE_FREQUENCY=args.mu_freq)
         if maxiter:
@@ -258,7 +262,7 @@ def run_gpu(args):
                     else "FP64 with adaptive projection" + (f", mu update every {args.mu_freq}" if args.mu_freq != 500 else ""),
             "warmup_steps": f"{args.warmup} batched calls capped at {args.warmup_outer} outer iterations",
             "l2": "inputs larger than L2 (no flush needed)",
-            "parallelism": f"instances dealt to {world} rank(s), no exchange",
+            "parallelism": f"instances bin-packed over {world} rank(s) by modelled cost, no exchange",
             "max_outer": args.max_outer or None,
         },
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -513,6 +514,7 @@ class GroupRun {
                 if (!std::isfinite(ep[b]) || !std::isfinite(ed[b]) || !std::isfinite(e_p)) {
                     res[b].status = V2G_ERR_NONFINITE;
                     active[b] = 0;
+                    report_nonfinite(b, oiter[b], mu[b], ii);
                     continue;
                 }
                 if (oiter[b] == o.maxiter) {
@@ -542,6 +544,23 @@ class GroupRun {
         cudaEventDestroy(e1);
         cudaEventDestroy(e2);
         cudaEventDestroy(e3);
+    }
+
+    // Which of y, x, z (and the CG scalars) turned non-finite, on stderr, so
+    // that a failing instance can be reproduced and traced alone.
+    void report_nonfinite(int b, int oiter, double mu, long cg_iters) {
+        double sums[3] = {0, 0, 0};
+        const DevBuf<double>* vecs[3] = {&y_, &x_, &z_};
+        const int64_t lens[3] = {nc_, nx_, nx_};
+        for (int k = 0; k < 3; k++) {
+            launch_reduce(RED_DOT, lens[k], B_, vecs[k]->p, vecs[k]->p, nullptr, nullptr, partial_.p, red_.p, s_);
+            CK(cudaMemcpyAsync(&sums[k], red_.p + b, sizeof(double), cudaMemcpyDeviceToHost, s_));
+            CK(cudaStreamSynchronize(s_));
+        }
+        std::fprintf(stderr,
+                     "v2g: instance %d of a group of %d (dimx %lld) non-finite after outer iteration %d: "
+                     "|y|^2 %g, |x|^2 %g, |z|^2 %g, mu %g, CG iterations %ld\n",
+                     b, B_, (long long)nx_, oiter, sums[0], sums[1], sums[2], mu, cg_iters);
     }
 
     long jacobi_sweeps() const { return sweeps_total_; }

@@ -68,6 +68,10 @@ typedef struct v2g_options {
                                    iteration; 0.01 is the plugin's rule (v2rdm_solver.cc:1797-1805),
                                    and values up to 0.1 trade fewer CG iterations for a few more
                                    outer ones (0.01) */
+    int spin_adapt_q2;          /* SPIN_ADAPT_Q2 (plugin.cc): Q2 as singlet / triplet blocks (0) */
+    int spin_adapt_g2;          /* SPIN_ADAPT_G2: G2 as singlet / triplet blocks; needs
+                                   constrain_spin = 0, as the plugin's maximal spin constraint
+                                   reads the unadapted G2ba block (0) */
 } v2g_options;
 
 typedef struct v2g_result {

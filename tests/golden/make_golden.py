@@ -40,6 +40,9 @@ MAP_CASES = {
     "c1_n4_dqgt1": ([4], [2], [0], "DQGT1", True, True),
     "c1_n4_dqgt2": ([4], [2], [0], "DQGT2", True, True),
     "c2_n4_doublet_dqgt": ([2, 2], [1, 0], [1, 0], "DQGT1T2", True, True),
+    # spin-adapted Q2 / G2 (SPIN_ADAPT_Q2, SPIN_ADAPT_G2); orbital energies in Pitzer order
+    "c1_n4_dqg_saq2": ([4], [2], [0], "DQG", True, True, True, False),
+    "c2v_dqg_saq2g2_nospin": ([2, 1, 1, 2], [1, 0, 0, 1], [0, 0, 0, 0], "DQG", False, True, True, True),
 }
 
 PACK_CASES = {
@@ -57,19 +60,25 @@ SOLVE_CASES = {
     "synthetic_n5_s2": (5, 2, 1e-6, 1e-7, None),      # singlet, N = 4
     "synthetic_n5_s2_doublet": (5, 2, 1e-6, 1e-7, 5),  # doublet, N = 5
     "synthetic_n4_s1_dqgt1": (4, 1, 1e-6, 1e-7, None, "DQGT1"),
+    "synthetic_n4_s0_saq2": (4, 0, 1e-6, 1e-7, None, "DQG", True),   # SPIN_ADAPT_Q2
 }
 
 
 def maps(name, spec):
-    amopi, docc, socc, pos, spin, sz = spec
+    amopi, docc, socc, pos, spin, sz = spec[:6]
+    saq2, sag2 = (spec[6], spec[7]) if len(spec) > 6 else (False, False)
+    extra = {}
+    if saq2 or sag2:
+        extra = dict(spin_adapt_q2=saq2, spin_adapt_g2=sag2, energies=np.arange(sum(amopi), dtype=float))
     r = RefSolver(amopi, docc, soccpi=socc, positivity=pos, constrain_spin=spin, constrain_sz=sz,
-                  multiplicity=sum(socc) + 1)
+                  multiplicity=sum(socc) + 1, **extra)
     rng = np.random.default_rng(12345)
     u = rng.standard_normal(r.dimx)
     w = rng.standard_normal(r.ncon)
     r.build_constraints()
     np.savez_compressed(os.path.join(HERE, f"maps_{name}.npz"), amopi=amopi, doccpi=docc, soccpi=socc,
                         positivity=pos, constrain_spin=spin, constrain_sz=sz, dimx=r.dimx, ncon=r.ncon,
+                        spin_adapt_q2=saq2, spin_adapt_g2=sag2,
                         block_dims=r.block_dims, u=u, w=w, Au=r.Au(u), ATw=r.ATu(w), b=r.get("b"))
 
 
@@ -122,15 +131,16 @@ def pack(name, spec):
 def solve(name, spec):
     n, seed, rc, ec, electrons = spec[:5]
     pos = spec[5] if len(spec) > 5 else "DQG"
+    saq2 = bool(spec[6]) if len(spec) > 6 else False
     a = synthetic(n, seed, electrons=electrons)
-    r = RefSolver([n], [a.nb], soccpi=[a.na - a.nb], multiplicity=a.multiplicity, positivity=pos,
+    r = RefSolver([n], [a.nb], soccpi=[a.na - a.nb], multiplicity=a.multiplicity, positivity=pos, spin_adapt_q2=saq2,
                   r_convergence=rc, e_convergence=ec)
     r.set_integrals(a.oei_packed, a.qmo, a.nq)
     r.guess()
     r.build_constraints()
     out = r.solve(trace_cap=100000)
     np.savez_compressed(os.path.join(HERE, f"solve_{name}.npz"), n=n, seed=seed, r_conv=rc, e_conv=ec,
-                        electrons=a.na + a.nb, positivity=pos,
+                        electrons=a.na + a.nb, positivity=pos, spin_adapt_q2=saq2,
                         e_primal=out["e_primal"], e_dual=out["e_dual"], ep=out["ep"], ed=out["ed"],
                         oiter=out["oiter"], iiter=out["iiter"], converged=out["converged"], trace=out["trace"],
                         x=r.get("x"), y=r.get("y"), z=r.get("z"))

@@ -17,6 +17,8 @@ def make_solver(V, g, **kw):
     na, nb = int(docc.sum() + socc.sum()), int(docc.sum())
     opts = dict(POSITIVITY=str(g["positivity"]), CONSTRAIN_SPIN=bool(g["constrain_spin"]),
                 CONSTRAIN_SZ=bool(g["constrain_sz"]))
+    if "spin_adapt_q2" in g:
+        opts.update(SPIN_ADAPT_Q2=bool(g["spin_adapt_q2"]), SPIN_ADAPT_G2=bool(g["spin_adapt_g2"]))
     return V.V2RDMSolver(g["amopi"].tolist(), na, nb, int(socc.sum()) + 1, options=opts, **kw)
 
 

@@ -96,6 +96,42 @@ def test_constraint_table_matches_oracle(v2g, ref, spec):
     assert np.abs(A.T @ w - t).max() <= 1e-13 * np.abs(t).max()
 
 
+@pytest.mark.parametrize("spec", [
+    ([4], 2, "DQG", True, False, True), ([5], 2, "DQG", True, True, False), ([3, 2], 2, "DQG", True, False, True),
+    ([2, 2, 1, 1], 3, "DQG", True, True, False), ([5], 2, "DG", False, True, False),
+])
+def test_spin_adapted_tables_match_oracle(v2g, ref, spec):
+    # SPIN_ADAPT_Q2 / SPIN_ADAPT_G2 (q2.cc:260-468, g2.cc:235-455); the oracle's
+    # orbital energies are given in Pitzer order, the order the layout assumes
+    amopi, nb, pos, saq2, sag2, spin = spec
+    docc, left = [], nb
+    for a in amopi:
+        docc.append(min(a, left))
+        left -= docc[-1]
+    r = ref.RefSolver(amopi, docc, positivity=pos, constrain_spin=spin, energies=np.arange(sum(amopi), dtype=float),
+                      spin_adapt_q2=saq2, spin_adapt_g2=sag2)
+    s = v2g.V2RDMSolver(amopi, nb, nb, 1, options=dict(POSITIVITY=pos, CONSTRAIN_SPIN=spin, SPIN_ADAPT_Q2=saq2,
+                                                        SPIN_ADAPT_G2=sag2))
+    assert (s.dimx, s.nconstraints) == (r.dimx, r.ncon)
+    assert list(s.dimensions) == list(r.block_dims)
+    A = csr_of(s)
+    rng = np.random.default_rng(7)
+    u, w = rng.standard_normal(s.dimx), rng.standard_normal(s.nconstraints)
+    a, t = r.Au(u), r.ATu(w)
+    assert np.abs(A @ u - a).max() <= 1e-13 * np.abs(a).max()
+    assert np.abs(A.T @ w - t).max() <= 1e-13 * np.abs(t).max()
+    r.build_constraints()
+    assert np.array_equal(s.b, r.get("b"))
+
+
+def test_spin_adaptation_restrictions(v2g):
+    # v2rdm_solver.cc:538-558: not with T1/T2, not for S = M != 0
+    with pytest.raises(v2g.V2GError):
+        v2g.V2RDMSolver([4], 2, 2, options=dict(POSITIVITY="DQGT2", SPIN_ADAPT_Q2=True))
+    with pytest.raises(v2g.V2GError):
+        v2g.V2RDMSolver([4], 3, 1, 3, options=dict(SPIN_ADAPT_G2=True, CONSTRAIN_SPIN=False))
+
+
 def test_invalid_options_fail_loudly(v2g):
     with pytest.raises(v2g.V2GError):
         v2g.V2RDMSolver([4], 2, 2, options=dict(POSITIVITY="DQX"))

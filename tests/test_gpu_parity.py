@@ -60,15 +60,17 @@ def _solve_golden(v2g, name):
     g = load(os.path.join(GOLDEN, f"solve_{name}.npz"))
     a = synthetic(int(g["n"]), int(g["seed"]), electrons=int(g["electrons"]))
     pos = str(g["positivity"]) if "positivity" in g else "DQG"
+    saq2 = bool(g["spin_adapt_q2"]) if "spin_adapt_q2" in g else False
     s = v2g.V2RDMSolver.from_active_space(
-        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]), POSITIVITY=pos),
+        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]), POSITIVITY=pos,
+                        SPIN_ADAPT_Q2=saq2),
         record_trace=True)
     s.guess()
     return g, s
 
 
 @pytest.mark.parametrize("name", ["synthetic_n4_s0", "synthetic_n4_s1", "synthetic_n5_s2", "synthetic_n5_s2_doublet",
-                                  "synthetic_n4_s1_dqgt1"])
+                                  "synthetic_n4_s1_dqgt1", "synthetic_n4_s0_saq2"])
 def test_solve_matches_reference(v2g, name):
     # Converged energies agree; individual iterations do not have to, since CG
     # on A A^T from the random start amplifies rounding (a sparse vs dense

@@ -55,6 +55,8 @@ class Options(ctypes.Structure):
         ("profile", ctypes.c_int),
         ("adaptive_projection", ctypes.c_int),
         ("cg_tolerance_factor", ctypes.c_double),
+        ("spin_adapt_q2", ctypes.c_int),
+        ("spin_adapt_g2", ctypes.c_int),
     ]
 
 
@@ -182,6 +184,8 @@ DEFAULT_OPTIONS = dict(
     CG_MAXITER=10000,
     TAU_PARAMETER=1.0,
     MU_UPDATE_FREQUENCY=500,
+    SPIN_ADAPT_Q2=False,
+    SPIN_ADAPT_G2=False,
 )
 
 
@@ -230,6 +234,8 @@ class V2RDMSolver:
             raise ValueError("projection is 'exact' or 'adaptive'")
         o.adaptive_projection = int(projection == "adaptive")
         o.cg_tolerance_factor = float(cg_tolerance_factor)
+        o.spin_adapt_q2 = int(bool(opts["SPIN_ADAPT_Q2"]))
+        o.spin_adapt_g2 = int(bool(opts["SPIN_ADAPT_G2"]))
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)

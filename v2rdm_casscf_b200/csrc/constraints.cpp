@@ -313,6 +313,126 @@ void rows_q2(const Layout& L, RowSink& S) {
     }
 }
 
+// q2.cc:260-468 (Q2_constraints_Au_spin_adapted): Q2 singlet block over the
+// spatial pairs and three triplet blocks (M = 0, +1, -1) over aa pairs.
+void rows_q2_spin_adapted(const Layout& L, RowSink& S) {
+    auto D2 = [&](int h, int r, int c) { return gem(L, F_D2AB, h, L.gems_ab[h], r, c); };
+    for (int trip = 0; trip < 2; trip++) {
+        // trip = 0: Q2s (gems_00); trip = 1: Q2t, M = 0 (gems_aa)
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = trip ? L.gems_aa[h] : L.gems_00[h];
+            const auto& bas = trip ? L.bas_aa[h] : L.bas_00[h];
+            const double sg = trip ? -1.0 : 1.0;
+            for (int ij = 0; ij < g; ij++) {
+                const int i = bas[ij][0], j = bas[ij][1];
+                const int ijd = L.ab(h, i, j), jid = L.ab(h, j, i);
+                for (int kl = 0; kl < g; kl++) {
+                    const int k = bas[kl][0], l = bas[kl][1];
+                    const int kld = L.ab(h, k, l), lkd = L.ab(h, l, k);
+                    S.add(gem(L, trip ? F_Q2T : F_Q2S, h, g, ij, kl), -1.0);
+                    S.add(D2(h, kld, ijd), 0.5);
+                    S.add(D2(h, lkd, ijd), 0.5 * sg);
+                    S.add(D2(h, kld, jid), 0.5 * sg);
+                    S.add(D2(h, lkd, jid), 0.5);
+                    if (j == l) {
+                        S.add(d1(L, F_Q1A, i, k), 0.5);
+                        S.add(d1(L, F_D1B, i, k), -0.5);
+                    }
+                    if (i == k) {
+                        S.add(d1(L, F_Q1A, l, j), 0.5);
+                        S.add(d1(L, F_D1B, l, j), -0.5);
+                    }
+                    if (j == k) {
+                        S.add(d1(L, F_Q1A, l, i), 0.5 * sg);
+                        S.add(d1(L, F_D1B, l, i), -0.5 * sg);
+                    }
+                    if (i == l) {
+                        S.add(d1(L, F_Q1A, k, j), 0.5 * sg);
+                        S.add(d1(L, F_D1B, k, j), -0.5 * sg);
+                    }
+                    S.end();
+                }
+            }
+        }
+    }
+    for (int beta = 0; beta < 2; beta++) {
+        // Q2t, M = +1 from D2aa; M = -1 from D2bb
+        const Fam fq = beta ? F_Q2TM : F_Q2TP, fd = beta ? F_D2BB : F_D2AA, fq1 = beta ? F_Q1B : F_Q1A,
+                  fd1 = beta ? F_D1B : F_D1A;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_aa[h];
+            for (int ij = 0; ij < g; ij++) {
+                const int i = L.bas_aa[h][ij][0], j = L.bas_aa[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    const int k = L.bas_aa[h][kl][0], l = L.bas_aa[h][kl][1];
+                    S.add(gem(L, fq, h, g, ij, kl), -1.0);
+                    S.add(gem(L, fd, h, g, kl, ij), 1.0);
+                    if (j == l) S.add(d1(L, fq1, i, k), 1.0);
+                    if (j == k) S.add(d1(L, fd1, l, i), 1.0);
+                    if (i == l) S.add(d1(L, fq1, j, k), -1.0);
+                    if (i == k) S.add(d1(L, fd1, l, j), -1.0);
+                    S.end();
+                }
+            }
+        }
+    }
+}
+
+// g2.cc:235-455 (G2_constraints_Au_spin_adapted): singlet and triplet
+// (M = 0, +1, -1) G2 blocks over ab pairs.
+void rows_g2_spin_adapted(const Layout& L, RowSink& S) {
+    for (int trip = 0; trip < 2; trip++) {
+        // trip = 0: G2s; trip = 1: G2t, M = 0 (the D2ab terms change sign)
+        const double sab = trip ? -0.5 : 0.5;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_ab[h];
+            for (int ij = 0; ij < g; ij++) {
+                const int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    const int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                    S.add(gem(L, trip ? F_G2T : F_G2S, h, g, ij, kl), -1.0);
+                    if (j == l) {
+                        S.add(d1(L, F_D1A, i, k), 0.5);
+                        S.add(d1(L, F_D1B, i, k), 0.5);
+                    }
+                    const int h2 = L.sym_pair(L.symmetry[i], L.symmetry[l]);
+                    if (i != l && k != j) {
+                        const double sgn = (i < l ? 1.0 : -1.0) * (k < j ? 1.0 : -1.0);
+                        const int ga = L.gems_aa[h2];
+                        S.add(gem(L, F_D2AA, h2, ga, L.aa(h2, i, l), L.aa(h2, k, j)), -0.5 * sgn);
+                        S.add(gem(L, F_D2BB, h2, ga, L.aa(h2, i, l), L.aa(h2, k, j)), -0.5 * sgn);
+                    }
+                    const int g2 = L.gems_ab[h2];
+                    S.add(gem(L, F_D2AB, h2, g2, L.ab(h2, i, l), L.ab(h2, j, k)), sab);
+                    S.add(gem(L, F_D2AB, h2, g2, L.ab(h2, l, i), L.ab(h2, k, j)), sab);
+                    S.end();
+                }
+            }
+        }
+    }
+    for (int beta = 0; beta < 2; beta++) {
+        // G2t, M = +1: D1a(i,k) d_jl - D2ab(il,kj); M = -1: D1b(i,k) d_jl - D2ab(li,jk)
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_ab[h];
+            for (int ij = 0; ij < g; ij++) {
+                const int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    const int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                    S.add(gem(L, beta ? F_G2TM : F_G2TP, h, g, ij, kl), -1.0);
+                    if (j == l) S.add(d1(L, beta ? F_D1B : F_D1A, i, k), 1.0);
+                    const int h2 = L.sym_pair(L.symmetry[i], L.symmetry[l]);
+                    const int g2 = L.gems_ab[h2];
+                    if (!beta)
+                        S.add(gem(L, F_D2AB, h2, g2, L.ab(h2, i, l), L.ab(h2, k, j)), -1.0);
+                    else
+                        S.add(gem(L, F_D2AB, h2, g2, L.ab(h2, l, i), L.ab(h2, j, k)), -1.0);
+                    S.end();
+                }
+            }
+        }
+    }
+}
+
 // g2.cc:1061-1260 (G2_constraints_Au, not spin adapted)
 void rows_g2(const Layout& L, RowSink& S) {
     // G2ab: -G2ab(ij,kl) + d_jl D1a(i,k) - D2ab(il,kj)
@@ -570,8 +690,8 @@ std::string build_A(const Layout& L, Csr& A) {
     RowSink S(A);
     rows_d2(L, S);
     if (L.opt.constrain_spin) rows_spin(L, S);
-    if (L.opt.constrain_q2) rows_q2(L, S);
-    if (L.opt.constrain_g2) rows_g2(L, S);
+    if (L.opt.constrain_q2) (L.opt.spin_adapt_q2 ? rows_q2_spin_adapted : rows_q2)(L, S);
+    if (L.opt.constrain_g2) (L.opt.spin_adapt_g2 ? rows_g2_spin_adapted : rows_g2)(L, S);
     if (L.opt.constrain_t1) rows_t1(L, S);
     if (L.opt.constrain_t2) rows_t2(L, S);
     A.nrows = S.rows();
@@ -628,7 +748,7 @@ void build_b(const Layout& L, std::vector<double>& b) {
         }
         if (L.opt.constrain_g2) o += 2 * (int64_t)L.gems_ab[0];
     }
-    if (L.opt.constrain_q2) {
+    if (L.opt.constrain_q2 && !L.opt.spin_adapt_q2) {  // spin-adapted Q2 rows have b = 0
         // v2rdm_solver.cc:2650-2695
         for (int h = 0; h < L.nirrep; h++) {
             const int g = L.gems_ab[h];

@@ -59,9 +59,18 @@ static void build_geminals(Layout& L) {
         L.gems_ab[h] = (int)L.bas_ab[h].size();
         L.gems_aa[h] = (int)L.bas_aa[h].size();
     }
-    // gems_00: unordered pairs i >= j per irrep (basis.cc:626-652)
+    // spatial pairs i >= j per irrep (basis.cc:626-652), numbered in the
+    // orbitals' energy order, taken here as Pitzer order
+    L.bas_00.assign(H, {});
+    L.ibas_00.assign(H, std::vector<int>(n * n, -1));
     for (int i = 0; i < n; i++)
-        for (int j = 0; j <= i; j++) L.gems_00[L.sym_pair(L.symmetry[i], L.symmetry[j])]++;
+        for (int j = 0; j <= i; j++) {
+            const int h = L.sym_pair(L.symmetry[i], L.symmetry[j]);
+            L.ibas_00[h][i * n + j] = L.gems_00[h];
+            L.ibas_00[h][j * n + i] = L.gems_00[h];
+            L.bas_00[h].push_back({i, j});
+            L.gems_00[h]++;
+        }
 }
 
 static void build_triplets(Layout& L) {
@@ -108,10 +117,15 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
                          int multiplicity, Layout& L) {
     if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) return "nirrep must be 1, 2, 4 or 8";
     if ((int)amopi.size() != nirrep) return "amopi must have nirrep entries";
-    if (opt.constrain_t1 || opt.constrain_t2) {
-        // (spin-adapted Q2/G2 are not offered, so the t1/t2 restriction of
-        // v2rdm_solver.cc:538-545 never triggers)
-    }
+    // restrictions of v2rdm_solver.cc:538-558
+    if ((opt.constrain_t1 || opt.constrain_t2) && (opt.spin_adapt_q2 || opt.spin_adapt_g2))
+        return "If constraining T1/T2, Q2 and G2 cannot currently be spin adapted.";
+    if ((opt.spin_adapt_q2 || opt.spin_adapt_g2) && multiplicity != 1)
+        return "Q2 / G2 are not spin adapted for S = M != 0";
+    // the maximal spin constraint reads the G2ba block (spin.cc:470-489),
+    // which the spin-adapted G2 layout does not have
+    if (opt.spin_adapt_g2 && opt.constrain_spin && opt.constrain_g2)
+        return "SPIN_ADAPT_G2 needs CONSTRAIN_SPIN false (the maximal spin constraint uses the G2ba block)";
     L = Layout();
     L.opt = opt;
     L.nirrep = nirrep;
@@ -154,15 +168,25 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
     place(F_D1B, amp, 1);
     place(F_Q1A, amp, 1);
     place(F_Q1B, amp, 1);
-    if (opt.constrain_q2) {
+    if (opt.constrain_q2 && !opt.spin_adapt_q2) {
         place(F_Q2AB, gab, 1);
         place(F_Q2AA, gaa, 1);
         place(F_Q2BB, gaa, 1);
+    } else if (opt.constrain_q2) {
+        place(F_Q2S, L.gems_00, 1);
+        place(F_Q2T, gaa, 1);
+        place(F_Q2TP, gaa, 1);
+        place(F_Q2TM, gaa, 1);
     }
-    if (opt.constrain_g2) {
+    if (opt.constrain_g2 && !opt.spin_adapt_g2) {
         place(F_G2AB, gab, 1);
         place(F_G2BA, gab, 1);
         place(F_G2AA, gab, 2);
+    } else if (opt.constrain_g2) {
+        place(F_G2S, gab, 1);
+        place(F_G2T, gab, 1);
+        place(F_G2TP, gab, 1);
+        place(F_G2TM, gab, 1);
     }
     if (opt.constrain_t1) {
         place(F_T1AAA, L.trip_aaa, 1);
@@ -196,9 +220,10 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
         if (opt.constrain_g2) m += 2 * (int64_t)gab[0];
     }
     if (opt.constrain_q2)
-        for (int h = 0; h < H; h++) m += sq(gab[h]) + 2 * sq(gaa[h]);
+        for (int h = 0; h < H; h++)
+            m += opt.spin_adapt_q2 ? sq(L.gems_00[h]) + 3 * sq(gaa[h]) : sq(gab[h]) + 2 * sq(gaa[h]);
     if (opt.constrain_g2)
-        for (int h = 0; h < H; h++) m += 2 * sq(gab[h]) + sq(2 * gab[h]);
+        for (int h = 0; h < H; h++) m += opt.spin_adapt_g2 ? 4 * sq(gab[h]) : 2 * sq(gab[h]) + sq(2 * gab[h]);
     if (opt.constrain_t1)
         for (int h = 0; h < H; h++) m += 2 * sq(L.trip_aaa[h]) + 2 * sq(L.trip_aab[h]);
     if (opt.constrain_t2)
@@ -217,15 +242,22 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
     dims(amp, 1);
     dims(amp, 1);
     dims(amp, 1);
-    if (opt.constrain_q2) {
+    if (opt.constrain_q2 && !opt.spin_adapt_q2) {
         dims(gab, 1);
+        dims(gaa, 1);
+        dims(gaa, 1);
+    } else if (opt.constrain_q2) {
+        dims(L.gems_00, 1);
+        dims(gaa, 1);
         dims(gaa, 1);
         dims(gaa, 1);
     }
-    if (opt.constrain_g2) {
+    if (opt.constrain_g2 && !opt.spin_adapt_g2) {
         dims(gab, 1);
         dims(gab, 1);
         dims(gab, 2);
+    } else if (opt.constrain_g2) {
+        for (int k = 0; k < 4; k++) dims(gab, 1);
     }
     if (opt.constrain_t1) {
         dims(L.trip_aaa, 1);

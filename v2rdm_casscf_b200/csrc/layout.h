@@ -42,6 +42,10 @@ struct Options {
     // CG tolerance = cg_tol_factor * min(eps_p, eps_d) after the first
     // iteration (0.01 in the reference, v2rdm_solver.cc:1797-1805).
     double cg_tol_factor = 0.01;
+    // SPIN_ADAPT_Q2 / SPIN_ADAPT_G2 (plugin.cc): Q2 and G2 in singlet and
+    // triplet blocks instead of spin blocks.
+    bool spin_adapt_q2 = false;
+    bool spin_adapt_g2 = false;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for
@@ -51,6 +55,8 @@ bool parse_positivity(const std::string& p, Options& o);
 enum Fam {
     F_D2AB, F_D2AA, F_D2BB, F_D200, F_D1A, F_D1B, F_Q1A, F_Q1B,
     F_Q2AB, F_Q2AA, F_Q2BB, F_G2AB, F_G2BA, F_G2AA,
+    F_Q2S, F_Q2T, F_Q2TP, F_Q2TM,  // spin-adapted Q2: singlet, triplet M = 0, +1, -1
+    F_G2S, F_G2T, F_G2TP, F_G2TM,  // spin-adapted G2
     F_T1AAA, F_T1BBB, F_T1AAB, F_T1BBA,
     F_T2AAA, F_T2BBB, F_T2AAB, F_T2BBA,
     F_COUNT
@@ -69,7 +75,8 @@ struct Layout {
 
     // geminals per irrep
     std::vector<int> gems_ab, gems_aa, gems_00;
-    std::vector<std::vector<std::array<int, 2>>> bas_ab, bas_aa;
+    std::vector<std::vector<std::array<int, 2>>> bas_ab, bas_aa, bas_00;
+    std::vector<std::vector<int>> ibas_00;            // [h][i*amo+j], spatial pairs in Pitzer order
     std::vector<std::vector<int>> ibas_ab, ibas_aa;  // [h][i*amo+j], -1 if (i,j) not in irrep h
     // triplets per irrep
     std::vector<int> trip_aaa, trip_aab, trip_aba;

@@ -43,6 +43,9 @@ MAP_CASES = {
     # spin-adapted Q2 / G2 (SPIN_ADAPT_Q2, SPIN_ADAPT_G2); orbital energies in Pitzer order
     "c1_n4_dqg_saq2": ([4], [2], [0], "DQG", True, True, True, False),
     "c2v_dqg_saq2g2_nospin": ([2, 1, 1, 2], [1, 0, 0, 1], [0, 0, 0, 0], "DQG", False, True, True, True),
+    # CONSTRAIN_D3
+    "c1_n4_dqg_d3": ([4], [2], [0], "DQG", True, True, False, False, True),
+    "c2_n5_doublet_d_d3": ([3, 2], [1, 1], [1, 0], "D", True, True, False, False, True),
 }
 
 PACK_CASES = {
@@ -67,9 +70,12 @@ SOLVE_CASES = {
 def maps(name, spec):
     amopi, docc, socc, pos, spin, sz = spec[:6]
     saq2, sag2 = (spec[6], spec[7]) if len(spec) > 6 else (False, False)
+    d3 = spec[8] if len(spec) > 8 else False
     extra = {}
     if saq2 or sag2:
         extra = dict(spin_adapt_q2=saq2, spin_adapt_g2=sag2, energies=np.arange(sum(amopi), dtype=float))
+    if d3:
+        extra["constrain_d3"] = True
     r = RefSolver(amopi, docc, soccpi=socc, positivity=pos, constrain_spin=spin, constrain_sz=sz,
                   multiplicity=sum(socc) + 1, **extra)
     rng = np.random.default_rng(12345)
@@ -78,7 +84,7 @@ def maps(name, spec):
     r.build_constraints()
     np.savez_compressed(os.path.join(HERE, f"maps_{name}.npz"), amopi=amopi, doccpi=docc, soccpi=socc,
                         positivity=pos, constrain_spin=spin, constrain_sz=sz, dimx=r.dimx, ncon=r.ncon,
-                        spin_adapt_q2=saq2, spin_adapt_g2=sag2,
+                        spin_adapt_q2=saq2, spin_adapt_g2=sag2, constrain_d3=d3,
                         block_dims=r.block_dims, u=u, w=w, Au=r.Au(u), ATw=r.ATu(w), b=r.get("b"))
 
 

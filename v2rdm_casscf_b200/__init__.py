@@ -57,6 +57,7 @@ class Options(ctypes.Structure):
         ("cg_tolerance_factor", ctypes.c_double),
         ("spin_adapt_q2", ctypes.c_int),
         ("spin_adapt_g2", ctypes.c_int),
+        ("constrain_d3", ctypes.c_int),
     ]
 
 
@@ -186,6 +187,7 @@ DEFAULT_OPTIONS = dict(
     MU_UPDATE_FREQUENCY=500,
     SPIN_ADAPT_Q2=False,
     SPIN_ADAPT_G2=False,
+    CONSTRAIN_D3=False,
 )
 
 
@@ -236,6 +238,7 @@ class V2RDMSolver:
         o.cg_tolerance_factor = float(cg_tolerance_factor)
         o.spin_adapt_q2 = int(bool(opts["SPIN_ADAPT_Q2"]))
         o.spin_adapt_g2 = int(bool(opts["SPIN_ADAPT_G2"]))
+        o.constrain_d3 = int(bool(opts["CONSTRAIN_D3"]))
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)

@@ -683,6 +683,127 @@ void rows_t2(const Layout& L, RowSink& S) {
     }
 }
 
+// d3.cc:57-298 (D3_constraints_Au): the partial traces of D3 onto D2, with
+// the active electron counts, and for singlets with CONSTRAIN_SPIN the
+// D3aab = D3bba and D3aaa / D3bbb <- D3aab / D3bba relations.
+void rows_d3(const Layout& L, RowSink& S) {
+    const Gem G{L};
+    const int n = L.amo;
+    const double na = L.na, nb = L.nb;
+    auto aaa = [&](int h, int i, int j, int k) {
+        const int v = L.aaa(h, i, j, k);
+        if (v < 0) throw std::logic_error("constraint row refers to a missing triplet");
+        return v;
+    };
+    auto aab = [&](int h, int i, int j, int k) {
+        const int v = L.aab(h, i, j, k);
+        if (v < 0) throw std::logic_error("constraint row refers to a missing triplet");
+        return v;
+    };
+    // D3aaa -> D2aa (na > 2), D3bbb -> D2bb (nb > 2)
+    for (int beta = 0; beta < 2; beta++) {
+        const double ne = beta ? nb : na;
+        if (!(ne > 2)) continue;
+        const Fam f2 = beta ? F_D2BB : F_D2AA, f3 = beta ? F_D3BBB : F_D3AAA;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_aa[h];
+            for (int ij = 0; ij < g; ij++) {
+                const int i = L.bas_aa[h][ij][0], j = L.bas_aa[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    const int k = L.bas_aa[h][kl][0], l = L.bas_aa[h][kl][1];
+                    S.add(gem(L, f2, h, g, ij, kl), ne - 2.0);
+                    for (int p = 0; p < n; p++) {
+                        if (i == p || j == p || k == p || l == p) continue;
+                        const int h2 = L.sym_pair(h, L.symmetry[p]);
+                        const int s = ((p < i) ^ (p < j) ^ (p < k) ^ (p < l)) ? -1 : 1;
+                        S.add(G.at(f3, h2, L.trip_aaa[h2], aaa(h2, i, j, p), aaa(h2, k, l, p)), -(double)s);
+                    }
+                    S.end();
+                }
+            }
+        }
+    }
+    // D3aab -> D2aa (times nb), D3bba -> D2bb (times na)
+    for (int beta = 0; beta < 2; beta++) {
+        const double ne = beta ? na : nb;
+        const Fam f2 = beta ? F_D2BB : F_D2AA, f3 = beta ? F_D3BBA : F_D3AAB;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_aa[h];
+            for (int ij = 0; ij < g; ij++) {
+                const int i = L.bas_aa[h][ij][0], j = L.bas_aa[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    const int k = L.bas_aa[h][kl][0], l = L.bas_aa[h][kl][1];
+                    S.add(gem(L, f2, h, g, ij, kl), ne);
+                    for (int p = 0; p < n; p++) {
+                        const int h2 = L.sym_pair(h, L.symmetry[p]);
+                        S.add(G.at(f3, h2, L.trip_aab[h2], aab(h2, i, j, p), aab(h2, k, l, p)), -1.0);
+                    }
+                    S.end();
+                }
+            }
+        }
+    }
+    // D3aab -> D2ab (na > 1), D3bba -> D2ab (nb > 1)
+    for (int beta = 0; beta < 2; beta++) {
+        const double ne = beta ? nb : na;
+        if (!(ne > 1)) continue;
+        const Fam f3 = beta ? F_D3BBA : F_D3AAB;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int g = L.gems_ab[h];
+            for (int ij = 0; ij < g; ij++) {
+                const int i = L.bas_ab[h][ij][0], j = L.bas_ab[h][ij][1];
+                for (int kl = 0; kl < g; kl++) {
+                    const int k = L.bas_ab[h][kl][0], l = L.bas_ab[h][kl][1];
+                    S.add(gem(L, F_D2AB, h, g, ij, kl), ne - 1.0);
+                    // alpha pair (i, p) with beta j; beta: beta pair (j, p) with alpha i
+                    const int a = beta ? j : i, c = beta ? l : k;
+                    const int o1 = beta ? i : j, o2 = beta ? k : l;
+                    for (int p = 0; p < n; p++) {
+                        if (a == p || c == p) continue;
+                        const int h2 = L.sym_pair(h, L.symmetry[p]);
+                        const int s = ((p < a) ^ (p < c)) ? -1 : 1;
+                        S.add(G.at(f3, h2, L.trip_aab[h2], aab(h2, a, p, o1), aab(h2, c, p, o2)), -(double)s);
+                    }
+                    S.end();
+                }
+            }
+        }
+    }
+    if (!(L.opt.constrain_spin && L.singlet())) return;
+    // D3aab = D3bba
+    for (int h = 0; h < L.nirrep; h++) {
+        const int t = L.trip_aab[h];
+        for (int r = 0; r < t; r++)
+            for (int c = 0; c < t; c++) {
+                S.add(G.at(F_D3AAB, h, t, r, c), 1.0);
+                S.add(G.at(F_D3BBA, h, t, r, c), -1.0);
+                S.end();
+            }
+    }
+    // D3aaa <- D3aab, D3bbb <- D3bba: D3aaa(pqr,stu) - 1/3 sum of the nine
+    // antisymmetrised D3aab elements
+    for (int beta = 0; beta < 2; beta++) {
+        const Fam f3 = beta ? F_D3BBB : F_D3AAA, fm = beta ? F_D3BBA : F_D3AAB;
+        for (int h = 0; h < L.nirrep; h++) {
+            const int t = L.trip_aaa[h], tb = L.trip_aab[h];
+            for (int r = 0; r < t; r++) {
+                const int p = L.bas_aaa[h][r][0], q = L.bas_aaa[h][r][1], rr = L.bas_aaa[h][r][2];
+                const int row[3] = {aab(h, p, q, rr), aab(h, p, rr, q), aab(h, q, rr, p)};
+                const double rs[3] = {1.0, -1.0, 1.0};
+                for (int c = 0; c < t; c++) {
+                    const int s_ = L.bas_aaa[h][c][0], tt = L.bas_aaa[h][c][1], u = L.bas_aaa[h][c][2];
+                    const int col[3] = {aab(h, s_, tt, u), aab(h, s_, u, tt), aab(h, tt, u, s_)};
+                    const double cs[3] = {1.0, -1.0, 1.0};
+                    S.add(G.at(f3, h, t, r, c), 1.0);
+                    for (int x = 0; x < 3; x++)
+                        for (int y = 0; y < 3; y++) S.add(G.at(fm, h, tb, row[x], col[y]), -(1.0 / 3.0) * rs[x] * cs[y]);
+                    S.end();
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 
 std::string build_A(const Layout& L, Csr& A) {
@@ -694,6 +815,7 @@ std::string build_A(const Layout& L, Csr& A) {
     if (L.opt.constrain_g2) (L.opt.spin_adapt_g2 ? rows_g2_spin_adapted : rows_g2)(L, S);
     if (L.opt.constrain_t1) rows_t1(L, S);
     if (L.opt.constrain_t2) rows_t2(L, S);
+    if (L.opt.constrain_d3) rows_d3(L, S);
     A.nrows = S.rows();
     A.ncols = L.dimx;
     if (A.nrows != L.ncon) return "internal error: constraint row count mismatch";

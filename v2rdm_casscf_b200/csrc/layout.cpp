@@ -143,7 +143,7 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
     if (L.amo == 0) return "empty active space";
     if (na < 0 || nb < 0 || na > L.amo || nb > L.amo) return "electron counts outside the active space";
     build_geminals(L);
-    if (opt.constrain_t1 || opt.constrain_t2) build_triplets(L);
+    if (opt.constrain_t1 || opt.constrain_t2 || opt.constrain_d3) build_triplets(L);
 
     const int H = nirrep;
     const auto& gab = L.gems_ab;
@@ -202,6 +202,12 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
         place(F_T2AAB, L.trip_aab, 1);
         place(F_T2BBA, L.trip_aab, 1);
     }
+    if (opt.constrain_d3) {  // v2rdm_solver.cc:846-862
+        place(F_D3AAA, L.trip_aaa, 1);
+        place(F_D3BBB, L.trip_aaa, 1);
+        place(F_D3AAB, L.trip_aab, 1);
+        place(F_D3BBA, L.trip_aab, 1);
+    }
     L.dimx = o;
 
     // constraint count, v2rdm_solver.cc:887-1127
@@ -228,6 +234,16 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
         for (int h = 0; h < H; h++) m += 2 * sq(L.trip_aaa[h]) + 2 * sq(L.trip_aab[h]);
     if (opt.constrain_t2)
         for (int h = 0; h < H; h++) m += 2 * sq(tsum(h)) + 2 * sq(L.trip_aab[h]);
+    if (opt.constrain_d3) {  // v2rdm_solver.cc:1046-1080, with active electron counts
+        for (int h = 0; h < H; h++) {
+            if (na > 2) m += sq(gaa[h]);
+            if (nb > 2) m += sq(gaa[h]);
+            m += 2 * sq(gaa[h]);
+            if (na > 1) m += sq(gab[h]);
+            if (nb > 1) m += sq(gab[h]);
+            if (opt.constrain_spin && L.singlet()) m += sq(L.trip_aab[h]) + 2 * sq(L.trip_aaa[h]);
+        }
+    }
     L.ncon = m;
 
     // block dimensions, v2rdm_solver.cc:1129-1270 (same order as the offsets)
@@ -270,6 +286,12 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
         for (int h = 0; h < H; h++) big[h] = tsum(h);
         dims(big, 1);
         dims(big, 1);
+        dims(L.trip_aab, 1);
+        dims(L.trip_aab, 1);
+    }
+    if (opt.constrain_d3) {
+        dims(L.trip_aaa, 1);
+        dims(L.trip_aaa, 1);
         dims(L.trip_aab, 1);
         dims(L.trip_aab, 1);
     }

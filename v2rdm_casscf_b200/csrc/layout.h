@@ -46,6 +46,8 @@ struct Options {
     // triplet blocks instead of spin blocks.
     bool spin_adapt_q2 = false;
     bool spin_adapt_g2 = false;
+    // CONSTRAIN_D3 (plugin.cc): 3-RDM positivity with its contractions to D2
+    bool constrain_d3 = false;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for
@@ -59,6 +61,7 @@ enum Fam {
     F_G2S, F_G2T, F_G2TP, F_G2TM,  // spin-adapted G2
     F_T1AAA, F_T1BBB, F_T1AAB, F_T1BBA,
     F_T2AAA, F_T2BBB, F_T2AAB, F_T2BBA,
+    F_D3AAA, F_D3BBB, F_D3AAB, F_D3BBA,
     F_COUNT
 };
 

@@ -20,3 +20,29 @@ def test_reference_two_electron_d_equals_fci(ref, n, seed):
     out = r.solve()
     assert out["converged"]
     assert abs(out["e_primal"] + a.enuc - fci_two_electron_singlet(a)) <= 1e-6
+
+
+def test_reference_three_electron_d_d3_equals_fci(ref):
+    # D plus the D3 condition is exact for three electrons (the reference's own
+    # H3 test relies on this): the doublet full-CI energy, independent of the
+    # reference, must be met
+    from tests.helpers import fci_spin_state
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a = synthetic(4, 1, electrons=3)
+    r = ref.RefSolver([4], [1], soccpi=[1], multiplicity=2, positivity="D", constrain_d3=True,
+                      r_convergence=1e-7, e_convergence=1e-8)
+    r.set_integrals(a.oei_packed, a.qmo, a.nq)
+    r.guess()
+    r.build_constraints()
+    out = r.solve()
+    assert out["converged"]
+    assert abs(out["e_primal"] + a.enuc - fci_spin_state(a, 2)) <= 1e-6
+
+
+def test_generic_fci_agrees_with_two_electron_formula():
+    from tests.helpers import fci_spin_state
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a = synthetic(4, 1, electrons=2)
+    assert abs(fci_spin_state(a, 1) - fci_two_electron_singlet(a)) <= 1e-10

@@ -219,3 +219,17 @@ def test_h10_chain_matches_reference(v2g):
     assert abs(e - float(g["e_primal"])) <= 1e-6
     assert e < float(g["scf_energy"])  # a lower bound below the RHF energy
     assert abs(s.result["oiter"] - int(g["oiter"])) <= 0.25 * int(g["oiter"])
+
+
+@pytest.mark.parametrize("n,seed", [(4, 0), (4, 1), (5, 2)])
+def test_three_electron_d_d3_equals_fci(v2g, n, seed):
+    # known answer independent of the reference: D + D3 is exact for three electrons
+    from tests.helpers import fci_spin_state
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a = synthetic(n, seed, electrons=3)
+    s = v2g.V2RDMSolver.from_active_space(
+        a, options=dict(POSITIVITY="D", CONSTRAIN_D3=True, R_CONVERGENCE=1e-7, E_CONVERGENCE=1e-8))
+    s.guess()
+    e = s.compute_energy()
+    assert abs(e - fci_spin_state(a, 2)) <= 1e-6

@@ -72,8 +72,9 @@ typedef struct v2g_options {
     int spin_adapt_g2;          /* SPIN_ADAPT_G2: G2 as singlet / triplet blocks; needs
                                    constrain_spin = 0, as the plugin's maximal spin constraint
                                    reads the unadapted G2ba block (0) */
-    int constrain_d3;           /* CONSTRAIN_D3: 3-RDM positivity and its partial traces (0);
-                                   CONSTRAIN_D4 is not offered */
+    int constrain_d3;           /* CONSTRAIN_D3: 3-RDM positivity and its partial traces (0) */
+    int constrain_d4;           /* CONSTRAIN_D4: 4-RDM positivity and its partial traces; implies
+                                   constrain_d3, as in the plugin (0) */
 } v2g_options;
 
 typedef struct v2g_result {

@@ -62,7 +62,7 @@ def lib():
         L.oref_solve.argtypes = [P, D, D, I, I, DP, DP, I]
         L.oref_set_threads.argtypes = [I]
         L.oref_set_next_energies.argtypes = [DP, I]
-        L.oref_set_next_spin_adapt.argtypes = [I, I, I]
+        L.oref_set_next_spin_adapt.argtypes = [I, I, I, I]
         L.oref_spatial_dims.restype = ctypes.c_long
         L.oref_spatial_dims.argtypes = [P, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long)]
         L.oref_pack_spatial.argtypes = [P, DP, DP]
@@ -94,9 +94,10 @@ class RefSolver:
                  multiplicity=1, positivity="DQG", constrain_spin=True, constrain_sz=True,
                  r_convergence=1e-4, e_convergence=1e-4, cg_convergence=1e-9, maxiter=10000,
                  cg_maxiter=10000, energies=None, spin_adapt_q2=False, spin_adapt_g2=False,
-                 constrain_d3=False):
+                 constrain_d3=False, constrain_d4=False):
         nirrep = len(nmopi)
-        lib().oref_set_next_spin_adapt(int(bool(spin_adapt_q2)), int(bool(spin_adapt_g2)), int(bool(constrain_d3)))
+        lib().oref_set_next_spin_adapt(int(bool(spin_adapt_q2)), int(bool(spin_adapt_g2)), int(bool(constrain_d3)),
+                                       int(bool(constrain_d4)))
         if energies is not None:  # orbital energies, all orbitals in Pitzer order
             e = np.ascontiguousarray(energies, dtype=np.float64)
             lib().oref_set_next_energies(_dptr(e), int(e.size))

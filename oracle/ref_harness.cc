@@ -46,7 +46,7 @@ SharedMatrix v2RDMSolver::GetOEI() { throw PsiException("GetOEI is not available
 void v2RDMSolver::GetTEIFromDisk() { throw PsiException("GetTEIFromDisk is not available in the oracle", __FILE__, __LINE__); }
 
 std::vector<double> g_next_eps;  // orbital energies for the next setup (Pitzer order)
-int g_next_spin_adapt[3] = {0, 0, 0};  // SPIN_ADAPT_Q2, SPIN_ADAPT_G2, CONSTRAIN_D3 for the next setup
+int g_next_spin_adapt[4] = {0, 0, 0, 0};  // SPIN_ADAPT_Q2, SPIN_ADAPT_G2, CONSTRAIN_D3, CONSTRAIN_D4 (next setup)
 
 class OracleSolver : public v2RDMSolver {
   public:
@@ -348,10 +348,11 @@ extern "C" {
 
 const char* oref_last_error() { return g_err.c_str(); }
 
-void oref_set_next_spin_adapt(int q2, int g2, int d3) {
+void oref_set_next_spin_adapt(int q2, int g2, int d3, int d4) {
     psi::v2rdm_casscf::g_next_spin_adapt[0] = q2;
     psi::v2rdm_casscf::g_next_spin_adapt[1] = g2;
     psi::v2rdm_casscf::g_next_spin_adapt[2] = d3;
+    psi::v2rdm_casscf::g_next_spin_adapt[3] = d4;
 }
 void oref_set_next_energies(const double* eps, int n) { psi::v2rdm_casscf::g_next_eps.assign(eps, eps + n); }
 long oref_spatial_dims(void* h, long* d1, long* d2) {
@@ -371,11 +372,11 @@ void* oref_create(int nirrep, const int* nmopi, const int* frzcpi, const int* rs
         hd->opts.set_num("CONSTRAIN_SPIN", constrain_spin);
         hd->opts.set_num("CONSTRAIN_SZ", constrain_sz);
         hd->opts.set_num("CONSTRAIN_D3", psi::v2rdm_casscf::g_next_spin_adapt[2]);
-        hd->opts.set_num("CONSTRAIN_D4", 0);
+        hd->opts.set_num("CONSTRAIN_D4", psi::v2rdm_casscf::g_next_spin_adapt[3]);
         hd->opts.set_num("SPIN_ADAPT_G2", psi::v2rdm_casscf::g_next_spin_adapt[1]);
         hd->opts.set_num("SPIN_ADAPT_Q2", psi::v2rdm_casscf::g_next_spin_adapt[0]);
         psi::v2rdm_casscf::g_next_spin_adapt[0] = psi::v2rdm_casscf::g_next_spin_adapt[1] = 0;
-        psi::v2rdm_casscf::g_next_spin_adapt[2] = 0;
+        psi::v2rdm_casscf::g_next_spin_adapt[2] = psi::v2rdm_casscf::g_next_spin_adapt[3] = 0;
         hd->opts.set_num("R_CONVERGENCE", r_conv);
         hd->opts.set_num("E_CONVERGENCE", e_conv);
         hd->opts.set_num("CG_CONVERGENCE", cg_conv);

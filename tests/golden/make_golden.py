@@ -46,6 +46,8 @@ MAP_CASES = {
     # CONSTRAIN_D3
     "c1_n4_dqg_d3": ([4], [2], [0], "DQG", True, True, False, False, True),
     "c2_n5_doublet_d_d3": ([3, 2], [1, 1], [1, 0], "D", True, True, False, False, True),
+    # CONSTRAIN_D4
+    "c1_n4_dqg_d4": ([4], [2], [0], "DQG", True, True, False, False, True, True),
 }
 
 PACK_CASES = {
@@ -71,11 +73,14 @@ def maps(name, spec):
     amopi, docc, socc, pos, spin, sz = spec[:6]
     saq2, sag2 = (spec[6], spec[7]) if len(spec) > 6 else (False, False)
     d3 = spec[8] if len(spec) > 8 else False
+    d4 = spec[9] if len(spec) > 9 else False
     extra = {}
     if saq2 or sag2:
         extra = dict(spin_adapt_q2=saq2, spin_adapt_g2=sag2, energies=np.arange(sum(amopi), dtype=float))
     if d3:
         extra["constrain_d3"] = True
+    if d4:
+        extra["constrain_d4"] = True
     r = RefSolver(amopi, docc, soccpi=socc, positivity=pos, constrain_spin=spin, constrain_sz=sz,
                   multiplicity=sum(socc) + 1, **extra)
     rng = np.random.default_rng(12345)
@@ -84,7 +89,7 @@ def maps(name, spec):
     r.build_constraints()
     np.savez_compressed(os.path.join(HERE, f"maps_{name}.npz"), amopi=amopi, doccpi=docc, soccpi=socc,
                         positivity=pos, constrain_spin=spin, constrain_sz=sz, dimx=r.dimx, ncon=r.ncon,
-                        spin_adapt_q2=saq2, spin_adapt_g2=sag2, constrain_d3=d3,
+                        spin_adapt_q2=saq2, spin_adapt_g2=sag2, constrain_d3=d3, constrain_d4=d4,
                         block_dims=r.block_dims, u=u, w=w, Au=r.Au(u), ATw=r.ATu(w), b=r.get("b"))
 
 

@@ -21,6 +21,8 @@ def make_solver(V, g, **kw):
         opts.update(SPIN_ADAPT_Q2=bool(g["spin_adapt_q2"]), SPIN_ADAPT_G2=bool(g["spin_adapt_g2"]))
     if "constrain_d3" in g:
         opts.update(CONSTRAIN_D3=bool(g["constrain_d3"]))
+    if "constrain_d4" in g:
+        opts.update(CONSTRAIN_D4=bool(g["constrain_d4"]))
     return V.V2RDMSolver(g["amopi"].tolist(), na, nb, int(socc.sum()) + 1, options=opts, **kw)
 
 

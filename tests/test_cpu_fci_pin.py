@@ -46,3 +46,18 @@ def test_generic_fci_agrees_with_two_electron_formula():
 
     a = synthetic(4, 1, electrons=2)
     assert abs(fci_spin_state(a, 1) - fci_two_electron_singlet(a)) <= 1e-10
+
+
+def test_reference_four_electron_d_d4_equals_fci(ref):
+    # D with the D3 and D4 conditions is exact for four electrons
+    from tests.helpers import fci_spin_state
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a = synthetic(4, 1, electrons=4)
+    r = ref.RefSolver([4], [2], positivity="D", constrain_d4=True, r_convergence=1e-7, e_convergence=1e-8)
+    r.set_integrals(a.oei_packed, a.qmo, a.nq)
+    r.guess()
+    r.build_constraints()
+    out = r.solve()
+    assert out["converged"]
+    assert abs(out["e_primal"] + a.enuc - fci_spin_state(a, 1)) <= 1e-6

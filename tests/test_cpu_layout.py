@@ -152,6 +152,35 @@ def test_d3_tables_match_oracle(v2g, ref, spec):
     assert np.array_equal(s.b, r.get("b"))
 
 
+@pytest.mark.parametrize("spec", [
+    ([4], 2, 2, 1, "DQG", True), ([5], 3, 2, 2, "DQG", True), ([6], 4, 4, 1, "D", False),
+    ([2, 2, 1, 1], 3, 3, 1, "DQG", True), ([5], 4, 1, 4, "D", True),
+])
+def test_d4_tables_match_oracle(v2g, ref, spec):
+    # CONSTRAIN_D4 (d4.cc:55-312, quartets basis.cc:758-904), including the two
+    # empty blocks the reference's constraint count adds at the end
+    amopi, na, nb, mult, pos, spin = spec
+    docc, socc, lb, ls = [], [], nb, na - nb
+    for a in amopi:
+        docc.append(min(a, lb))
+        lb -= docc[-1]
+        socc.append(min(a - docc[-1], ls))
+        ls -= socc[-1]
+    r = ref.RefSolver(amopi, docc, soccpi=socc, multiplicity=mult, positivity=pos, constrain_spin=spin,
+                      constrain_d4=True)
+    s = v2g.V2RDMSolver(amopi, na, nb, mult, options=dict(POSITIVITY=pos, CONSTRAIN_SPIN=spin, CONSTRAIN_D4=True))
+    assert (s.dimx, s.nconstraints) == (r.dimx, r.ncon)
+    assert list(s.dimensions) == list(r.block_dims)
+    A = csr_of(s)
+    rng = np.random.default_rng(13)
+    u, w = rng.standard_normal(s.dimx), rng.standard_normal(s.nconstraints)
+    a, t = r.Au(u), r.ATu(w)
+    assert np.abs(A @ u - a).max() <= 1e-13 * np.abs(a).max()
+    assert np.abs(A.T @ w - t).max() <= 1e-13 * np.abs(t).max()
+    r.build_constraints()
+    assert np.array_equal(s.b, r.get("b"))
+
+
 def test_spin_adaptation_restrictions(v2g):
     # v2rdm_solver.cc:538-558: not with T1/T2, not for S = M != 0
     with pytest.raises(v2g.V2GError):

@@ -233,3 +233,17 @@ def test_three_electron_d_d3_equals_fci(v2g, n, seed):
     s.guess()
     e = s.compute_energy()
     assert abs(e - fci_spin_state(a, 2)) <= 1e-6
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_four_electron_d_d4_equals_fci(v2g, seed):
+    # known answer independent of the reference: D + D3 + D4 is exact for four electrons
+    from tests.helpers import fci_spin_state
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a = synthetic(4, seed, electrons=4)
+    s = v2g.V2RDMSolver.from_active_space(
+        a, options=dict(POSITIVITY="D", CONSTRAIN_D4=True, R_CONVERGENCE=1e-7, E_CONVERGENCE=1e-8))
+    s.guess()
+    e = s.compute_energy()
+    assert abs(e - fci_spin_state(a, 1)) <= 1e-6

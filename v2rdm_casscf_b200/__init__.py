@@ -58,6 +58,7 @@ class Options(ctypes.Structure):
         ("spin_adapt_q2", ctypes.c_int),
         ("spin_adapt_g2", ctypes.c_int),
         ("constrain_d3", ctypes.c_int),
+        ("constrain_d4", ctypes.c_int),
     ]
 
 
@@ -188,6 +189,7 @@ DEFAULT_OPTIONS = dict(
     SPIN_ADAPT_Q2=False,
     SPIN_ADAPT_G2=False,
     CONSTRAIN_D3=False,
+    CONSTRAIN_D4=False,
 )
 
 
@@ -239,6 +241,7 @@ class V2RDMSolver:
         o.spin_adapt_q2 = int(bool(opts["SPIN_ADAPT_Q2"]))
         o.spin_adapt_g2 = int(bool(opts["SPIN_ADAPT_G2"]))
         o.constrain_d3 = int(bool(opts["CONSTRAIN_D3"]))
+        o.constrain_d4 = int(bool(opts["CONSTRAIN_D4"]))
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)

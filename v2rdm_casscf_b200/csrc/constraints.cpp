@@ -804,6 +804,114 @@ void rows_d3(const Layout& L, RowSink& S) {
     }
 }
 
+// d4.cc:55-312 (D4_constraints_Au): partial traces of D4 onto D3 with the
+// active electron counts; the reference's constraint count adds two empty
+// blocks after them (see build_layout).
+void rows_d4(const Layout& L, RowSink& S) {
+    const Gem G{L};
+    const int n = L.amo;
+    const double na = L.na, nb = L.nb;
+    auto chk = [](int v) {
+        if (v < 0) throw std::logic_error("constraint row refers to a missing quartet");
+        return v;
+    };
+    auto q = [&](const std::vector<std::vector<int>>& m, int h, int a, int b, int c, int d) {
+        return chk(L.q4(m, h, a, b, c, d));
+    };
+    auto parity = [](int p, std::initializer_list<int> xs) {
+        int c = 0;
+        for (int x : xs) c += p < x;
+        return (c & 1) ? -1.0 : 1.0;
+    };
+    // rows over same-spin triplets (bas_aaa): D4aaaa/bbbb (p distinct, signed) or
+    // D4aaab/bbba (all p, unsigned)
+    auto aaa_rows = [&](Fam f3, double coef, Fam f4, bool four_same) {
+        for (int h = 0; h < L.nirrep; h++) {
+            const int t = L.trip_aaa[h];
+            for (int r = 0; r < t; r++) {
+                const int i = L.bas_aaa[h][r][0], j = L.bas_aaa[h][r][1], k = L.bas_aaa[h][r][2];
+                for (int c = 0; c < t; c++) {
+                    const int l = L.bas_aaa[h][c][0], m = L.bas_aaa[h][c][1], nn = L.bas_aaa[h][c][2];
+                    S.add(G.at(f3, h, t, r, c), coef);
+                    for (int p = 0; p < n; p++) {
+                        const int h2 = L.sym_pair(h, L.symmetry[p]);
+                        if (four_same) {
+                            if (p == i || p == j || p == k || p == l || p == m || p == nn) continue;
+                            S.add(G.at(f4, h2, L.quart_aaaa[h2], q(L.ibas_aaaa, h2, i, j, k, p),
+                                       q(L.ibas_aaaa, h2, l, m, nn, p)),
+                                  -parity(p, {i, j, k, l, m, nn}));
+                        } else {
+                            S.add(G.at(f4, h2, L.quart_aaab[h2], q(L.ibas_aaab, h2, i, j, k, p),
+                                       q(L.ibas_aaab, h2, l, m, nn, p)),
+                                  -1.0);
+                        }
+                    }
+                    S.end();
+                }
+            }
+        }
+    };
+    // rows over mixed triplets (bas_aab) from D4aaab / D4bbba: the same-spin
+    // pair (i,j) gains p
+    auto aab_rows_3 = [&](Fam f3, double coef, Fam f4) {
+        for (int h = 0; h < L.nirrep; h++) {
+            const int t = L.trip_aab[h];
+            for (int r = 0; r < t; r++) {
+                const int i = L.bas_aab[h][r][0], j = L.bas_aab[h][r][1], k = L.bas_aab[h][r][2];
+                for (int c = 0; c < t; c++) {
+                    const int l = L.bas_aab[h][c][0], m = L.bas_aab[h][c][1], nn = L.bas_aab[h][c][2];
+                    S.add(G.at(f3, h, t, r, c), coef);
+                    for (int p = 0; p < n; p++) {
+                        if (p == i || p == j || p == l || p == m) continue;
+                        const int h2 = L.sym_pair(h, L.symmetry[p]);
+                        S.add(G.at(f4, h2, L.quart_aaab[h2], q(L.ibas_aaab, h2, i, j, p, k),
+                                   q(L.ibas_aaab, h2, l, m, p, nn)),
+                              -parity(p, {i, j, l, m}));
+                    }
+                    S.end();
+                }
+            }
+        }
+    };
+    if (na > 3) aaa_rows(F_D3AAA, na - 3.0, F_D4AAAA, true);
+    if (na > 2 && nb > 0) {
+        aaa_rows(F_D3AAA, nb, F_D4AAAB, false);
+        aab_rows_3(F_D3AAB, na - 2.0, F_D4AAAB);
+    }
+    if (na > 1 && nb > 1) {
+        // D4aabb -> D3aab (times nb - 1) and -> D3bba (times na - 1)
+        for (int beta = 0; beta < 2; beta++) {
+            for (int h = 0; h < L.nirrep; h++) {
+                const int t = L.trip_aab[h];
+                for (int r = 0; r < t; r++) {
+                    const int i = L.bas_aab[h][r][0], j = L.bas_aab[h][r][1], k = L.bas_aab[h][r][2];
+                    for (int c = 0; c < t; c++) {
+                        const int l = L.bas_aab[h][c][0], m = L.bas_aab[h][c][1], nn = L.bas_aab[h][c][2];
+                        S.add(G.at(beta ? F_D3BBA : F_D3AAB, h, t, r, c), beta ? na - 1.0 : nb - 1.0);
+                        for (int p = 0; p < n; p++) {
+                            const int h2 = L.sym_pair(h, L.symmetry[p]);
+                            if (p == k || p == nn) continue;
+                            const int a = beta ? q(L.ibas_aabb, h2, k, p, i, j) : q(L.ibas_aabb, h2, i, j, k, p);
+                            const int b = beta ? q(L.ibas_aabb, h2, nn, p, l, m) : q(L.ibas_aabb, h2, l, m, nn, p);
+                            S.add(G.at(F_D4AABB, h2, L.quart_aabb[h2], a, b), -parity(p, {k, nn}));
+                        }
+                        S.end();
+                    }
+                }
+            }
+        }
+    }
+    if (na > 0 && nb > 2) {
+        aaa_rows(F_D3BBB, na, F_D4BBBA, false);
+        aab_rows_3(F_D3BBA, nb - 2.0, F_D4BBBA);
+    }
+    if (nb > 3) aaa_rows(F_D3BBB, nb - 3.0, F_D4BBBB, true);
+    // the empty rows the reference's count adds (v2rdm_solver.cc:1108-1115)
+    if (na > 1 && nb > 1)
+        for (int h = 0; h < L.nirrep; h++)
+            for (int64_t r = 0; r < 2 * (int64_t)L.trip_aab[h] * L.trip_aab[h]; r++) S.end();
+}
+
 }  // namespace
 
 std::string build_A(const Layout& L, Csr& A) {
@@ -816,6 +924,7 @@ std::string build_A(const Layout& L, Csr& A) {
     if (L.opt.constrain_t1) rows_t1(L, S);
     if (L.opt.constrain_t2) rows_t2(L, S);
     if (L.opt.constrain_d3) rows_d3(L, S);
+    if (L.opt.constrain_d4) rows_d4(L, S);
     A.nrows = S.rows();
     A.ncols = L.dimx;
     if (A.nrows != L.ncon) return "internal error: constraint row count mismatch";

@@ -113,6 +113,61 @@ static void build_triplets(Layout& L) {
     }
 }
 
+static void build_quartets(Layout& L) {
+    // basis.cc:758-904: all (i,j,k,l) of irrep h in loop order; each map
+    // gives every permutation of its same-spin indices the same number
+    const int n = L.amo, H = L.nirrep;
+    const size_t n4 = (size_t)n * n * n * n;
+    L.quart_aaaa.assign(H, 0);
+    L.quart_aaab.assign(H, 0);
+    L.quart_aabb.assign(H, 0);
+    L.bas_aaaa.assign(H, {});
+    L.bas_aaab.assign(H, {});
+    L.bas_aabb.assign(H, {});
+    L.ibas_aaaa.assign(H, std::vector<int>(n4, -1));
+    L.ibas_aaab.assign(H, std::vector<int>(n4, -1));
+    L.ibas_aabb.assign(H, std::vector<int>(n4, -1));
+    auto at = [n](int i, int j, int k, int l) { return ((size_t)(i * n + j) * n + k) * n + l; };
+    for (int h = 0; h < H; h++)
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++)
+                for (int k = 0; k < n; k++)
+                    for (int l = 0; l < n; l++) {
+                        const int s = L.sym_pair(L.sym_pair(L.symmetry[i], L.symmetry[j]),
+                                                 L.sym_pair(L.symmetry[k], L.symmetry[l]));
+                        if (s != h) continue;
+                        if (i < j && k < l) {
+                            const int c = (int)L.bas_aabb[h].size();
+                            for (auto t : {at(i, j, k, l), at(j, i, k, l), at(i, j, l, k), at(j, i, l, k)})
+                                L.ibas_aabb[h][t] = c;
+                            L.bas_aabb[h].push_back({i, j, k, l});
+                        }
+                        if (i < j && j < k) {
+                            const int c = (int)L.bas_aaab[h].size();
+                            const int a3[3] = {i, j, k};
+                            int perm[3] = {0, 1, 2};
+                            do {
+                                L.ibas_aaab[h][at(a3[perm[0]], a3[perm[1]], a3[perm[2]], l)] = c;
+                            } while (std::next_permutation(perm, perm + 3));
+                            L.bas_aaab[h].push_back({i, j, k, l});
+                        }
+                        if (i < j && j < k && k < l) {
+                            const int c = (int)L.bas_aaaa[h].size();
+                            const int a4[4] = {i, j, k, l};
+                            int perm[4] = {0, 1, 2, 3};
+                            do {
+                                L.ibas_aaaa[h][at(a4[perm[0]], a4[perm[1]], a4[perm[2]], a4[perm[3]])] = c;
+                            } while (std::next_permutation(perm, perm + 4));
+                            L.bas_aaaa[h].push_back({i, j, k, l});
+                        }
+                    }
+    for (int h = 0; h < H; h++) {
+        L.quart_aaaa[h] = (int)L.bas_aaaa[h].size();
+        L.quart_aaab[h] = (int)L.bas_aaab[h].size();
+        L.quart_aabb[h] = (int)L.bas_aabb[h].size();
+    }
+}
+
 std::string build_layout(const Options& opt, int nirrep, const std::vector<int>& amopi, double na, double nb,
                          int multiplicity, Layout& L) {
     if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) return "nirrep must be 1, 2, 4 or 8";
@@ -143,7 +198,9 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
     if (L.amo == 0) return "empty active space";
     if (na < 0 || nb < 0 || na > L.amo || nb > L.amo) return "electron counts outside the active space";
     build_geminals(L);
+    if (opt.constrain_d4 && !opt.constrain_d3) return "internal error: CONSTRAIN_D4 without D3";
     if (opt.constrain_t1 || opt.constrain_t2 || opt.constrain_d3) build_triplets(L);
+    if (opt.constrain_d4) build_quartets(L);
 
     const int H = nirrep;
     const auto& gab = L.gems_ab;
@@ -208,6 +265,13 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
         place(F_D3AAB, L.trip_aab, 1);
         place(F_D3BBA, L.trip_aab, 1);
     }
+    if (opt.constrain_d4) {  // v2rdm_solver.cc:864-880
+        place(F_D4AAAA, L.quart_aaaa, 1);
+        place(F_D4AAAB, L.quart_aaab, 1);
+        place(F_D4AABB, L.quart_aabb, 1);
+        place(F_D4BBBA, L.quart_aaab, 1);
+        place(F_D4BBBB, L.quart_aaaa, 1);
+    }
     L.dimx = o;
 
     // constraint count, v2rdm_solver.cc:887-1127
@@ -242,6 +306,20 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
             if (na > 1) m += sq(gab[h]);
             if (nb > 1) m += sq(gab[h]);
             if (opt.constrain_spin && L.singlet()) m += sq(L.trip_aab[h]) + 2 * sq(L.trip_aaa[h]);
+        }
+    }
+    if (opt.constrain_d4) {
+        // v2rdm_solver.cc:1084-1127.  The count lists the D4aabb contractions
+        // twice while D4_constraints_Au writes them once, so the reference's
+        // constraint vector ends with 2 sum trip_aab^2 empty rows (b = 0);
+        // they are kept for an identical layout.
+        for (int h = 0; h < H; h++) {
+            const int64_t ta = sq(L.trip_aaa[h]), tb = sq(L.trip_aab[h]);
+            if (na > 3) m += ta;
+            if (na > 2 && nb > 0) m += ta + tb;
+            if (na > 1 && nb > 1) m += 4 * tb;
+            if (na > 0 && nb > 2) m += tb + ta;
+            if (nb > 3) m += ta;
         }
     }
     L.ncon = m;
@@ -294,6 +372,13 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
         dims(L.trip_aaa, 1);
         dims(L.trip_aab, 1);
         dims(L.trip_aab, 1);
+    }
+    if (opt.constrain_d4) {
+        dims(L.quart_aaaa, 1);
+        dims(L.quart_aaab, 1);
+        dims(L.quart_aabb, 1);
+        dims(L.quart_aaab, 1);
+        dims(L.quart_aaaa, 1);
     }
     int64_t bo = 0;
     for (int d : L.block_dims) {

@@ -48,6 +48,8 @@ struct Options {
     bool spin_adapt_g2 = false;
     // CONSTRAIN_D3 (plugin.cc): 3-RDM positivity with its contractions to D2
     bool constrain_d3 = false;
+    // CONSTRAIN_D4: 4-RDM positivity with its contractions to D3 (implies D3)
+    bool constrain_d4 = false;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for
@@ -62,6 +64,7 @@ enum Fam {
     F_T1AAA, F_T1BBB, F_T1AAB, F_T1BBA,
     F_T2AAA, F_T2BBB, F_T2AAB, F_T2BBA,
     F_D3AAA, F_D3BBB, F_D3AAB, F_D3BBA,
+    F_D4AAAA, F_D4AAAB, F_D4AABB, F_D4BBBA, F_D4BBBB,
     F_COUNT
 };
 
@@ -86,6 +89,11 @@ struct Layout {
     std::vector<std::vector<std::array<int, 3>>> bas_aaa, bas_aab, bas_aba;
     std::vector<std::vector<int>> ibas_aaa, ibas_aab, ibas_aba;  // [h][(i*amo+j)*amo+k]
 
+    // quartets per irrep (basis.cc:758-904): aaaa i<j<k<l, aaab i<j<k, aabb i<j & k<l
+    std::vector<int> quart_aaaa, quart_aaab, quart_aabb;
+    std::vector<std::vector<std::array<int, 4>>> bas_aaaa, bas_aaab, bas_aabb;
+    std::vector<std::vector<int>> ibas_aaaa, ibas_aaab, ibas_aabb;  // [h][((i*amo+j)*amo+k)*amo+l]
+
     // primal layout
     std::array<std::vector<int64_t>, F_COUNT> off;  // per family, per irrep
     int64_t dimx = 0;
@@ -100,6 +108,9 @@ struct Layout {
     int aab(int h, int i, int j, int k) const { return ibas_aab[h][(i * amo + j) * amo + k]; }
     int aba(int h, int i, int j, int k) const { return ibas_aba[h][(i * amo + j) * amo + k]; }
     int aaa(int h, int i, int j, int k) const { return ibas_aaa[h][(i * amo + j) * amo + k]; }
+    int q4(const std::vector<std::vector<int>>& m, int h, int i, int j, int k, int l) const {
+        return m[h][((i * amo + j) * amo + k) * amo + l];
+    }
 };
 
 // Builds the layout.  orbital_irrep lists the irrep of each active orbital in

@@ -160,7 +160,7 @@ std::string layout_key(const Layout& L, int device) {
     std::ostringstream s;
     const Options& o = L.opt;
     s << device << '|' << o.constrain_q2 << o.constrain_g2 << o.constrain_t1 << o.constrain_t2 << o.constrain_spin
-      << o.constrain_sz << o.spin_adapt_q2 << o.spin_adapt_g2 << o.constrain_d3 << '|' << L.nirrep << '|';
+      << o.constrain_sz << o.spin_adapt_q2 << o.spin_adapt_g2 << o.constrain_d3 << o.constrain_d4 << '|' << L.nirrep << '|';
     for (int a : L.amopi) s << a << ',';
     s << '|' << L.na << '|' << L.nb << '|' << L.multiplicity;
     return s.str();
@@ -852,6 +852,7 @@ void v2g_default_options(v2g_options* o) {
     o->spin_adapt_q2 = 0;
     o->spin_adapt_g2 = 0;
     o->constrain_d3 = 0;
+    o->constrain_d4 = 0;
 }
 
 const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
@@ -877,7 +878,8 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         o.cg_tol_factor = opt->cg_tolerance_factor;
         o.spin_adapt_q2 = opt->spin_adapt_q2 != 0;
         o.spin_adapt_g2 = opt->spin_adapt_g2 != 0;
-        o.constrain_d3 = opt->constrain_d3 != 0;
+        o.constrain_d4 = opt->constrain_d4 != 0;
+        o.constrain_d3 = opt->constrain_d3 != 0 || o.constrain_d4;  // v2rdm_solver.cc:527-532
         if (!(o.cg_tol_factor > 0.0 && o.cg_tol_factor < 1.0))
             return v2g::fail(V2G_ERR_ARG, "cg_tolerance_factor must be in (0, 1)");
         if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)

@@ -71,12 +71,16 @@ struct Epi {
     const double* dotv;
     double* out;
 };
+template <bool STREAM = false>
 __device__ __forceinline__ double epilogue(const Epi& e, int64_t r, int B, int b, double s) {
     const int64_t t = r * B + b;
     if (e.sub) s -= e.sub[r];
     if (e.coef) s *= e.coef[b];
     if (e.add) s += e.add[t];
-    e.out[t] = s;
+    if (STREAM)
+        __stcs(e.out + t, s);  // written once, not read again by this launch
+    else
+        e.out[t] = s;
     return e.dotv ? e.dotv[t] * s : 0.0;
 }
 
@@ -96,7 +100,7 @@ struct Blocks {
     int nchunk;                  // instance chunks per row tile
 };
 
-template <int W, bool VEC, int CH>
+template <int W, bool VEC, int CH, bool STREAM>
 __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0, int64_t ntile, int B, int b0,
                                          int cnt, unsigned act, const double* __restrict__ in, const Epi& e,
                                          double (&dot)[CH]) {
@@ -115,8 +119,13 @@ __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0,
             double v[KB];
 #pragma unroll
             for (int k = 0; k < KB; k++) {
-                c[k] = __ldg(cols + (int64_t)(k0 + k) * ns + i);
-                v[k] = __ldg(vals + (int64_t)(k0 + k) * ns + i);
+                if (STREAM) {
+                    c[k] = __ldcs(cols + (int64_t)(k0 + k) * ns + i);
+                    v[k] = __ldcs(vals + (int64_t)(k0 + k) * ns + i);
+                } else {
+                    c[k] = __ldg(cols + (int64_t)(k0 + k) * ns + i);
+                    v[k] = __ldg(vals + (int64_t)(k0 + k) * ns + i);
+                }
             }
 #pragma unroll
             for (int k = 0; k < KB; k++) {
@@ -137,10 +146,10 @@ __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0,
                 }
             }
         }
-        const int64_t r = rows[i];
+        const int64_t r = STREAM ? __ldcs(rows + i) : rows[i];
 #pragma unroll
         for (int j = 0; j < CH; j++)
-            if (j < cnt && ((act >> j) & 1u)) dot[j] += epilogue(e, r, B, b0 + j, acc[j]);
+            if (j < cnt && ((act >> j) & 1u)) dot[j] += epilogue<STREAM>(e, r, B, b0 + j, acc[j]);
     }
 }
 
@@ -157,7 +166,7 @@ __device__ __forceinline__ void chunk_range(int B, int nchunk, int ch, int& b0, 
     }
 }
 
-template <int CH>
+template <int CH, bool STREAM>
 __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in,
                                                        Epi e, const int* __restrict__ mask,
                                                        double* __restrict__ partial) {
@@ -177,18 +186,18 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int 
         const int64_t t0 = tile - bl.start[bi], nt = bl.start[bi + 1] - bl.start[bi];
         const bool vec = (B & 1) == 0;
         switch (M.width[bi] * 2 + (vec ? 1 : 0)) {
-            case 2: ell_rows<1, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 3: ell_rows<1, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 4: ell_rows<2, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 5: ell_rows<2, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 8: ell_rows<4, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 9: ell_rows<4, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 16: ell_rows<8, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 17: ell_rows<8, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 32: ell_rows<16, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 33: ell_rows<16, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 64: ell_rows<32, false, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            default: ell_rows<32, true, CH>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 2: ell_rows<1, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 3: ell_rows<1, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 4: ell_rows<2, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 5: ell_rows<2, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 8: ell_rows<4, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 9: ell_rows<4, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 16: ell_rows<8, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 17: ell_rows<8, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 32: ell_rows<16, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 33: ell_rows<16, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            case 64: ell_rows<32, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
+            default: ell_rows<32, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
         }
     }
     if (!partial) return;
@@ -436,10 +445,17 @@ static int run_map(const DevMap& M, int B, const double* in, double* out, const 
     Epi e{sub, coef, add, dotv, out};
     const Blocks bl = map_blocks(M, B);
     if (M.nb > 0) {
+        // with 8 or more instances the table loads and the output stores are
+        // streamed past L1/L2 (cache-streaming hints), leaving the caches to
+        // the gathered input: 7 % faster at n = 17..20 on B200, slower for
+        // single instances
+        const int g = bl.start[M.nb] * bl.nchunk;
         if (B <= 2)
-            ell_kernel<2><<<bl.start[M.nb] * bl.nchunk, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+            ell_kernel<2, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+        else if (B < 8)
+            ell_kernel<4, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
         else
-            ell_kernel<4><<<bl.start[M.nb] * bl.nchunk, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+            ell_kernel<4, true><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
         g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     }
     if (M.nlong > 0) {

@@ -54,10 +54,10 @@ ITER_FILE = os.path.join(ROOT, "profiles", "batch256_outer_iterations.json")
 # from one ncu capture of exactly those launches (cold caches, as ncu replays them):
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:ell_kernel -c 46 --csv python bench.py --roofline-only
-# A: 437.8 MB read + 206.4 MB written; A^T: 518.5 MB + 235.4 MB (B200, 20 launches each).
+# A: 442.8 MB read + 203.6 MB written; A^T: 528.1 MB + 237.4 MB (B200, 20 launches each).
 ROOFLINE_TRAFFIC = {
     "n=20, 19 instances interleaved": {
-        "bytes_per_launch": 0.5 * ((437.8 + 206.4) + (518.5 + 235.4)) * 1e6,
+        "bytes_per_launch": 0.5 * ((442.8 + 203.6) + (528.1 + 237.4)) * 1e6,
         "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same launches "
                   "(python bench.py --roofline-only), mean of A and A^T",
     },

@@ -1,7 +1,7 @@
 // Constraint maps, CG vector kernels and per-instance reductions (FP64).
 //
-// The maps A and A^T are applied as gathers over CSR tables shared by all
-// instances of a group (see kernels.cuh for the interleaved layout).  A^T is
+// The maps A and A^T are applied as gathers over bucketed-ELL tables shared
+// by all instances of a group (see kernels.cuh for the layouts).  A^T is
 // the transpose of A's table, so every primal element sums its contributing
 // constraints itself: no atomics, deterministic order, and the two maps are
 // exact adjoints.  These kernels are HBM-bound; their algorithmic traffic per

@@ -4,8 +4,10 @@ boundary-point SDP solve of a batch of active spaces on B200.
 
 Workload (default "batch256"): 256 seeded synthetic active spaces, n ~ U{8..20}
 orbitals, singlets with N = n electrons (N = n - 1 for odd n), C1, DQG
-with CONSTRAIN_SPIN, each started from the reference's random guess (srand(0)),
-all solved in one batched call of the C ABI (v2g_solve_batch).  One step = one
+with CONSTRAIN_SPIN, all solved in one batched call of the C ABI
+(v2g_solve_batch).  By default every instance starts from the least-norm
+feasible point of A x = b with zero duals (computed on the GPU inside the
+timed solve); --start state / --plain use the reference's random start.  One step = one
 full batched solve.  Inputs are far larger than L2 (the primal/dual vectors of
 the batch take several GB), so no L2 flush is needed between steps.
 
@@ -159,7 +161,8 @@ def run_gpu(args):
         if maxiter:
             opts["MAXITER"] = maxiter
         return [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
-                                                projection=args.projection, cg_tolerance_factor=args.cg_factor)
+                                                projection=args.projection, cg_tolerance_factor=args.cg_factor,
+                                                start=args.start)
                 for i in mine]
 
     solvers = make(args.max_outer)
@@ -251,15 +254,20 @@ def run_gpu(args):
         "data": "synthetic (seeded Philox active spaces; no public dataset involved)",
         "config": {
             "workload": f"{args.workload}: {args.count} synthetic active spaces n~U{{8..20}}, singlet N=n (n-1 for odd n), C1, DQG, "
-                        "CONSTRAIN_SPIN, E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6, random start (srand(0))",
+                        "CONSTRAIN_SPIN, E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6",
             "instances": args.count,
             "precision": "FP64 (maps, CG, projection)",
             "projection": args.projection,
             "cg_tolerance_factor": args.cg_factor,
             "mu_update_frequency": args.mu_freq,
-            "mode": "plain FP64 (reference algorithm and options)"
-                    if (args.projection == "exact" and args.cg_factor == 0.01 and args.mu_freq == 500)
-                    else "FP64 with adaptive projection" + (f", mu update every {args.mu_freq}" if args.mu_freq != 500 else ""),
+            "start": ("least-norm feasible point of A x = b, zero duals, mu 1 (computed on the GPU inside "
+                      "the timed solve)") if args.start == "feasible" else "the reference's random start (srand(0))",
+            "mode": "plain FP64 (reference algorithm, options and start)"
+                    if (args.projection == "exact" and args.cg_factor == 0.01 and args.mu_freq == 500
+                        and args.start == "state")
+                    else "FP64 maps/CG/projection, adaptive projection accuracy"
+                         + (", feasible warm start" if args.start == "feasible" else "")
+                         + (f", mu update every {args.mu_freq}" if args.mu_freq != 500 else ""),
             "warmup_steps": f"{args.warmup} batched calls capped at {args.warmup_outer} outer iterations",
             "l2": "inputs larger than L2 (no flush needed)",
             "parallelism": f"instances bin-packed over {world} rank(s) by modelled cost, no exchange",
@@ -295,9 +303,12 @@ def run_gpu(args):
     if rank == 0:
         out["outer_iterations"] = {str(k): v for k, v in sorted(oiters.items())}
         if args.cpu_baseline and world == 1:
-            out["cpu_baseline"] = cpu_baseline(all_spaces, [results[k]["oiter"] for k in range(len(results))],
-                                               args.cpu_sample)
-        if args.save_iterations and world == 1 and not args.max_outer:
+            # the reference runs from its own random start: its iteration counts are
+            # those of a solve from that start (recorded), else this run's
+            oiters, src = reference_iterations(args, [results[k]["oiter"] for k in range(len(results))])
+            out["cpu_baseline"] = cpu_baseline(all_spaces, oiters, args.cpu_sample)
+            out["cpu_baseline"]["sample"] += "; iteration counts: " + src
+        if args.save_iterations and world == 1 and not args.max_outer and args.start == "state":
             os.makedirs(os.path.dirname(ITER_FILE), exist_ok=True)
             json.dump({"workload": args.workload, "count": args.count,
                        "outer_iterations": [int(r["oiter"]) for r in results],
@@ -364,6 +375,15 @@ def ref_time_per_iteration(space, iters, threads):
     return max(t1 - t0, 1e-9) / iters
 
 
+def reference_iterations(args, fallback):
+    """Outer-iteration counts of the reference's own start for this workload."""
+    if args.workload == "batch256" and args.count == 256 and os.path.exists(ITER_FILE):
+        d = json.load(open(ITER_FILE))
+        return d["outer_iterations"], ("outer-iteration counts of the same instances solved on the GPU from the "
+                                       "reference's random start with its loop options (profiles/)")
+    return fallback, "outer-iteration counts of this run"
+
+
 def cpu_baseline(spaces, oiters, sample_sizes):
     """Reference CPU time for the batch, extrapolated from a timed sample."""
     from oracle import ref as R
@@ -405,12 +425,8 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built on this box"}))
         return
     spaces = workload(args.workload, args.count)
-    if os.path.exists(ITER_FILE):
-        d = json.load(open(ITER_FILE))
-        oiters = d["outer_iterations"]
-        src = "outer-iteration counts of the same instances from the GPU solve (profiles/)"
-    else:
-        oiters = [2500] * len(spaces)
+    oiters, src = reference_iterations(args, [2500] * len(spaces))
+    if not os.path.exists(ITER_FILE):
         src = "2500 outer iterations per instance (no recorded counts)"
     vals = []
     base = None
@@ -446,8 +462,11 @@ def main():
                     help="CG tolerance factor (0.01 = the reference's rule)")
     ap.add_argument("--mu-update-frequency", dest="mu_freq", type=int, default=500,
                     help="MU_UPDATE_FREQUENCY (the reference's default is 500)")
+    ap.add_argument("--start", default="feasible", choices=["feasible", "state"],
+                    help="feasible: least-norm feasible warm start; state: the reference's random start")
     ap.add_argument("--plain", action="store_true",
-                    help="reference algorithm and options: exact projection, CG factor 0.01, mu update every 500")
+                    help="reference algorithm, options and start: exact projection, CG factor 0.01, "
+                         "mu update every 500, random start")
     ap.add_argument("--warmup-outer", type=int, default=3, help="outer iterations per warm-up step")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-sample", type=lambda s: [int(v) for v in s.split(",")], default=[8, 12, 16, 20])
@@ -457,7 +476,7 @@ def main():
                     help="run only the timed A / A^T launches of the roofline (for profiling)")
     args = ap.parse_args()
     if args.plain:
-        args.projection, args.cg_factor, args.mu_freq = "exact", 0.01, 500
+        args.projection, args.cg_factor, args.mu_freq, args.start = "exact", 0.01, 500, "state"
     if args.impl == "reference":
         run_reference(args)
     else:

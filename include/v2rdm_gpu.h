@@ -75,6 +75,10 @@ typedef struct v2g_options {
     int constrain_d3;           /* CONSTRAIN_D3: 3-RDM positivity and its partial traces (0) */
     int constrain_d4;           /* CONSTRAIN_D4: 4-RDM positivity and its partial traces; implies
                                    constrain_d3, as in the plugin (0) */
+    int start;                  /* 0: solve from the handle's state (v2g_guess_random, the plugin's
+                                   TPDM_GUESS=RANDOM, or v2g_set_state); 1: from the least-norm
+                                   point of A x = b with zero duals and mu = 1, computed on the
+                                   GPU at the start of the solve (no counterpart in the plugin) (0) */
 } v2g_options;
 
 typedef struct v2g_result {

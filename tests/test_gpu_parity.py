@@ -247,3 +247,18 @@ def test_four_electron_d_d4_equals_fci(v2g, seed):
     s.guess()
     e = s.compute_energy()
     assert abs(e - fci_spin_state(a, 1)) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["synthetic_n4_s0", "synthetic_n5_s2_doublet"])
+def test_feasible_start_reaches_reference_energy(v2g, name):
+    # the least-norm feasible start (start="feasible") changes the path, not the answer
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, f"solve_{name}.npz"))
+    a = synthetic(int(g["n"]), int(g["seed"]), electrons=int(g["electrons"]))
+    s = v2g.V2RDMSolver.from_active_space(
+        a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])), start="feasible",
+        projection="adaptive")
+    e = s.compute_energy()
+    assert s.result["status"] == 0
+    assert abs(e - float(g["e_primal"])) <= 1e-6

@@ -59,6 +59,7 @@ class Options(ctypes.Structure):
         ("spin_adapt_g2", ctypes.c_int),
         ("constrain_d3", ctypes.c_int),
         ("constrain_d4", ctypes.c_int),
+        ("start", ctypes.c_int),
     ]
 
 
@@ -208,7 +209,7 @@ class V2RDMSolver:
 
     def __init__(self, active, nalpha, nbeta, multiplicity=1, frozen_docc=None, restricted_docc=None,
                  restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False,
-                 profile=False, projection="exact", cg_tolerance_factor=0.01):
+                 profile=False, projection="exact", cg_tolerance_factor=0.01, start="state"):
         L = lib()
         self.active = list(active)
         opts = dict(DEFAULT_OPTIONS)
@@ -242,6 +243,9 @@ class V2RDMSolver:
         o.spin_adapt_g2 = int(bool(opts["SPIN_ADAPT_G2"]))
         o.constrain_d3 = int(bool(opts["CONSTRAIN_D3"]))
         o.constrain_d4 = int(bool(opts["CONSTRAIN_D4"]))
+        if start not in ("state", "feasible"):
+            raise ValueError("start is 'state' (guess()/set_state) or 'feasible'")
+        o.start = int(start == "feasible")
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)

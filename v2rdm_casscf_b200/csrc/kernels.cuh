@@ -64,6 +64,8 @@ int64_t reduce_partial_size(int B);
 
 // z = c - z for active instances (v2rdm_solver.cc:1789-1790)
 void launch_c_minus_z(int64_t n, int B, const double* c, double* z, const int* mask, cudaStream_t s);
+// out[e * B + b] = row[e] (or 0 when row is null) for the instances with mask[b] set
+void launch_set_rows(int64_t n, int B, const double* row, double* out, const int* mask, cudaStream_t s);
 
 // CG pieces (cg_solver.cc:125-177), per instance with cg_active masks.
 struct CgScalars {

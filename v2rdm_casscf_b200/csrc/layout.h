@@ -50,6 +50,9 @@ struct Options {
     bool constrain_d3 = false;
     // CONSTRAIN_D4: 4-RDM positivity with its contractions to D3 (implies D3)
     bool constrain_d4 = false;
+    // Start the solve from the least-norm point of {A x = b} (x = A^T w with
+    // A A^T w = b, y = z = 0, mu = 1) instead of the handle's state.
+    bool feasible_start = false;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for

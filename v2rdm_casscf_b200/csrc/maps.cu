@@ -303,6 +303,18 @@ __global__ void reduce_stage2(int nblk, int B, const double* __restrict__ partia
     if (threadIdx.x == 0) out[b] = sh[0];
 }
 
+// out[e * B + b] = row ? row[e] : 0 for instances with mask[b] set
+__global__ void set_rows_kernel(int64_t n, int B, const double* __restrict__ row, double* __restrict__ out,
+                                const int* __restrict__ mask) {
+    const int64_t total = n * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t % B);
+        if (mask && !mask[b]) continue;
+        out[t] = row ? row[t / B] : 0.0;
+    }
+}
+
 __global__ void c_minus_z_kernel(int64_t n, int B, const double* __restrict__ c, double* __restrict__ z,
                                  const int* __restrict__ mask) {
     const int64_t total = n * B;
@@ -484,6 +496,11 @@ void launch_reduce(ReduceMode mode, int64_t n, int B, const double* u, const dou
     reduce_stage1<<<kRedBlocks, kThreads, 0, s>>>((int)mode, n, B, u, v, w, row, partial);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     reduce_stage2<<<B, kThreads, 0, s>>>(kRedBlocks, B, partial, out);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_set_rows(int64_t n, int B, const double* row, double* out, const int* mask, cudaStream_t s) {
+    set_rows_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, row, out, mask);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -435,6 +435,19 @@ class GroupRun {
         double t_cg = 0, t_xz = 0;
         CK(cudaEventRecord(e3, s_));
         std::vector<CgScalars> cs(B_);
+        {
+            std::vector<int> fs(B_);
+            bool any = false;
+            for (int b = 0; b < B_; b++) any |= (fs[b] = opt(b).feasible_start ? 1 : 0) != 0;
+            if (any) {
+                feasible_start(fs, cs);
+                for (int b = 0; b < B_; b++)
+                    if (fs[b]) {
+                        mu[b] = 1.0;
+                        iiter[b] += cs[b].iter;
+                    }
+            }
+        }
         int it = 0;
         while (true) {
             int nactive = 0;
@@ -561,6 +574,38 @@ class GroupRun {
                      "v2g: instance %d of a group of %d (dimx %lld) non-finite after outer iteration %d: "
                      "|y|^2 %g, |x|^2 %g, |z|^2 %g, mu %g, CG iterations %ld\n",
                      b, B_, (long long)nx_, oiter, sums[0], sums[1], sums[2], mu, cg_iters);
+    }
+
+    // Least-norm feasible start for the instances with fs[b] set: w solves
+    // A A^T w = b by the loop's CG (to 1e-10 ||b||), x = A^T w, y = z = 0,
+    // mu = 1.  A x = b is then met to the CG tolerance; the BPSDP iteration
+    // starts from a feasible primal with zero duals.
+    void feasible_start(const std::vector<int>& fs, std::vector<CgScalars>& cs) {
+        CK(cudaMemcpyAsync(mask_.p, fs.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        double bn = 0.0;
+        for (double v : T_.hb) bn += v * v;
+        bn = std::sqrt(bn);
+        for (int b = 0; b < B_; b++) {
+            cs[b] = CgScalars{};
+            cs[b].tol = 1e-10 * std::max(1.0, bn);
+            cs[b].active = fs[b];
+            cs[b].maxiter = P_[b]->opt.cg_maxiter;
+        }
+        CK(cudaMemcpyAsync(cs_.p, cs.data(), B_ * sizeof(CgScalars), cudaMemcpyHostToDevice, s_));
+        launch_set_rows(nc_, B_, T_.b.p, bv_.p, mask_.p, s_);  // right-hand side b
+        launch_set_rows(nc_, B_, nullptr, y_.p, mask_.p, s_);  // w starts at 0
+        cg_solve();
+        CK(cudaMemcpyAsync(cs.data(), cs_.p, B_ * sizeof(CgScalars), cudaMemcpyDeviceToHost, s_));
+        launch_spmv(T_.AT(), B_, y_.p, x_.p, nullptr, nullptr, nullptr, mask_.p, s_);
+        launch_set_rows(nc_, B_, nullptr, y_.p, mask_.p, s_);
+        launch_set_rows(nx_, B_, nullptr, z_.p, mask_.p, s_);
+        std::vector<double> mu(B_);
+        CK(cudaMemcpyAsync(mu.data(), mu_.p, B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
+        for (int b = 0; b < B_; b++)
+            if (fs[b]) mu[b] = 1.0;
+        CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaStreamSynchronize(s_));
     }
 
     long jacobi_sweeps() const { return sweeps_total_; }
@@ -853,6 +898,7 @@ void v2g_default_options(v2g_options* o) {
     o->spin_adapt_g2 = 0;
     o->constrain_d3 = 0;
     o->constrain_d4 = 0;
+    o->start = 0;
 }
 
 const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
@@ -880,6 +926,8 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         o.spin_adapt_g2 = opt->spin_adapt_g2 != 0;
         o.constrain_d4 = opt->constrain_d4 != 0;
         o.constrain_d3 = opt->constrain_d3 != 0 || o.constrain_d4;  // v2rdm_solver.cc:527-532
+        if (opt->start != 0 && opt->start != 1) return v2g::fail(V2G_ERR_ARG, "start must be 0 or 1");
+        o.feasible_start = opt->start == 1;
         if (!(o.cg_tol_factor > 0.0 && o.cg_tol_factor < 1.0))
             return v2g::fail(V2G_ERR_ARG, "cg_tolerance_factor must be in (0, 1)");
         if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)

@@ -172,6 +172,13 @@ int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const dou
 int v2g_spatial_density_dims(const v2g_handle* h, long* d1_dim, long* d2_dim);
 int v2g_pack_spatial_density(v2g_handle* h, const double* active_energies, double* d1, double* d2);
 
+/* Checkpoint and restart (WriteCheckpointFile / ReadFromCheckpointFile,
+ * checkpoint.cc:56-121): the entries MU, PRIMAL, DUAL 1, DUAL 2 of the
+ * handle's state in a small named-record file (not Psi4's PSIO container).
+ * Reading checks that the file belongs to the same layout. */
+int v2g_write_checkpoint(const v2g_handle* h, const char* path);
+int v2g_read_checkpoint(v2g_handle* h, const char* path);
+
 /* The full BPSDP solve from the handle's current state. */
 int v2g_solve(v2g_handle* h, v2g_result* res);
 

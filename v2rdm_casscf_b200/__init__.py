@@ -35,6 +35,7 @@ EXPORTS = [
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
     "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density",
+    "v2g_write_checkpoint", "v2g_read_checkpoint",
 ]
 
 
@@ -144,6 +145,8 @@ def lib():
         L.v2g_update_xz_noalloc.argtypes = [P, D, P, P, P, P, P]
         L.v2g_spatial_density_dims.argtypes = [P, LP, LP]
         L.v2g_pack_spatial_density.argtypes = [P, DP, DP, DP]
+        L.v2g_write_checkpoint.argtypes = [P, ctypes.c_char_p]
+        L.v2g_read_checkpoint.argtypes = [P, ctypes.c_char_p]
         L.v2g_solve.argtypes = [P, ctypes.POINTER(Result)]
         L.v2g_solve_batch.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(Result)]
         L.v2g_export_A.argtypes = [P, LP, IP, DP]
@@ -353,6 +356,14 @@ class V2RDMSolver:
 
     def update_xz(self, mu):
         _check(lib().v2g_update_xz(self.h, float(mu)))
+
+    def write_checkpoint(self, path):
+        """Write mu, x, y, z (the plugin's checkpoint entries) to path."""
+        _check(lib().v2g_write_checkpoint(self.h, os.fspath(path).encode()))
+
+    def read_checkpoint(self, path):
+        """Restore mu, x, y, z from a checkpoint of the same layout."""
+        _check(lib().v2g_read_checkpoint(self.h, os.fspath(path).encode()))
 
     def pack_spatial_density(self, active_energies=None):
         """(d1, d2) handed to focas, as PackSpatialDensity (v2rdm_solver.cc:3664-3773)."""

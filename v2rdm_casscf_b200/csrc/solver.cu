@@ -1022,6 +1022,96 @@ int v2g_set_state(v2g_handle* h, const double* x, const double* y, const double*
     return V2G_OK;
 }
 
+// Checkpoint file: the entries of WriteCheckpointFile (checkpoint.cc:56-88),
+// "MU", "PRIMAL", "DUAL 1", "DUAL 2", as named records in a small container of
+// our own (Psi4's PSIO container is not reproduced):
+//   magic "V2GCKPT1", int64 record count, then per record an 80-byte
+//   zero-padded key, an int64 byte length and the bytes.
+// A "LAYOUT" record (dimx, nconstraints) guards against restarting a
+// different problem.
+namespace {
+const char kCkptMagic[8] = {'V', '2', 'G', 'C', 'K', 'P', 'T', '1'};
+
+void ckpt_put(std::FILE* f, const char* key, const void* data, int64_t bytes) {
+    char k[80] = {};
+    std::strncpy(k, key, sizeof(k) - 1);
+    if (std::fwrite(k, 1, sizeof(k), f) != sizeof(k) || std::fwrite(&bytes, sizeof(bytes), 1, f) != 1 ||
+        (bytes > 0 && std::fwrite(data, 1, (size_t)bytes, f) != (size_t)bytes))
+        throw std::invalid_argument("checkpoint write failed");
+}
+}  // namespace
+
+int v2g_write_checkpoint(const v2g_handle* h, const char* path) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !path) return v2g::fail(V2G_ERR_ARG, "null argument");
+        const Problem& P = h->P;
+        std::FILE* f = std::fopen(path, "wb");
+        if (!f) return v2g::fail(V2G_ERR_ARG, std::string("cannot open ") + path + " for writing");
+        try {
+            const int64_t n = 5;
+            const int64_t layout[2] = {P.L.dimx, P.L.ncon};
+            if (std::fwrite(kCkptMagic, 1, 8, f) != 8 || std::fwrite(&n, sizeof(n), 1, f) != 1)
+                throw std::invalid_argument("checkpoint write failed");
+            ckpt_put(f, "LAYOUT", layout, sizeof(layout));
+            ckpt_put(f, "MU", &P.mu, sizeof(double));
+            ckpt_put(f, "PRIMAL", P.x.data(), (int64_t)P.x.size() * 8);
+            ckpt_put(f, "DUAL 1", P.y.data(), (int64_t)P.y.size() * 8);
+            ckpt_put(f, "DUAL 2", P.z.data(), (int64_t)P.z.size() * 8);
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        if (std::fclose(f) != 0) return v2g::fail(V2G_ERR_ARG, "checkpoint write failed");
+        return V2G_OK;
+    });
+}
+
+int v2g_read_checkpoint(v2g_handle* h, const char* path) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !path) return v2g::fail(V2G_ERR_ARG, "null argument");
+        Problem& P = h->P;
+        std::FILE* f = std::fopen(path, "rb");
+        if (!f) return v2g::fail(V2G_ERR_ARG, std::string("cannot open ") + path);
+        std::map<std::string, std::vector<char>> rec;
+        bool ok = true;
+        char magic[8];
+        int64_t n = 0;
+        ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCkptMagic, 8) == 0 &&
+             std::fread(&n, sizeof(n), 1, f) == 1 && n >= 0 && n < 64;
+        for (int64_t i = 0; ok && i < n; i++) {
+            char k[81] = {};
+            int64_t bytes = 0;
+            ok = std::fread(k, 1, 80, f) == 80 && std::fread(&bytes, sizeof(bytes), 1, f) == 1 && bytes >= 0 &&
+                 bytes <= (int64_t)1 << 40;
+            if (!ok) break;
+            std::vector<char> buf((size_t)bytes);
+            ok = bytes == 0 || std::fread(buf.data(), 1, (size_t)bytes, f) == (size_t)bytes;
+            rec[std::string(k)] = std::move(buf);
+        }
+        std::fclose(f);
+        if (!ok) return v2g::fail(V2G_ERR_ARG, std::string(path) + " is not a v2g checkpoint file");
+        for (const char* k : {"LAYOUT", "MU", "PRIMAL", "DUAL 1", "DUAL 2"})
+            if (!rec.count(k)) return v2g::fail(V2G_ERR_ARG, std::string("checkpoint lacks the entry ") + k);
+        int64_t layout[2];
+        if (rec["LAYOUT"].size() != sizeof(layout)) return v2g::fail(V2G_ERR_ARG, "bad LAYOUT entry");
+        std::memcpy(layout, rec["LAYOUT"].data(), sizeof(layout));
+        if (layout[0] != P.L.dimx || layout[1] != P.L.ncon)
+            return v2g::fail(V2G_ERR_ARG, "checkpoint belongs to a different layout (dimx " + std::to_string(layout[0]) +
+                                              ", nconstraints " + std::to_string(layout[1]) + ")");
+        if (rec["MU"].size() != 8 || rec["PRIMAL"].size() != (size_t)P.L.dimx * 8 ||
+            rec["DUAL 1"].size() != (size_t)P.L.ncon * 8 || rec["DUAL 2"].size() != (size_t)P.L.dimx * 8)
+            return v2g::fail(V2G_ERR_ARG, "checkpoint entry sizes do not match the layout");
+        std::memcpy(&P.mu, rec["MU"].data(), 8);
+        P.x.resize(P.L.dimx);
+        P.y.resize(P.L.ncon);
+        P.z.resize(P.L.dimx);
+        std::memcpy(P.x.data(), rec["PRIMAL"].data(), rec["PRIMAL"].size());
+        std::memcpy(P.y.data(), rec["DUAL 1"].data(), rec["DUAL 1"].size());
+        std::memcpy(P.z.data(), rec["DUAL 2"].data(), rec["DUAL 2"].size());
+        return V2G_OK;
+    });
+}
+
 int v2g_get_state(const v2g_handle* h, double* x, double* y, double* z, double* mu) {
     if (!h) return V2G_ERR_ARG;
     const Problem& P = h->P;

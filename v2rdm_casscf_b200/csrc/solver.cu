@@ -448,8 +448,20 @@ class GroupRun {
                     }
             }
         }
+        // an instance whose iterate turns non-finite restarts (at most twice)
+        std::vector<int> restarts_left(B_, 2), recover(B_, 0);
         int it = 0;
         while (true) {
+            if (std::find(recover.begin(), recover.end(), 1) != recover.end()) {
+                feasible_start(recover, cs);
+                for (int b = 0; b < B_; b++)
+                    if (recover[b]) {
+                        mu[b] = 1.0;
+                        iiter[b] += cs[b].iter;
+                        recover[b] = 0;
+                    }
+                warm_ = false;  // every large block of the group starts its projection cold again
+            }
             int nactive = 0;
             for (int b = 0; b < B_; b++) nactive += active[b];
             if (nactive == 0) break;
@@ -525,9 +537,17 @@ class GroupRun {
                 res[b].efzc = P.efzc;
                 res[b].enuc = P.enuc;
                 if (!std::isfinite(ep[b]) || !std::isfinite(ed[b]) || !std::isfinite(e_p)) {
+                    report_nonfinite(b, oiter[b], mu[b], ii);
+                    if (restarts_left[b] > 0) {
+                        // restart this instance from the feasible start and
+                        // the whole group's projection cold (below)
+                        restarts_left[b]--;
+                        recover[b] = 1;
+                        ep[b] = ed[b] = 1.0;  // CG and projection tolerances as in iteration 0
+                        continue;
+                    }
                     res[b].status = V2G_ERR_NONFINITE;
                     active[b] = 0;
-                    report_nonfinite(b, oiter[b], mu[b], ii);
                     continue;
                 }
                 if (oiter[b] == o.maxiter) {

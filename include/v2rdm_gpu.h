@@ -170,6 +170,13 @@ int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const dou
  * energies do (basis.cc:626-652); NULL numbers them in Pitzer order.  The
  * values equal the reference's bit for bit. */
 int v2g_spatial_density_dims(const v2g_handle* h, long* d1_dim, long* d2_dim);
+
+/* Orbital energies of the active orbitals (Pitzer order), as the plugin's
+ * epsilon_a_: they number the spatial pairs of the spin-adapted Q2 singlet
+ * block and of the packed 2-RDM (basis.cc:626-652).  Without this call the
+ * pairs follow Pitzer order, which is the reference's for C1.  Call before the
+ * first map or solve of the handle (its device tables are rebuilt). */
+int v2g_set_active_orbital_energies(v2g_handle* h, const double* energies);
 int v2g_pack_spatial_density(v2g_handle* h, const double* active_energies, double* d1, double* d2);
 
 /* Checkpoint and restart (WriteCheckpointFile / ReadFromCheckpointFile,

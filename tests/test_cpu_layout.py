@@ -224,3 +224,24 @@ def test_spatial_density_dims(v2g):
             for j in range(i + 1):
                 g00[sym[i] ^ sym[j]] += 1
         assert n2.value == sum(g * (g + 1) // 2 for g in g00)
+
+
+@pytest.mark.parametrize("amopi,energies", [
+    ([2, 1, 1, 2], [0.3, 1.1, 0.2, 0.5, 0.1, 0.9]), ([3, 2], [0.2, 0.4, 0.9, 0.3, 0.35]),
+    ([5], [0.5, 0.1, 0.3, 0.3, 0.2]),
+])
+def test_spin_adapted_q2_follows_orbital_energies(v2g, ref, amopi, energies):
+    # the singlet Q2 block is numbered by spatial pairs in orbital-energy order
+    nb = sum(amopi) // 2
+    docc, left = [], nb
+    for a in amopi:
+        docc.append(min(a, left))
+        left -= docc[-1]
+    r = ref.RefSolver(amopi, docc, energies=energies, spin_adapt_q2=True)
+    s = v2g.V2RDMSolver(amopi, nb, nb, options=dict(SPIN_ADAPT_Q2=True))
+    s.set_active_orbital_energies(energies)
+    A = csr_of(s)
+    rng = np.random.default_rng(17)
+    u = rng.standard_normal(s.dimx)
+    a = r.Au(u)
+    assert np.abs(A @ u - a).max() <= 1e-13 * np.abs(a).max()

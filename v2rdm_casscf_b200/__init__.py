@@ -35,7 +35,7 @@ EXPORTS = [
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
     "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density",
-    "v2g_write_checkpoint", "v2g_read_checkpoint",
+    "v2g_write_checkpoint", "v2g_read_checkpoint", "v2g_set_active_orbital_energies",
 ]
 
 
@@ -146,6 +146,7 @@ def lib():
         L.v2g_spatial_density_dims.argtypes = [P, LP, LP]
         L.v2g_pack_spatial_density.argtypes = [P, DP, DP, DP]
         L.v2g_write_checkpoint.argtypes = [P, ctypes.c_char_p]
+        L.v2g_set_active_orbital_energies.argtypes = [P, DP]
         L.v2g_read_checkpoint.argtypes = [P, ctypes.c_char_p]
         L.v2g_solve.argtypes = [P, ctypes.POINTER(Result)]
         L.v2g_solve_batch.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(Result)]
@@ -356,6 +357,13 @@ class V2RDMSolver:
 
     def update_xz(self, mu):
         _check(lib().v2g_update_xz(self.h, float(mu)))
+
+    def set_active_orbital_energies(self, energies):
+        """Orbital energies of the active orbitals (Pitzer order); they number the
+        spatial pairs as the plugin's orbital energies do."""
+        e = np.ascontiguousarray(energies, dtype=np.float64)
+        assert e.size == sum(self.active)
+        _check(lib().v2g_set_active_orbital_energies(self.h, _dp(e)))
 
     def write_checkpoint(self, path):
         """Write mu, x, y, z (the plugin's checkpoint entries) to path."""

@@ -59,12 +59,13 @@ static void build_geminals(Layout& L) {
         L.gems_ab[h] = (int)L.bas_ab[h].size();
         L.gems_aa[h] = (int)L.bas_aa[h].size();
     }
-    // spatial pairs i >= j per irrep (basis.cc:626-652), numbered in the
-    // orbitals' energy order, taken here as Pitzer order
+    // spatial pairs per irrep (basis.cc:626-652): for orbitals taken in energy
+    // order, each with every orbital before it (and itself)
     L.bas_00.assign(H, {});
     L.ibas_00.assign(H, std::vector<int>(n * n, -1));
-    for (int i = 0; i < n; i++)
-        for (int j = 0; j <= i; j++) {
+    for (int ie = 0; ie < n; ie++)
+        for (int je = 0; je <= ie; je++) {
+            const int i = L.energy_order[ie], j = L.energy_order[je];
             const int h = L.sym_pair(L.symmetry[i], L.symmetry[j]);
             L.ibas_00[h][i * n + j] = L.gems_00[h];
             L.ibas_00[h][j * n + i] = L.gems_00[h];
@@ -169,7 +170,7 @@ static void build_quartets(Layout& L) {
 }
 
 std::string build_layout(const Options& opt, int nirrep, const std::vector<int>& amopi, double na, double nb,
-                         int multiplicity, Layout& L) {
+                         int multiplicity, Layout& L, const std::vector<int>& energy_order) {
     if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) return "nirrep must be 1, 2, 4 or 8";
     if ((int)amopi.size() != nirrep) return "amopi must have nirrep entries";
     // restrictions of v2rdm_solver.cc:538-558
@@ -197,6 +198,17 @@ std::string build_layout(const Options& opt, int nirrep, const std::vector<int>&
     }
     if (L.amo == 0) return "empty active space";
     if (na < 0 || nb < 0 || na > L.amo || nb > L.amo) return "electron counts outside the active space";
+    if (energy_order.empty()) {
+        L.energy_order.resize(L.amo);
+        for (int i = 0; i < L.amo; i++) L.energy_order[i] = i;
+    } else {
+        std::vector<int> seen(L.amo, 0);
+        if ((int)energy_order.size() != L.amo) return "energy order must list every active orbital";
+        for (int i : energy_order) {
+            if (i < 0 || i >= L.amo || seen[i]++) return "energy order must be a permutation of the active orbitals";
+        }
+        L.energy_order = energy_order;
+    }
     build_geminals(L);
     if (opt.constrain_d4 && !opt.constrain_d3) return "internal error: CONSTRAIN_D4 without D3";
     if (opt.constrain_t1 || opt.constrain_t2 || opt.constrain_d3) build_triplets(L);

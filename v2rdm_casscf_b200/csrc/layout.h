@@ -85,7 +85,8 @@ struct Layout {
     // geminals per irrep
     std::vector<int> gems_ab, gems_aa, gems_00;
     std::vector<std::vector<std::array<int, 2>>> bas_ab, bas_aa, bas_00;
-    std::vector<std::vector<int>> ibas_00;            // [h][i*amo+j], spatial pairs in Pitzer order
+    std::vector<std::vector<int>> ibas_00;            // [h][i*amo+j], spatial pairs in energy order
+    std::vector<int> energy_order;                    // active orbitals by orbital energy
     std::vector<std::vector<int>> ibas_ab, ibas_aa;  // [h][i*amo+j], -1 if (i,j) not in irrep h
     // triplets per irrep
     std::vector<int> trip_aaa, trip_aab, trip_aba;
@@ -119,7 +120,9 @@ struct Layout {
 // Builds the layout.  orbital_irrep lists the irrep of each active orbital in
 // Pitzer order (irreps non-decreasing); na/nb are active electron counts.
 // Returns an empty string on success, else the reason.
+// energy_order lists the active orbitals in increasing orbital energy (it
+// numbers the spatial pairs, basis.cc:626-652); empty = Pitzer order.
 std::string build_layout(const Options& opt, int nirrep, const std::vector<int>& amopi, double na, double nb,
-                         int multiplicity, Layout& L);
+                         int multiplicity, Layout& L, const std::vector<int>& energy_order = {});
 
 }  // namespace v2g

@@ -162,7 +162,8 @@ std::string layout_key(const Layout& L, int device) {
     s << device << '|' << o.constrain_q2 << o.constrain_g2 << o.constrain_t1 << o.constrain_t2 << o.constrain_spin
       << o.constrain_sz << o.spin_adapt_q2 << o.spin_adapt_g2 << o.constrain_d3 << o.constrain_d4 << '|' << L.nirrep << '|';
     for (int a : L.amopi) s << a << ',';
-    s << '|' << L.na << '|' << L.nb << '|' << L.multiplicity;
+    s << '|' << L.na << '|' << L.nb << '|' << L.multiplicity << '|';
+    for (int i : L.energy_order) s << i << ',';
     return s.str();
 }
 
@@ -208,6 +209,7 @@ struct Problem {
     bool have_c = false;
     std::shared_ptr<DeviceTables> T;
     std::vector<std::array<double, 8>> trace;
+    std::vector<double> energies;  // active orbital energies, if the caller gave them
 
     DeviceTables& tables() {
         if (!T) T = get_tables(L, device);
@@ -1191,6 +1193,25 @@ int v2g_apply_AT_batched_device(v2g_handle* h, int nvec, const double* u, double
     return apply_batched(h, nvec, u, out, stream, true);
 }
 
+int v2g_set_active_orbital_energies(v2g_handle* h, const double* energies) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !energies) return v2g::fail(V2G_ERR_ARG, "null argument");
+        Problem& P = h->P;
+        std::vector<int> order(P.L.amo);
+        for (int i = 0; i < P.L.amo; i++) order[i] = i;
+        // the reference takes the first strict minimum (basis.cc:211-238): ties keep Pitzer order
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return energies[a] < energies[b]; });
+        v2g::Layout L;
+        std::string err = v2g::build_layout(P.L.opt, P.L.nirrep, P.L.amopi, P.L.na, P.L.nb, P.L.multiplicity, L, order);
+        if (!err.empty()) return v2g::fail(V2G_ERR_ARG, err);
+        if (L.dimx != P.L.dimx || L.ncon != P.L.ncon) return v2g::fail(V2G_ERR_ARG, "internal error: layout changed size");
+        P.L = std::move(L);
+        P.T.reset();  // device tables are rebuilt for the new pair numbering
+        P.energies.assign(energies, energies + P.L.amo);
+        return V2G_OK;
+    });
+}
+
 int v2g_spatial_density_dims(const v2g_handle* h, long* d1_dim, long* d2_dim) {
     return v2g::guarded([&]() -> int {
         if (!h || !d1_dim || !d2_dim) return v2g::fail(V2G_ERR_ARG, "null argument");
@@ -1217,7 +1238,8 @@ int v2g_pack_spatial_density(v2g_handle* h, const double* active_energies, doubl
         if ((int64_t)P.x.size() != P.L.dimx) return v2g::fail(V2G_ERR_ARG, "the handle has no primal state");
         v2g::Csr M;
         int64_t n1 = 0, n2 = 0;
-        v2g::build_spatial_map(P.L, active_energies, M, n1, n2);
+        v2g::build_spatial_map(P.L, active_energies ? active_energies : (P.energies.empty() ? nullptr : P.energies.data()),
+                               M, n1, n2);
         CK(cudaSetDevice(P.device));
         v2g::MapTable T;
         T.build(M);

@@ -294,6 +294,16 @@ def run_gpu(args):
                          "oiter": int(r["oiter"])} for k, r in enumerate(results) if r["status"] != 0],
         "wall_s": wall,
     }
+    # energies against a recorded solve of the same instances from the reference's
+    # start (the metric asks for |E - E_FP64| <= 1e-6 Eh per instance)
+    if world == 1 and args.workload == "batch256" and args.count == 256 and os.path.exists(ITER_FILE):
+        rec = json.load(open(ITER_FILE))
+        if "energies" in rec:
+            d = [abs(results[k]["e_total"] - rec["energies"][mine[k]]) for k in range(len(results))
+                 if results[k]["status"] == 0 and rec["status"][mine[k]] == 0]
+            out["energy_check"] = {"against": "recorded FP64 solve from the reference's random start",
+                                   "instances": len(d), "max_abs_diff_Eh": max(d) if d else None,
+                                   "within_1e-6": int(sum(x <= 1e-6 for x in d))}
     if clocks:
         out["clocks"] = clocks
     if world > 1:
@@ -312,6 +322,8 @@ def run_gpu(args):
             os.makedirs(os.path.dirname(ITER_FILE), exist_ok=True)
             json.dump({"workload": args.workload, "count": args.count,
                        "outer_iterations": [int(r["oiter"]) for r in results],
+                       "energies": [float(r["e_total"]) for r in results],
+                       "status": [int(r["status"]) for r in results],
                        "n": [int(a.n) for a in all_spaces]}, open(ITER_FILE, "w"))
         print(json.dumps(out))
 

@@ -73,7 +73,26 @@ def workload(name, count):
     if name.startswith("uniform"):  # uniformN: count instances of n = N (experiments)
         n = int(name[len("uniform"):])
         return [synthetic(n, s) for s in range(count)]
+    if name == "h10":  # linear H10, 0.9 A, STO-3G RHF orbitals, all active
+        from v2rdm_casscf_b200.hchain import hydrogen_chain
+
+        return [hydrogen_chain(10, 0.9)]
+    if name == "h20scan":  # symmetric H20 dissociation scan, spacings 0.6..3.0 A
+        from v2rdm_casscf_b200.hchain import hydrogen_scan
+
+        return hydrogen_scan(20, 0.6, 3.0, count if count != 256 else 64)
     raise SystemExit(f"unknown workload {name}")
+
+
+def workload_text(args, count):
+    opts = "C1, DQG, CONSTRAIN_SPIN, E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6"
+    if args.workload == "batch256":
+        return f"batch256: {count} synthetic active spaces n~U{{8..20}}, singlet N=n (n-1 for odd n), " + opts
+    if args.workload == "h10":
+        return "h10: linear H10, 0.9 A, STO-3G RHF orbitals, (10e,10o) all active, " + opts
+    if args.workload == "h20scan":
+        return f"h20scan: {count} linear H20 geometries, spacing 0.6..3.0 A, STO-3G RHF orbitals, (20e,20o), " + opts
+    return f"{args.workload}: {count} synthetic active spaces, " + opts
 
 
 def dist_env():
@@ -251,11 +270,12 @@ def run_gpu(args):
         "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded Philox active spaces; no public dataset involved)",
+        "data": ("generated (STO-3G hydrogen-chain integrals and RHF computed in the project; no dataset involved)"
+                 if args.workload.startswith("h") else
+                 "synthetic (seeded Philox active spaces; no public dataset involved)"),
         "config": {
-            "workload": f"{args.workload}: {args.count} synthetic active spaces n~U{{8..20}}, singlet N=n (n-1 for odd n), C1, DQG, "
-                        "CONSTRAIN_SPIN, E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6",
-            "instances": args.count,
+            "workload": workload_text(args, len(all_spaces)),
+            "instances": len(all_spaces),
             "precision": "FP64 (maps, CG, projection)",
             "projection": args.projection,
             "cg_tolerance_factor": args.cg_factor,
@@ -406,7 +426,7 @@ def cpu_baseline(spaces, oiters, sample_sizes):
     by_n = {}
     for a in spaces:
         by_n.setdefault(a.n, a)
-    sample = [n for n in sample_sizes if n in by_n]
+    sample = [n for n in sample_sizes if n in by_n] or sorted(by_n)[:4]
     t0 = time.time()
     per_it = {}
     for n in sample:
@@ -415,7 +435,10 @@ def cpu_baseline(spaces, oiters, sample_sizes):
     # power-law fit t(n) = a n^p over the sampled sizes for the others
     xs = np.log(np.array(sample, dtype=float))
     ys = np.log(np.array([per_it[n] for n in sample]))
-    p, lna = np.polyfit(xs, ys, 1)
+    if len(sample) > 1:
+        p, lna = np.polyfit(xs, ys, 1)
+    else:  # one size only: every instance has it
+        p, lna = 0.0, float(ys[0])
     total = 0.0
     for a, k in zip(spaces, oiters):
         t = per_it.get(a.n, float(np.exp(lna) * a.n ** p))
@@ -451,8 +474,8 @@ def run_reference(args):
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": f"{args.workload}: {args.count} synthetic active spaces (see GPU arm)",
-                      "instances": args.count, "mu_update_frequency": args.mu_freq,
+           "config": {"workload": workload_text(args, len(spaces)),
+                      "instances": len(spaces), "mu_update_frequency": args.mu_freq,
                       "note": "reference CPU path (oracle/_ref) with the same options; time per outer iteration "
                               "sampled, times the outer-iteration counts the GPU solve needed with those options"},
            "cpu_baseline": base,

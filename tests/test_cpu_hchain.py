@@ -38,3 +38,13 @@ def test_h10_chain_active_space():
     occ = range(5)
     e = a.enuc + sum(2 * a.h[i, i] for i in occ) + sum(2 * g[i, i, j, j] - g[i, j, j, i] for i in occ for j in occ)
     assert abs(e - a.scf_energy) < 1e-8
+
+
+def test_dissociation_scan_converges_along_the_curve():
+    from v2rdm_casscf_b200.hchain import hydrogen_scan
+
+    scan = hydrogen_scan(6, 0.6, 3.0, 9)
+    e = [a.scf_energy for a in scan]
+    k = int(np.argmin(e))
+    assert 0 < k < len(e) - 1  # a minimum inside the range
+    assert all(e[i] < e[i + 1] for i in range(k, len(e) - 1))  # rising towards dissociation

@@ -87,44 +87,63 @@ def nuclear_repulsion(coords):
     return e
 
 
-def rhf(S, Hcore, eri, nocc, max_iter=500, conv=1e-12):
-    """Closed-shell RHF with DIIS; returns (energy without enuc, C, orbital energies)."""
+def rhf(S, Hcore, eri, nocc, max_iter=3000, conv=1e-10, guess=None, damping=0.7):
+    """Closed-shell RHF; returns (energy without enuc, C, orbital energies).
+
+    While the orbital gradient is large the density is damped (the Fock
+    matrix is built from damping * D_old + (1 - damping) * D_new); close to
+    convergence DIIS on the gradient commutator takes over.  guess: starting MO
+    coefficients (e.g. from a neighbouring geometry).  Raises if the
+    commutator does not fall below 1e-8."""
     s, U = np.linalg.eigh(S)
     X = U @ np.diag(s ** -0.5) @ U.T
-    e, Cp = np.linalg.eigh(X.T @ Hcore @ X)
-    C = X @ Cp
+    if guess is None:
+        e, Cp = np.linalg.eigh(X.T @ Hcore @ X)
+        C = X @ Cp
+    else:
+        C = guess
+    D = C[:, :nocc] @ C[:, :nocc].T
     focks, errs = [], []
     E_old = 0.0
+    converged = False
     for _ in range(max_iter):
-        D = C[:, :nocc] @ C[:, :nocc].T
         J = np.einsum("pqrs,rs->pq", eri, D)
         Kx = np.einsum("prqs,rs->pq", eri, D)
         F = Hcore + 2.0 * J - Kx
         E = float(np.sum(D * (Hcore + F)))
         err = X.T @ (F @ D @ S - S @ D @ F) @ X
-        focks.append(F)
-        errs.append(err)
-        if len(focks) > 8:
-            focks.pop(0)
-            errs.pop(0)
-        m = len(focks)
-        Bm = -np.ones((m + 1, m + 1))
-        Bm[m, m] = 0.0
-        for i in range(m):
-            for j in range(m):
-                Bm[i, j] = np.sum(errs[i] * errs[j])
-        rhs = np.zeros(m + 1)
-        rhs[m] = -1.0
-        try:
-            cvec = np.linalg.solve(Bm, rhs)[:m]
-            F = sum(ci * Fi for ci, Fi in zip(cvec, focks))
-        except np.linalg.LinAlgError:
-            pass
-        e, Cp = np.linalg.eigh(X.T @ F @ X)
-        C = X @ Cp
-        if abs(E - E_old) < conv and np.abs(err).max() < 1e-9:
+        gnorm = np.abs(err).max()
+        if abs(E - E_old) < conv and gnorm < 1e-9:
+            converged = True
             break
         E_old = E
+        Fx = F
+        if gnorm < 1e-2:
+            focks.append(F)
+            errs.append(err)
+            if len(focks) > 8:
+                focks.pop(0)
+                errs.pop(0)
+            m = len(focks)
+            if m > 1:
+                Bm = -np.ones((m + 1, m + 1))
+                Bm[m, m] = 0.0
+                for i in range(m):
+                    for j in range(m):
+                        Bm[i, j] = np.sum(errs[i] * errs[j])
+                rhs = np.zeros(m + 1)
+                rhs[m] = -1.0
+                try:
+                    cvec = np.linalg.solve(Bm, rhs)[:m]
+                    Fx = sum(ci * Fi for ci, Fi in zip(cvec, focks))
+                except np.linalg.LinAlgError:
+                    pass
+        e, Cp = np.linalg.eigh(X.T @ Fx @ X)
+        C = X @ Cp
+        Dn = C[:, :nocc] @ C[:, :nocc].T
+        D = Dn if gnorm < 1e-2 else damping * D + (1.0 - damping) * Dn
+    if not converged:
+        raise RuntimeError("RHF did not converge")
     return E, C, e
 
 
@@ -149,15 +168,17 @@ def pivoted_cholesky(M, tol):
     return np.array(vecs)
 
 
-def hydrogen_chain(natoms, spacing_angstrom, cd_tolerance=1e-10):
-    """ActiveSpace of an H_natoms chain: all RHF orbitals active, N = natoms (singlet)."""
+def hydrogen_chain(natoms, spacing_angstrom, cd_tolerance=1e-10, guess=None):
+    """ActiveSpace of an H_natoms chain: all RHF orbitals active, N = natoms (singlet).
+
+    guess: RHF MO coefficients to start from (a neighbouring geometry's)."""
     if natoms % 2:
         raise ValueError("closed-shell chains only (even natoms)")
     coords = chain_geometry(natoms, spacing_angstrom)
     S, T, V, eri = ao_integrals(coords)
     Hc = T + V
     enuc = nuclear_repulsion(coords)
-    E, C, eps = rhf(S, Hc, eri, natoms // 2)
+    E, C, eps = rhf(S, Hc, eri, natoms // 2, guess=guess)
     n = natoms
     Lao = pivoted_cholesky(eri.reshape(n * n, n * n), cd_tolerance).reshape(-1, n, n)
     Lmo = np.einsum("pi,Qpq,qj->Qij", C, Lao, C)
@@ -167,4 +188,16 @@ def hydrogen_chain(natoms, spacing_angstrom, cd_tolerance=1e-10):
     a = ActiveSpace(h, Lmo, natoms // 2, natoms // 2, enuc=enuc, name=f"H{natoms} chain {spacing_angstrom} A STO-3G")
     a.scf_energy = E + enuc
     a.orbital_energies = eps
+    a.mo_coefficients = C
     return a
+
+
+def hydrogen_scan(natoms=20, first=0.6, last=3.0, points=64):
+    """The symmetric dissociation scan: spacings linear in [first, last] Angstrom,
+    each RHF started from the previous geometry's orbitals."""
+    out, guess = [], None
+    for r in np.linspace(first, last, points):
+        a = hydrogen_chain(natoms, float(r), guess=guess)
+        guess = a.mo_coefficients
+        out.append(a)
+    return out

@@ -332,6 +332,13 @@ def run_gpu(args):
         dist.destroy_process_group()
     if rank == 0:
         out["outer_iterations"] = {str(k): v for k, v in sorted(oiters.items())}
+        allit = [int(r["oiter"]) for r in results]
+        if allit:
+            # the slowest instance sets the time to solution; seconds per outer
+            # iteration of the batch while it runs
+            out["time_per_outer_iteration_s"] = value / max(allit)
+            out["outer_iterations_summary"] = {"max": max(allit), "median": float(np.median(allit)),
+                                               "total": int(sum(allit))}
         if args.cpu_baseline and world == 1:
             # the reference runs from its own random start: its iteration counts are
             # those of a solve from that start (recorded), else this run's

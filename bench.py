@@ -248,6 +248,11 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         launches, h2d, d2h = int(t[0]), float(t[1]), float(t[2])
     conv = [r["status"] == 0 for r in results]
+    n_conv = int(sum(conv))
+    if world > 1:  # instances converged on all ranks
+        t = torch.tensor([float(n_conv)], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        n_conv = int(t[0])
     if rank == 0:
         oiters = {}
         for i, r in zip(mine, results):
@@ -309,7 +314,7 @@ def run_gpu(args):
             "traffic_source": ROOFLINE_TRAFFIC.get(map_detail["group"], {}).get("source"),
             "launches_timed": map_n,
         },
-        "converged": int(sum(conv)),
+        "converged": n_conv,
         "unconverged": [{"instance": int(mine[k]), "n": int(all_spaces[mine[k]].n), "status": int(r["status"]),
                          "oiter": int(r["oiter"])} for k, r in enumerate(results) if r["status"] != 0],
         "wall_s": wall,

@@ -40,6 +40,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -218,8 +219,9 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clk = Clocks(dev, os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
-                                   f"clocks_rank{rank}.csv")) if args.clocks else None
+    # the raw clock samples go to $V2G_CLOCKS_DIR (default: the temporary directory)
+    clk_dir = os.environ.get("V2G_CLOCKS_DIR", tempfile.gettempdir())
+    clk = Clocks(dev, os.path.join(clk_dir, f"clocks_rank{rank}.csv")) if args.clocks else None
     t0 = time.time()
     dev_s, e2e_s, stats, results = [], [], [], None
     for _ in range(args.steps):

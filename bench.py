@@ -182,7 +182,7 @@ def run_gpu(args):
             opts["MAXITER"] = maxiter
         return [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
                                                 projection=args.projection, cg_tolerance_factor=args.cg_factor,
-                                                start=args.start)
+                                                start=args.start, cg_extrapolate=args.cg_extrapolate)
                 for i in mine]
 
     solvers = make(args.max_outer)
@@ -286,14 +286,16 @@ def run_gpu(args):
             "precision": "FP64 (maps, CG, projection)",
             "projection": args.projection,
             "cg_tolerance_factor": args.cg_factor,
+            "cg_start": "extrapolated y_k + (y_k - y_k-1)" if args.cg_extrapolate else "previous y (the reference's)",
             "mu_update_frequency": args.mu_freq,
             "start": ("least-norm feasible point of A x = b, zero duals, mu 1 (computed on the GPU inside "
                       "the timed solve)") if args.start == "feasible" else "the reference's random start (srand(0))",
             "mode": "plain FP64 (reference algorithm, options and start)"
                     if (args.projection == "exact" and args.cg_factor == 0.01 and args.mu_freq == 500
-                        and args.start == "state")
+                        and args.start == "state" and not args.cg_extrapolate)
                     else "FP64 maps/CG/projection, adaptive projection accuracy"
                          + (", feasible warm start" if args.start == "feasible" else "")
+                         + (", extrapolated CG start" if args.cg_extrapolate else "")
                          + (f", mu update every {args.mu_freq}" if args.mu_freq != 500 else ""),
             "warmup_steps": f"{args.warmup} batched calls capped at {args.warmup_outer} outer iterations",
             "l2": "inputs larger than L2 (no flush needed)",
@@ -513,6 +515,8 @@ def main():
                     help="MU_UPDATE_FREQUENCY (the reference's default is 500)")
     ap.add_argument("--start", default="feasible", choices=["feasible", "state"],
                     help="feasible: least-norm feasible warm start; state: the reference's random start")
+    ap.add_argument("--cg-extrapolate", action="store_true",
+                    help="start each CG from y_k + (y_k - y_k-1) instead of y_k (same stopping test)")
     ap.add_argument("--plain", action="store_true",
                     help="reference algorithm, options and start: exact projection, CG factor 0.01, "
                          "mu update every 500, random start")
@@ -526,6 +530,7 @@ def main():
     args = ap.parse_args()
     if args.plain:
         args.projection, args.cg_factor, args.mu_freq, args.start = "exact", 0.01, 500, "state"
+        args.cg_extrapolate = False
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -79,6 +79,10 @@ typedef struct v2g_options {
                                    TPDM_GUESS=RANDOM, or v2g_set_state); 1: from the least-norm
                                    point of A x = b with zero duals and mu = 1, computed on the
                                    GPU at the start of the solve (no counterpart in the plugin) (0) */
+    int cg_extrapolate;         /* 1: each outer iteration's CG starts from y_k + (y_k - y_{k-1}),
+                                   the linear extrapolation of the last two CG solutions, instead of
+                                   y_k (cg_solver.cc:125 warm-starts from y_k); the stopping test is
+                                   unchanged, so only the CG iteration count changes (0) */
 } v2g_options;
 
 typedef struct v2g_result {

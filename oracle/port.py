@@ -346,18 +346,31 @@ def cg(A, y, rhs, tol, maxiter):
 
 
 def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_maxiter=10000, tau=1.0,
-          mu_update_frequency=500):
-    """The outer loop of v2rdm_solver.cc:1778-1908 (no orbital optimisation)."""
+          mu_update_frequency=500, cg_extrapolate=False):
+    """The outer loop of v2rdm_solver.cc:1778-1908 (no orbital optimisation).
+
+    cg_extrapolate: the product's option of that name; from the third outer
+    iteration on, CG starts from y_k + (y_k - y_{k-1}) (the last two CG
+    solutions) instead of y_k, with the same stopping test.
+    """
     mu = 1.0
     ep = ed = 0.0
     oiter = 0
+    iiter = 0
+    starts = []  # the y each CG started from, before extrapolation
     while True:
         Ax = -tau * mu * (A @ x - b)
         z = c - z
         B = A @ z + Ax
         tol = 0.01 if oiter == 0 else 0.01 * min(ep, ed)
         tol = max(tol, cg_conv)
-        y, _ = cg(A, y, B, tol, cg_maxiter)
+        if cg_extrapolate:
+            y0 = y if len(starts) < 2 else y + (y - starts[-1])
+            starts.append(y)
+        else:
+            y0 = y
+        y, k = cg(A, y0, B, tol, cg_maxiter)
+        iiter += k
         x, z = update_xz(A, L, x, y, c, mu)
         ed = np.linalg.norm(A.T @ y + z - c)
         ep = np.linalg.norm(A @ x - b)
@@ -366,7 +379,8 @@ def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_m
         ep_energy, ed_energy = c @ x, b @ y
         oiter += 1
         if oiter == maxiter:
-            return dict(converged=False, e_primal=ep_energy, e_dual=ed_energy, oiter=oiter, x=x, y=y, z=z)
-        if not (ep > r_conv or ed > r_conv or abs(ep_energy - ed_energy) > e_conv):
-            return dict(converged=True, e_primal=ep_energy, e_dual=ed_energy, oiter=oiter, ep=ep, ed=ed, x=x, y=y,
+            return dict(converged=False, e_primal=ep_energy, e_dual=ed_energy, oiter=oiter, iiter=iiter, x=x, y=y,
                         z=z)
+        if not (ep > r_conv or ed > r_conv or abs(ep_energy - ed_energy) > e_conv):
+            return dict(converged=True, e_primal=ep_energy, e_dual=ed_energy, oiter=oiter, iiter=iiter, ep=ep, ed=ed,
+                        x=x, y=y, z=z)

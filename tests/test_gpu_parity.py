@@ -176,6 +176,29 @@ def test_cg_tolerance_factor_reaches_the_same_energy(v2g):
     assert s.result["iiter"] < int(g["iiter"])
 
 
+def test_cg_extrapolation_reaches_the_same_energy(v2g):
+    # cg_extrapolate: CG starts from y_k + (y_k - y_{k-1}) with the reference's
+    # stopping test, so the energy is the reference's and CG needs fewer
+    # iterations.  Solved in one group with two instances that do not
+    # extrapolate: the mode is per instance.
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    opts = dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]))
+    solvers = []
+    for seed, ex in ((int(g["seed"]), True), (int(g["seed"]), False), (1, False)):
+        s = v2g.V2RDMSolver.from_active_space(synthetic(4, seed), options=opts, cg_extrapolate=ex)
+        s.guess()
+        solvers.append(s)
+    res = v2g.solve_batch(solvers)
+    assert all(r["status"] == 0 for r in res)
+    assert abs(res[0]["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert abs(res[1]["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert res[0]["iiter"] < res[1]["iiter"]
+    g1 = load(os.path.join(GOLDEN, "solve_synthetic_n4_s1.npz"))
+    assert abs(res[2]["e_total"] - float(g1["e_primal"])) <= 1e-6
+
+
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "pack_*.npz"))),
                          ids=lambda p: os.path.basename(p))
 def test_spatial_density_matches_reference(v2g, path):

@@ -61,6 +61,7 @@ class Options(ctypes.Structure):
         ("constrain_d3", ctypes.c_int),
         ("constrain_d4", ctypes.c_int),
         ("start", ctypes.c_int),
+        ("cg_extrapolate", ctypes.c_int),
     ]
 
 
@@ -208,12 +209,15 @@ class V2RDMSolver:
     eigendecomposition whose residual is below 0.01 min(eps(p), eps(d)) (the
     CG tolerance rule); the default "exact" converges every projection, as
     the plugin does.  ``cg_tolerance_factor`` replaces the 0.01 of the CG
-    tolerance rule 0.01 min(eps(p), eps(d)).
+    tolerance rule 0.01 min(eps(p), eps(d)).  ``cg_extrapolate=True`` starts
+    each outer iteration's CG from y_k + (y_k - y_{k-1}) instead of y_k (same
+    stopping test, fewer CG iterations).
     """
 
     def __init__(self, active, nalpha, nbeta, multiplicity=1, frozen_docc=None, restricted_docc=None,
                  restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False,
-                 profile=False, projection="exact", cg_tolerance_factor=0.01, start="state"):
+                 profile=False, projection="exact", cg_tolerance_factor=0.01, start="state",
+                 cg_extrapolate=False):
         L = lib()
         self.active = list(active)
         opts = dict(DEFAULT_OPTIONS)
@@ -250,6 +254,7 @@ class V2RDMSolver:
         if start not in ("state", "feasible"):
             raise ValueError("start is 'state' (guess()/set_state) or 'feasible'")
         o.start = int(start == "feasible")
+        o.cg_extrapolate = int(bool(cg_extrapolate))
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)

@@ -87,6 +87,9 @@ void launch_cg_update_yr(int64_t n, int B, double* y, double* r, const double* p
 void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cudaStream_t s);
 // p = beta p + r
 void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s);
+// CG start extrapolation over [e * B + b]: where mode[b] == 2,
+// y <- y + (y - yprev); where mode[b] >= 1, yprev <- y (its value on entry)
+void launch_cg_extrapolate(int64_t n, int B, double* y, double* yprev, const int* mode, cudaStream_t s);
 // rr <- initial r.r
 void launch_cg_set_rr(int B, CgScalars* cs, const double* rr, int* n_active, cudaStream_t s);
 

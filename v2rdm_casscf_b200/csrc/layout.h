@@ -53,6 +53,11 @@ struct Options {
     // Start the solve from the least-norm point of {A x = b} (x = A^T w with
     // A A^T w = b, y = z = 0, mu = 1) instead of the handle's state.
     bool feasible_start = false;
+    // Start each outer iteration's CG from y_k + (y_k - y_{k-1}), the linear
+    // extrapolation of the last two CG solutions, instead of from y_k.  CG
+    // still stops on the same residual test, so only its iteration count
+    // changes.
+    bool cg_extrapolate = false;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for

@@ -326,6 +326,19 @@ __global__ void c_minus_z_kernel(int64_t n, int B, const double* __restrict__ c,
     }
 }
 
+__global__ void cg_extrapolate_kernel(int64_t n, int B, double* __restrict__ y, double* __restrict__ yprev,
+                                      const int* __restrict__ mode) {
+    const int64_t total = n * B;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int m = mode[(int)(t % B)];
+        if (m == 0) continue;
+        const double v = y[t];
+        if (m == 2) y[t] = v + (v - yprev[t]);
+        yprev[t] = v;
+    }
+}
+
 __global__ void cg_init_kernel(int64_t n, int B, const double* __restrict__ rhs, const double* __restrict__ Ap,
                                double* __restrict__ r, double* __restrict__ p, const CgScalars* __restrict__ cs) {
     const int64_t total = n * B;
@@ -501,6 +514,11 @@ void launch_reduce(ReduceMode mode, int64_t n, int B, const double* u, const dou
 
 void launch_set_rows(int64_t n, int B, const double* row, double* out, const int* mask, cudaStream_t s) {
     set_rows_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, row, out, mask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_cg_extrapolate(int64_t n, int B, double* y, double* yprev, const int* mode, cudaStream_t s) {
+    cg_extrapolate_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, y, yprev, mode);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -247,6 +247,11 @@ class GroupRun {
         mask_.alloc(B_);
         cs_.alloc(B_);
         nact_.alloc(8);  // counters: CG, Jacobi, refinement, fallback, restart
+        for (auto* p : P_) extrapolate_ = extrapolate_ || p->opt.cg_extrapolate;
+        if (extrapolate_) {
+            yprev_.alloc(C);
+            ex_.alloc(B_);
+        }
         CK(cudaMallocHost(&hscal_, sizeof(double) * 4 * B_));
         CK(cudaMallocHost(&hnact_, sizeof(int) * 8));
         build_projection_plan();
@@ -452,6 +457,8 @@ class GroupRun {
         }
         // an instance whose iterate turns non-finite restarts (at most twice)
         std::vector<int> restarts_left(B_, 2), recover(B_, 0);
+        // CG solutions seen per instance since its (re)start, for cg_extrapolate
+        std::vector<int> ycount(B_, 0), exmode(B_, 0);
         int it = 0;
         while (true) {
             if (std::find(recover.begin(), recover.end(), 1) != recover.end()) {
@@ -461,6 +468,7 @@ class GroupRun {
                         mu[b] = 1.0;
                         iiter[b] += cs[b].iter;
                         recover[b] = 0;
+                        ycount[b] = 0;
                     }
                 warm_ = false;  // every large block of the group starts its projection cold again
             }
@@ -491,6 +499,16 @@ class GroupRun {
                 cs[b].maxiter = o.cg_maxiter;
             }
             CK(cudaMemcpyAsync(cs_.p, cs.data(), B_ * sizeof(CgScalars), cudaMemcpyHostToDevice, s_));
+            // CG starts from y_k + (y_k - y_{k-1}) once two CG solutions exist
+            // (mode 2); before that it only records y_k (mode 1)
+            if (extrapolate_) {
+                for (int b = 0; b < B_; b++) {
+                    exmode[b] = (active[b] && opt(b).cg_extrapolate) ? (ycount[b] >= 2 ? 2 : 1) : 0;
+                    if (exmode[b]) ycount[b]++;
+                }
+                CK(cudaMemcpyAsync(ex_.p, exmode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+                launch_cg_extrapolate(nc_, B_, y_.p, yprev_.p, ex_.p, s_);
+            }
             cg_solve();
             CK(cudaMemcpyAsync(cs.data(), cs_.p, B_ * sizeof(CgScalars), cudaMemcpyDeviceToHost, s_));
             CK(cudaEventRecord(e1, s_));
@@ -836,6 +854,11 @@ class GroupRun {
     DevBuf<double> c_, x_, z_, aty_, atp_, y_, ax_, bv_, r_, p_, ap_, partial_, red_, mu_, coef_;
     DevBuf<int> mask_, nact_;
     DevBuf<CgScalars> cs_;
+    // CG start extrapolation (cg_extrapolate): the previous CG start and the
+    // per-instance mode of the extrapolation kernel
+    DevBuf<double> yprev_;
+    DevBuf<int> ex_;
+    bool extrapolate_ = false;
     double* hscal_ = nullptr;
     int* hnact_ = nullptr;
     // projection plan
@@ -921,6 +944,7 @@ void v2g_default_options(v2g_options* o) {
     o->constrain_d3 = 0;
     o->constrain_d4 = 0;
     o->start = 0;
+    o->cg_extrapolate = 0;
 }
 
 const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
@@ -950,6 +974,9 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         o.constrain_d3 = opt->constrain_d3 != 0 || o.constrain_d4;  // v2rdm_solver.cc:527-532
         if (opt->start != 0 && opt->start != 1) return v2g::fail(V2G_ERR_ARG, "start must be 0 or 1");
         o.feasible_start = opt->start == 1;
+        if (opt->cg_extrapolate != 0 && opt->cg_extrapolate != 1)
+            return v2g::fail(V2G_ERR_ARG, "cg_extrapolate must be 0 or 1");
+        o.cg_extrapolate = opt->cg_extrapolate == 1;
         if (!(o.cg_tol_factor > 0.0 && o.cg_tol_factor < 1.0))
             return v2g::fail(V2G_ERR_ARG, "cg_tolerance_factor must be in (0, 1)");
         if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)

@@ -199,6 +199,21 @@ def test_cg_extrapolation_reaches_the_same_energy(v2g):
     assert abs(res[2]["e_total"] - float(g1["e_primal"])) <= 1e-6
 
 
+def test_tau_parameter_reaches_the_same_energy(v2g):
+    # TAU_PARAMETER at the top of the plugin's documented range [1.0, 1.6]
+    # (plugin.cc:94-97) changes the path, not the answer
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    s = v2g.V2RDMSolver.from_active_space(
+        synthetic(4, int(g["seed"])),
+        options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]), TAU_PARAMETER=1.6),
+        start="feasible")
+    e = s.compute_energy()
+    assert s.result["status"] == 0
+    assert abs(e - float(g["e_primal"])) <= 1e-6
+
+
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "pack_*.npz"))),
                          ids=lambda p: os.path.basename(p))
 def test_spatial_density_matches_reference(v2g, path):

@@ -182,7 +182,8 @@ def run_gpu(args):
             opts["MAXITER"] = maxiter
         return [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
                                                 projection=args.projection, cg_tolerance_factor=args.cg_factor,
-                                                start=args.start, cg_extrapolate=args.cg_extrapolate)
+                                                start=args.start, cg_extrapolate=args.cg_extrapolate,
+                                                anderson_memory=args.anderson)
                 for i in mine]
 
     solvers = make(args.max_outer)
@@ -289,16 +290,19 @@ def run_gpu(args):
             "cg_start": "extrapolated y_k + (y_k - y_k-1)" if args.cg_extrapolate else "previous y (the reference's)",
             "mu_update_frequency": args.mu_freq,
             "tau_parameter": args.tau,
+            "anderson_memory": args.anderson,
             "start": ("least-norm feasible point of A x = b, zero duals, mu 1 (computed on the GPU inside "
                       "the timed solve)") if args.start == "feasible" else "the reference's random start (srand(0))",
             "mode": "plain FP64 (reference algorithm, options and start)"
                     if (args.projection == "exact" and args.cg_factor == 0.01 and args.mu_freq == 500
-                        and args.start == "state" and not args.cg_extrapolate and args.tau == 1.0)
+                        and args.start == "state" and not args.cg_extrapolate and args.tau == 1.0
+                        and args.anderson == 0)
                     else "FP64 maps/CG/projection, adaptive projection accuracy"
                          + (", feasible warm start" if args.start == "feasible" else "")
                          + (", extrapolated CG start" if args.cg_extrapolate else "")
                          + (f", mu update every {args.mu_freq}" if args.mu_freq != 500 else "")
-                         + (f", TAU_PARAMETER {args.tau}" if args.tau != 1.0 else ""),
+                         + (f", TAU_PARAMETER {args.tau}" if args.tau != 1.0 else "")
+                         + (f", Anderson acceleration (memory {args.anderson})" if args.anderson else ""),
             "warmup_steps": f"{args.warmup} batched calls capped at {args.warmup_outer} outer iterations",
             "l2": "inputs larger than L2 (no flush needed)",
             "parallelism": f"instances bin-packed over {world} rank(s) by modelled cost, no exchange",
@@ -519,6 +523,8 @@ def main():
                     help="feasible: least-norm feasible warm start; state: the reference's random start")
     ap.add_argument("--tau", type=float, default=1.0,
                     help="TAU_PARAMETER (the plugin's default 1.0; its documented range is [1.0, 1.6])")
+    ap.add_argument("--anderson", type=int, default=0,
+                    help="Anderson acceleration of the outer iteration with this memory (0 = off)")
     ap.add_argument("--cg-extrapolate", action="store_true",
                     help="start each CG from y_k + (y_k - y_k-1) instead of y_k (same stopping test)")
     ap.add_argument("--plain", action="store_true",
@@ -534,7 +540,7 @@ def main():
     args = ap.parse_args()
     if args.plain:
         args.projection, args.cg_factor, args.mu_freq, args.start = "exact", 0.01, 500, "state"
-        args.cg_extrapolate, args.tau = False, 1.0
+        args.cg_extrapolate, args.tau, args.anderson = False, 1.0, 0
     if args.impl == "reference":
         run_reference(args)
     else:

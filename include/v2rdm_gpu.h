@@ -83,6 +83,12 @@ typedef struct v2g_options {
                                    the linear extrapolation of the last two CG solutions, instead of
                                    y_k (cg_solver.cc:125 warm-starts from y_k); the stopping test is
                                    unchanged, so only the CG iteration count changes (0) */
+    int anderson_memory;        /* m > 0: Anderson acceleration of the outer iteration: the next
+                                   (x, z) is the step's result minus the combination of the last m
+                                   step differences that minimises the fixed-point residual; the
+                                   stopping test and the energies are taken on the un-accelerated
+                                   step as in the plugin; the history restarts when mu changes;
+                                   0 = off, at most 16 (0) */
 } v2g_options;
 
 typedef struct v2g_result {

@@ -346,19 +346,28 @@ def cg(A, y, rhs, tol, maxiter):
 
 
 def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_maxiter=10000, tau=1.0,
-          mu_update_frequency=500, cg_extrapolate=False):
+          mu_update_frequency=500, cg_extrapolate=False, anderson_memory=0):
     """The outer loop of v2rdm_solver.cc:1778-1908 (no orbital optimisation).
 
     cg_extrapolate: the product's option of that name; from the third outer
     iteration on, CG starts from y_k + (y_k - y_{k-1}) (the last two CG
     solutions) instead of y_k, with the same stopping test.
+
+    anderson_memory: the product's option of that name (Anderson's method,
+    type II, on w = (x, z)).  After each step g = (x', z') from w, f = g - w;
+    with difference columns dF_j = f_{j+1} - f_j and dG_j = g_{j+1} - g_j of
+    the last m steps, the next state is g - dG gamma, where
+    (dF^T dF + 1e-10 tr(dF^T dF) I) gamma = dF^T f.  The stopping test and the
+    energies are those of g; the history restarts whenever mu changes.
     """
     mu = 1.0
     ep = ed = 0.0
     oiter = 0
     iiter = 0
     starts = []  # the y each CG started from, before extrapolation
+    hist_w, hist_f = [], []  # Anderson history: states and residuals
     while True:
+        x_in, z_in = x, z
         Ax = -tau * mu * (A @ x - b)
         z = c - z
         B = A @ z + Ax
@@ -371,11 +380,14 @@ def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_m
             y0 = y
         y, k = cg(A, y0, B, tol, cg_maxiter)
         iiter += k
+        w = np.concatenate([x_in, z_in]) if anderson_memory else None
         x, z = update_xz(A, L, x, y, c, mu)
         ed = np.linalg.norm(A.T @ y + z - c)
         ep = np.linalg.norm(A @ x - b)
+        mu_changed = False
         if oiter % mu_update_frequency == 0 and oiter > 0:
             mu = mu * ep / ed
+            mu_changed = True
         ep_energy, ed_energy = c @ x, b @ y
         oiter += 1
         if oiter == maxiter:
@@ -384,3 +396,21 @@ def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_m
         if not (ep > r_conv or ed > r_conv or abs(ep_energy - ed_energy) > e_conv):
             return dict(converged=True, e_primal=ep_energy, e_dual=ed_energy, oiter=oiter, iiter=iiter, ep=ep, ed=ed,
                         x=x, y=y, z=z)
+        if anderson_memory:
+            if mu_changed:
+                hist_w, hist_f = [], []
+            g = np.concatenate([x, z])
+            hist_w.append(w)
+            hist_f.append(g - w)
+            if len(hist_w) > anderson_memory + 1:
+                hist_w.pop(0)
+                hist_f.pop(0)
+            if len(hist_f) >= 2:
+                dF = np.stack([hist_f[i + 1] - hist_f[i] for i in range(len(hist_f) - 1)], axis=1)
+                dG = np.stack([(hist_w[i + 1] + hist_f[i + 1]) - (hist_w[i] + hist_f[i])
+                               for i in range(len(hist_f) - 1)], axis=1)
+                M = dF.T @ dF
+                M = M + (1e-10 * np.trace(M) + 1e-300) * np.eye(M.shape[0])
+                gamma = np.linalg.solve(M, dF.T @ hist_f[-1])
+                g = g - dG @ gamma
+                x, z = g[:L.dimx], g[L.dimx:]

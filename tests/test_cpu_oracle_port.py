@@ -75,6 +75,26 @@ def test_port_cg_extrapolation_same_energy_fewer_cg_iterations():
     assert extr["iiter"] <= 0.7 * plain["iiter"]
 
 
+@pytest.mark.parametrize("m", [5, 10])
+def test_port_anderson_same_energy_fewer_outer_iterations(m):
+    # the product's anderson_memory option, restated in the port: same
+    # stopping test on the plain step, so the reference's energy, in a
+    # fraction of the outer iterations (about 2-5x fewer at n = 4..8)
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    a = synthetic(4, int(g["seed"]))
+    L = port.Layout(4, a.na, a.nb)
+    A = port.build_A(L)
+    b = port.build_b(L, A.shape[0])
+    c = port.build_c(L, a.h, a.eri())
+    x, y, z = port.random_guess(L.dimx, A.shape[0])
+    out = port.solve(L, A, b, c, x, y, z, float(g["r_conv"]), float(g["e_conv"]), anderson_memory=m)
+    assert out["converged"]
+    assert abs(out["e_primal"] - float(g["e_primal"])) <= 1e-6
+    assert out["oiter"] <= 0.6 * int(g["oiter"])
+
+
 def test_port_agrees_with_product_table(v2g):
     L = port.Layout(5, 3, 2, 2)
     A = port.build_A(L)

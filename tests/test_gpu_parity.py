@@ -199,6 +199,29 @@ def test_cg_extrapolation_reaches_the_same_energy(v2g):
     assert abs(res[2]["e_total"] - float(g1["e_primal"])) <= 1e-6
 
 
+def test_anderson_acceleration_reaches_the_same_energy(v2g):
+    # anderson_memory: the stopping test and energies are the plain step's, so
+    # the reference's energy is reached, in far fewer outer iterations.  One
+    # group holds instances with memories 10, 5 and 0 (per-instance history
+    # rings inside one allocation of 10 columns).
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    opts = dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]))
+    solvers = []
+    for m in (10, 5, 0):
+        s = v2g.V2RDMSolver.from_active_space(synthetic(4, int(g["seed"])), options=opts, anderson_memory=m,
+                                              cg_extrapolate=m > 0)
+        s.guess()
+        solvers.append(s)
+    res = v2g.solve_batch(solvers)
+    assert all(r["status"] == 0 for r in res)
+    for r in res:
+        assert abs(r["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert res[0]["oiter"] <= 0.6 * res[2]["oiter"]
+    assert res[1]["oiter"] <= 0.8 * res[2]["oiter"]
+
+
 def test_tau_parameter_reaches_the_same_energy(v2g):
     # TAU_PARAMETER at the top of the plugin's documented range [1.0, 1.6]
     # (plugin.cc:94-97) changes the path, not the answer

@@ -62,6 +62,7 @@ class Options(ctypes.Structure):
         ("constrain_d4", ctypes.c_int),
         ("start", ctypes.c_int),
         ("cg_extrapolate", ctypes.c_int),
+        ("anderson_memory", ctypes.c_int),
     ]
 
 
@@ -211,13 +212,16 @@ class V2RDMSolver:
     the plugin does.  ``cg_tolerance_factor`` replaces the 0.01 of the CG
     tolerance rule 0.01 min(eps(p), eps(d)).  ``cg_extrapolate=True`` starts
     each outer iteration's CG from y_k + (y_k - y_{k-1}) instead of y_k (same
-    stopping test, fewer CG iterations).
+    stopping test, fewer CG iterations).  ``anderson_memory=m`` (1..16)
+    accelerates the outer iteration on (x, z) with the last m step
+    differences (Anderson's method; the stopping test and energies are those
+    of the plain step).
     """
 
     def __init__(self, active, nalpha, nbeta, multiplicity=1, frozen_docc=None, restricted_docc=None,
                  restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False,
                  profile=False, projection="exact", cg_tolerance_factor=0.01, start="state",
-                 cg_extrapolate=False):
+                 cg_extrapolate=False, anderson_memory=0):
         L = lib()
         self.active = list(active)
         opts = dict(DEFAULT_OPTIONS)
@@ -255,6 +259,7 @@ class V2RDMSolver:
             raise ValueError("start is 'state' (guess()/set_state) or 'feasible'")
         o.start = int(start == "feasible")
         o.cg_extrapolate = int(bool(cg_extrapolate))
+        o.anderson_memory = int(anderson_memory)
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)

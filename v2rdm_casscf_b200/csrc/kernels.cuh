@@ -93,6 +93,28 @@ void launch_cg_extrapolate(int64_t n, int B, double* y, double* yprev, const int
 // rr <- initial r.r
 void launch_cg_set_rr(int B, CgScalars* cs, const double* rr, int* n_active, cudaStream_t s);
 
+// ---- Anderson acceleration of the outer iteration --------------------------
+// The state w = (x, z) of one instance is the 2 * nx rows e < nx of x and
+// e >= nx of z, interleaved [e * B + b] like every vector; the history holds
+// m difference columns dF_j = f_{k+1} - f_k and dG_j = g_{k+1} - g_k (f = g - w,
+// g = the iterate the step produced), each 2 * nx * B doubles, column j at
+// j * 2 * nx * B.
+constexpr int kAndersonMax = 16;
+// w <- (x, z) for the instances with mode[b] != 0
+void launch_aa_save(int64_t nx, int B, const double* x, const double* z, double* w, const int* mode, cudaStream_t s);
+// f = g - w; mode[b] == 2: dF[slot[b]] = f - fprev, dG[slot[b]] = g - gprev and
+// dots[(2 j) * B + b] = dF[slot].dF[j], dots[(2 j + 1) * B + b] = dF[j].f for j < m;
+// mode[b] >= 1: fprev = f, gprev = g.  partial holds aa_partial_size(nx, B, m)
+// doubles; the sums are deterministic.
+void launch_aa_update(int64_t nx, int B, int m, const double* x, const double* z, const double* w, double* fprev,
+                      double* gprev, double* dF, double* dG, const int* mode, const int* slot, double* partial,
+                      double* dots, cudaStream_t s);
+int64_t aa_partial_size(int64_t nx, int B, int m);
+// (x, z) <- g - sum_j gamma[b * m + j] dG_j for the instances with mix[b] set
+// (columns with gamma 0 are not read)
+void launch_aa_mix(int64_t nx, int B, int m, double* x, double* z, const double* dG, const double* gamma,
+                   const int* mix, cudaStream_t s);
+
 // ---- projection (Update_xz) ----------------------------------------------
 
 // Description of one PSD block of one instance.

@@ -58,6 +58,10 @@ struct Options {
     // still stops on the same residual test, so only its iteration count
     // changes.
     bool cg_extrapolate = false;
+    // Anderson acceleration (type II) of the outer iteration on (x, z) with
+    // this many difference columns; 0 = off.  The history restarts whenever mu
+    // changes.
+    int anderson_memory = 0;
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for

@@ -339,6 +339,120 @@ __global__ void cg_extrapolate_kernel(int64_t n, int B, double* __restrict__ y, 
     }
 }
 
+// ---- Anderson acceleration (kernels.cuh) ----
+
+__global__ void aa_save_kernel(int64_t nx, int B, const double* __restrict__ x, const double* __restrict__ z,
+                               double* __restrict__ w, const int* __restrict__ mode) {
+    const int64_t half = nx * B, total = 2 * half;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (!mode[(int)(t % B)]) continue;
+        w[t] = (t < half) ? x[t] : z[t - half];
+    }
+}
+
+// Rows e of the state are walked with the chunk mapping of the reducing
+// kernels, so each thread keeps one instance and its 2 m dot products come
+// out in a fixed order.
+template <int MAXM>
+__global__ void __launch_bounds__(kThreads) aa_update_kernel(
+    int64_t nx, int B, int m, const double* __restrict__ x, const double* __restrict__ z,
+    const double* __restrict__ w, double* __restrict__ fprev, double* __restrict__ gprev, double* __restrict__ dF,
+    double* __restrict__ dG, const int* __restrict__ mode, const int* __restrict__ slot,
+    double* __restrict__ partial) {
+    const int64_t nrows = 2 * nx, half = nx * B;
+    const size_t col = (size_t)nrows * B;
+    const Chunk ch = chunk_of(nrows, B);
+    double acc[2 * MAXM];
+#pragma unroll
+    for (int k = 0; k < 2 * MAXM; k++) acc[k] = 0.0;
+    if (ch.live) {
+        const int b = ch.b;
+        const int md = mode[b];
+        const int s = slot[b];
+        if (md) {
+            for (int64_t e = ch.first; e < ch.nrows; e += ch.stride) {
+                const int64_t t = e * B + b;
+                const double g = (e < nx) ? x[t] : z[t - half];
+                const double f = g - w[t];
+                if (md == 2) {
+                    const double df = f - fprev[t];
+                    dF[(size_t)s * col + t] = df;
+                    dG[(size_t)s * col + t] = g - gprev[t];
+#pragma unroll
+                    for (int j = 0; j < MAXM; j++) {
+                        if (j < m) {
+                            const double dj = (j == s) ? df : dF[(size_t)j * col + t];
+                            acc[2 * j] += df * dj;
+                            acc[2 * j + 1] += dj * f;
+                        }
+                    }
+                }
+                fprev[t] = f;
+                gprev[t] = g;
+            }
+        }
+    }
+    // partial[(k * gridDim.x + block) * B + b] for k < 2 m
+    __shared__ double sh[kThreads];
+    const int rows_per_pass = blockDim.x / B;
+#pragma unroll
+    for (int k = 0; k < 2 * MAXM; k++) {
+        if (k < 2 * m) {
+            sh[threadIdx.x] = acc[k];
+            __syncthreads();
+            if ((int)threadIdx.x < B) {
+                double sum = 0.0;
+                for (int r = 0; r < rows_per_pass; r++) sum += sh[threadIdx.x + r * B];
+                partial[((int64_t)k * gridDim.x + blockIdx.x) * B + threadIdx.x] = sum;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// out[k * B + b] = sum over blocks of partial[(k * nblk + block) * B + b], one
+// CTA per (k, b), fixed tree order
+__global__ void reduce_stage2_multi(int nblk, int B, const double* __restrict__ partial, double* __restrict__ out) {
+    __shared__ double sh[kThreads];
+    const int k = blockIdx.x / B, b = blockIdx.x % B;
+    const double* p = partial + (int64_t)k * nblk * B;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += p[(int64_t)i * B + b];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+template <int MAXM>
+__global__ void aa_mix_kernel(int64_t nx, int B, int m, double* __restrict__ x, double* __restrict__ z,
+                              const double* __restrict__ dG, const double* __restrict__ gamma,
+                              const int* __restrict__ mix) {
+    const int64_t half = nx * B, total = 2 * half;
+    const size_t col = (size_t)total;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t % B);
+        if (!mix[b]) continue;
+        double v = (t < half) ? x[t] : z[t - half];
+#pragma unroll
+        for (int j = 0; j < MAXM; j++) {
+            if (j < m) {
+                const double gj = gamma[b * m + j];
+                if (gj != 0.0) v -= gj * dG[(size_t)j * col + t];
+            }
+        }
+        if (t < half)
+            x[t] = v;
+        else
+            z[t - half] = v;
+    }
+}
+
 __global__ void cg_init_kernel(int64_t n, int B, const double* __restrict__ rhs, const double* __restrict__ Ap,
                                double* __restrict__ r, double* __restrict__ p, const CgScalars* __restrict__ cs) {
     const int64_t total = n * B;
@@ -514,6 +628,41 @@ void launch_reduce(ReduceMode mode, int64_t n, int B, const double* u, const dou
 
 void launch_set_rows(int64_t n, int B, const double* row, double* out, const int* mask, cudaStream_t s) {
     set_rows_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, row, out, mask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_aa_save(int64_t nx, int B, const double* x, const double* z, double* w, const int* mode, cudaStream_t s) {
+    aa_save_kernel<<<grid_for(2 * nx * B), kThreads, 0, s>>>(nx, B, x, z, w, mode);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+int64_t aa_partial_size(int64_t nx, int B, int m) { return (int64_t)2 * m * spmv_grid(2 * nx, B) * B; }
+
+void launch_aa_update(int64_t nx, int B, int m, const double* x, const double* z, const double* w, double* fprev,
+                      double* gprev, double* dF, double* dG, const int* mode, const int* slot, double* partial,
+                      double* dots, cudaStream_t s) {
+    const int g = spmv_grid(2 * nx, B);
+    if (m <= 4)
+        aa_update_kernel<4><<<g, kThreads, 0, s>>>(nx, B, m, x, z, w, fprev, gprev, dF, dG, mode, slot, partial);
+    else if (m <= 8)
+        aa_update_kernel<8><<<g, kThreads, 0, s>>>(nx, B, m, x, z, w, fprev, gprev, dF, dG, mode, slot, partial);
+    else
+        aa_update_kernel<kAndersonMax><<<g, kThreads, 0, s>>>(nx, B, m, x, z, w, fprev, gprev, dF, dG, mode, slot,
+                                                               partial);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    reduce_stage2_multi<<<2 * m * B, kThreads, 0, s>>>(g, B, partial, dots);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_aa_mix(int64_t nx, int B, int m, double* x, double* z, const double* dG, const double* gamma,
+                   const int* mix, cudaStream_t s) {
+    const int g = grid_for(2 * nx * B);
+    if (m <= 4)
+        aa_mix_kernel<4><<<g, kThreads, 0, s>>>(nx, B, m, x, z, dG, gamma, mix);
+    else if (m <= 8)
+        aa_mix_kernel<8><<<g, kThreads, 0, s>>>(nx, B, m, x, z, dG, gamma, mix);
+    else
+        aa_mix_kernel<kAndersonMax><<<g, kThreads, 0, s>>>(nx, B, m, x, z, dG, gamma, mix);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -219,6 +219,62 @@ struct Problem {
 
 namespace {
 
+// Host half of the Anderson acceleration: per instance, the Gram matrix of
+// its difference columns dF (indexed by ring slot) and the small solve.
+struct AndersonGram {
+    int B = 0, M = 0;
+    std::vector<double> g;  // [b][M][M]
+    AndersonGram(int nb, int m) : B(nb), M(m), g((size_t)nb * m * m, 0.0) {}
+    double& at(int b, int i, int j) { return g[((size_t)b * M + i) * M + j]; }
+    // Enters the new column at `slot` (dots[(2 j) * B + b] = dF_slot . dF_j,
+    // dots[(2 j + 1) * B + b] = dF_j . f) and solves (G + lambda I) gamma = dF^T f
+    // over the `count` valid slots of a ring of `mb`; gamma is indexed by slot.
+    // Returns false when the solution is not finite.
+    bool solve(int b, int mb, int slot, int count, const std::vector<double>& dots, double* gamma) {
+        std::vector<int> sl(count);
+        for (int i = 0; i < count; i++) sl[i] = (slot - i + mb) % mb;
+        for (int i = 0; i < count; i++) {
+            const double v = dots[(size_t)(2 * sl[i]) * B + b];
+            at(b, slot, sl[i]) = v;
+            at(b, sl[i], slot) = v;
+        }
+        const int c = count;
+        std::vector<double> a((size_t)c * c), r(c);
+        double tr = 0.0;
+        for (int i = 0; i < c; i++) tr += at(b, sl[i], sl[i]);
+        const double lambda = 1e-10 * tr + 1e-300;
+        for (int i = 0; i < c; i++) {
+            for (int k = 0; k < c; k++) a[(size_t)i * c + k] = at(b, sl[i], sl[k]) + (i == k ? lambda : 0.0);
+            r[i] = dots[(size_t)(2 * sl[i] + 1) * B + b];
+        }
+        // Gaussian elimination with partial pivoting (c <= 16)
+        for (int k = 0; k < c; k++) {
+            int piv = k;
+            for (int i = k + 1; i < c; i++)
+                if (std::fabs(a[(size_t)i * c + k]) > std::fabs(a[(size_t)piv * c + k])) piv = i;
+            if (!(std::fabs(a[(size_t)piv * c + k]) > 0.0)) return false;
+            if (piv != k) {
+                for (int j = 0; j < c; j++) std::swap(a[(size_t)k * c + j], a[(size_t)piv * c + j]);
+                std::swap(r[k], r[piv]);
+            }
+            for (int i = k + 1; i < c; i++) {
+                const double f = a[(size_t)i * c + k] / a[(size_t)k * c + k];
+                for (int j = k; j < c; j++) a[(size_t)i * c + j] -= f * a[(size_t)k * c + j];
+                r[i] -= f * r[k];
+            }
+        }
+        std::vector<double> x(c);
+        for (int k = c - 1; k >= 0; k--) {
+            double s = r[k];
+            for (int j = k + 1; j < c; j++) s -= a[(size_t)k * c + j] * x[j];
+            x[k] = s / a[(size_t)k * c + k];
+            if (!std::isfinite(x[k])) return false;
+        }
+        for (int i = 0; i < c; i++) gamma[sl[i]] = x[i];
+        return true;
+    }
+};
+
 // Lock-step solve of B instances that share one layout.
 class GroupRun {
   public:
@@ -251,6 +307,20 @@ class GroupRun {
         if (extrapolate_) {
             yprev_.alloc(C);
             ex_.alloc(B_);
+        }
+        for (auto* p : P_) aa_m_ = std::max(aa_m_, p->opt.anderson_memory);
+        if (aa_m_ > 0) {
+            aw_.alloc(2 * X);
+            af_.alloc(2 * X);
+            ag_.alloc(2 * X);
+            adF_.alloc(2 * X * aa_m_);
+            adG_.alloc(2 * X * aa_m_);
+            agam_.alloc((size_t)B_ * aa_m_);
+            apart_.alloc(aa_partial_size(nx_, B_, aa_m_));
+            adots_.alloc((size_t)2 * aa_m_ * B_);
+            amode_.alloc(B_);
+            aslot_.alloc(B_);
+            amix_.alloc(B_);
         }
         CK(cudaMallocHost(&hscal_, sizeof(double) * 4 * B_));
         CK(cudaMallocHost(&hnact_, sizeof(int) * 8));
@@ -459,6 +529,10 @@ class GroupRun {
         std::vector<int> restarts_left(B_, 2), recover(B_, 0);
         // CG solutions seen per instance since its (re)start, for cg_extrapolate
         std::vector<int> ycount(B_, 0), exmode(B_, 0);
+        // Anderson acceleration, per instance: f and g stored, valid columns,
+        // newest ring slot, this iteration's kernel mode, mu changed
+        std::vector<int> aa_have(B_, 0), aa_count(B_, 0), aa_slot(B_, 0), aa_mode(B_, 0), mu_changed(B_, 0);
+        AndersonGram gram(B_, aa_m_);
         int it = 0;
         while (true) {
             if (std::find(recover.begin(), recover.end(), 1) != recover.end()) {
@@ -469,6 +543,7 @@ class GroupRun {
                         iiter[b] += cs[b].iter;
                         recover[b] = 0;
                         ycount[b] = 0;
+                        aa_have[b] = aa_count[b] = 0;
                     }
                 warm_ = false;  // every large block of the group starts its projection cold again
             }
@@ -479,6 +554,13 @@ class GroupRun {
             for (int b = 0; b < B_; b++) coef[b] = -opt(b).tau * mu[b];
             CK(cudaMemcpyAsync(coef_.p, coef.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
             CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+            if (aa_m_ > 0) {
+                // w = the (x, z) this step starts from
+                for (int b = 0; b < B_; b++) aa_mode[b] = (active[b] && opt(b).anderson_memory > 0) ? 1 : 0;
+                CK(cudaMemcpyAsync(amode_.p, aa_mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+                launch_aa_save(nx_, B_, x_.p, z_.p, aw_.p, amode_.p, s_);
+            }
+            std::fill(mu_changed.begin(), mu_changed.end(), 0);
             CK(cudaEventRecord(e0, s_));
             // Ax = -tau mu (A x - b); z <- c - z; B = A z + Ax   (:1783-1794)
             launch_spmv(T_.A(), B_, x_.p, ax_.p, T_.b.p, coef_.p, nullptr, mask_.p, s_);
@@ -540,7 +622,10 @@ class GroupRun {
                 const double e_p = hscal_[2 * B_ + b], e_d = hscal_[3 * B_ + b];
                 const long ii = cs[b].iter;
                 iiter[b] += ii;
-                if (oiter[b] % o.mu_update_frequency == 0 && oiter[b] > 0) mu[b] = mu[b] * ep[b] / ed[b];
+                if (oiter[b] % o.mu_update_frequency == 0 && oiter[b] > 0) {
+                    mu[b] = mu[b] * ep[b] / ed[b];
+                    mu_changed[b] = 1;
+                }
                 const double shift = P.enuc + P.efzc;
                 if (P.record_trace)
                     P.trace.push_back({(double)oiter[b], (double)ii, e_p + shift, e_d + shift, std::fabs(e_p - e_d),
@@ -581,6 +666,7 @@ class GroupRun {
                     active[b] = 0;
                 }
             }
+            if (aa_m_ > 0) anderson(active, recover, mu_changed, aa_have, aa_count, aa_slot, aa_mode, gram);
             it++;
         }
         CK(cudaEventRecord(e2, s_));
@@ -597,6 +683,58 @@ class GroupRun {
         cudaEventDestroy(e1);
         cudaEventDestroy(e2);
         cudaEventDestroy(e3);
+    }
+
+    // Anderson acceleration after a step: f = g - w enters the history of every
+    // instance still iterating with anderson_memory > 0 (after a mu change the
+    // history restarts from this f), and an instance with at least one
+    // difference column continues from g - sum_j gamma_j dG_j, where gamma
+    // minimises |f - sum_j gamma_j dF_j| (a Tikhonov term of 1e-10 tr(dF^T dF)
+    // keeps the small system regular).
+    void anderson(const std::vector<int>& active, const std::vector<int>& recover, const std::vector<int>& mu_changed,
+                  std::vector<int>& have, std::vector<int>& count, std::vector<int>& slot, std::vector<int>& mode,
+                  AndersonGram& gram) {
+        bool any = false;
+        for (int b = 0; b < B_; b++) {
+            const int mb = P_[b]->opt.anderson_memory;
+            mode[b] = 0;
+            if (!active[b] || mb == 0 || recover[b]) continue;
+            if (mu_changed[b]) have[b] = count[b] = 0;
+            if (have[b]) {
+                slot[b] = count[b] == 0 ? 0 : (slot[b] + 1) % mb;
+                count[b] = std::min(count[b] + 1, mb);
+                mode[b] = 2;
+            } else {
+                mode[b] = 1;
+                have[b] = 1;
+            }
+            any = true;
+        }
+        if (!any) return;
+        CK(cudaMemcpyAsync(amode_.p, mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(aslot_.p, slot.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        launch_aa_update(nx_, B_, aa_m_, x_.p, z_.p, aw_.p, af_.p, ag_.p, adF_.p, adG_.p, amode_.p, aslot_.p,
+                         apart_.p, adots_.p, s_);
+        std::vector<double> dots((size_t)2 * aa_m_ * B_);
+        CK(cudaMemcpyAsync(dots.data(), adots_.p, dots.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
+        std::vector<double> gamma((size_t)B_ * aa_m_, 0.0);
+        std::vector<int> mix(B_, 0);
+        bool anymix = false;
+        for (int b = 0; b < B_; b++) {
+            if (mode[b] != 2) continue;
+            if (gram.solve(b, P_[b]->opt.anderson_memory, slot[b], count[b], dots, &gamma[(size_t)b * aa_m_])) {
+                mix[b] = 1;
+                anymix = true;
+            } else {
+                have[b] = count[b] = 0;  // a singular or non-finite system restarts the history
+            }
+        }
+        if (!anymix) return;
+        CK(cudaMemcpyAsync(agam_.p, gamma.data(), gamma.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(amix_.p, mix.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        launch_aa_mix(nx_, B_, aa_m_, x_.p, z_.p, adG_.p, agam_.p, amix_.p, s_);
+        CK(cudaStreamSynchronize(s_));
     }
 
     // Which of y, x, z (and the CG scalars) turned non-finite, on stderr, so
@@ -859,6 +997,13 @@ class GroupRun {
     DevBuf<double> yprev_;
     DevBuf<int> ex_;
     bool extrapolate_ = false;
+    // Anderson acceleration (anderson_memory): the saved state w, the previous
+    // f and g, the difference columns, and the per-instance modes, slots,
+    // mixing flags and coefficients; aa_m_ = columns allocated (the largest
+    // memory of the group)
+    int aa_m_ = 0;
+    DevBuf<double> aw_, af_, ag_, adF_, adG_, agam_, apart_, adots_;
+    DevBuf<int> amode_, aslot_, amix_;
     double* hscal_ = nullptr;
     int* hnact_ = nullptr;
     // projection plan
@@ -945,6 +1090,7 @@ void v2g_default_options(v2g_options* o) {
     o->constrain_d4 = 0;
     o->start = 0;
     o->cg_extrapolate = 0;
+    o->anderson_memory = 0;
 }
 
 const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
@@ -977,6 +1123,9 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         if (opt->cg_extrapolate != 0 && opt->cg_extrapolate != 1)
             return v2g::fail(V2G_ERR_ARG, "cg_extrapolate must be 0 or 1");
         o.cg_extrapolate = opt->cg_extrapolate == 1;
+        if (opt->anderson_memory < 0 || opt->anderson_memory > v2g::kAndersonMax)
+            return v2g::fail(V2G_ERR_ARG, "anderson_memory must be in 0..16");
+        o.anderson_memory = opt->anderson_memory;
         if (!(o.cg_tol_factor > 0.0 && o.cg_tol_factor < 1.0))
             return v2g::fail(V2G_ERR_ARG, "cg_tolerance_factor must be in (0, 1)");
         if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)

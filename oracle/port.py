@@ -358,7 +358,9 @@ def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_m
     with difference columns dF_j = f_{j+1} - f_j and dG_j = g_{j+1} - g_j of
     the last m steps, the next state is g - dG gamma, where
     (dF^T dF + 1e-10 tr(dF^T dF) I) gamma = dF^T f.  The stopping test and the
-    energies are those of g; the history restarts whenever mu changes.
+    energies are those of g; the history restarts from the current f whenever
+    mu changes and when |f| more than doubled since the previous step (that
+    step is then not mixed).
     """
     mu = 1.0
     ep = ed = 0.0
@@ -366,6 +368,7 @@ def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_m
     iiter = 0
     starts = []  # the y each CG started from, before extrapolation
     hist_w, hist_f = [], []  # Anderson history: states and residuals
+    fnorm_prev = None
     while True:
         x_in, z_in = x, z
         Ax = -tau * mu * (A @ x - b)
@@ -397,9 +400,11 @@ def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_m
             return dict(converged=True, e_primal=ep_energy, e_dual=ed_energy, oiter=oiter, iiter=iiter, ep=ep, ed=ed,
                         x=x, y=y, z=z)
         if anderson_memory:
-            if mu_changed:
-                hist_w, hist_f = [], []
             g = np.concatenate([x, z])
+            fnorm = np.linalg.norm(g - w)
+            if mu_changed or (fnorm_prev is not None and fnorm > 2.0 * fnorm_prev):
+                hist_w, hist_f = [], []
+            fnorm_prev = fnorm
             hist_w.append(w)
             hist_f.append(g - w)
             if len(hist_w) > anderson_memory + 1:

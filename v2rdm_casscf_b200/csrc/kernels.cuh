@@ -104,8 +104,8 @@ constexpr int kAndersonMax = 16;
 void launch_aa_save(int64_t nx, int B, const double* x, const double* z, double* w, const int* mode, cudaStream_t s);
 // f = g - w; mode[b] == 2: dF[slot[b]] = f - fprev, dG[slot[b]] = g - gprev and
 // dots[(2 j) * B + b] = dF[slot].dF[j], dots[(2 j + 1) * B + b] = dF[j].f for j < m;
-// mode[b] >= 1: fprev = f, gprev = g.  partial holds aa_partial_size(nx, B, m)
-// doubles; the sums are deterministic.
+// mode[b] >= 1: dots[(2 m) * B + b] = f.f, fprev = f, gprev = g.  partial holds
+// aa_partial_size(nx, B, m) doubles; the sums are deterministic.
 void launch_aa_update(int64_t nx, int B, int m, const double* x, const double* z, const double* w, double* fprev,
                       double* gprev, double* dF, double* dG, const int* mode, const int* slot, double* partial,
                       double* dots, cudaStream_t s);

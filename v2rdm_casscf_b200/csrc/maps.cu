@@ -363,9 +363,12 @@ __global__ void __launch_bounds__(kThreads) aa_update_kernel(
     const int64_t nrows = 2 * nx, half = nx * B;
     const size_t col = (size_t)nrows * B;
     const Chunk ch = chunk_of(nrows, B);
-    double acc[2 * MAXM];
+    // acc[2 j] = dF_slot.dF_j, acc[2 j + 1] = dF_j.f; f.f in ff (one spare
+    // entry keeps every unrolled index of the output loop in bounds)
+    double acc[2 * MAXM + 1];
 #pragma unroll
-    for (int k = 0; k < 2 * MAXM; k++) acc[k] = 0.0;
+    for (int k = 0; k < 2 * MAXM + 1; k++) acc[k] = 0.0;
+    double ff = 0.0;
     if (ch.live) {
         const int b = ch.b;
         const int md = mode[b];
@@ -388,18 +391,19 @@ __global__ void __launch_bounds__(kThreads) aa_update_kernel(
                         }
                     }
                 }
+                ff += f * f;
                 fprev[t] = f;
                 gprev[t] = g;
             }
         }
     }
-    // partial[(k * gridDim.x + block) * B + b] for k < 2 m
+    // partial[(k * gridDim.x + block) * B + b] for k <= 2 m
     __shared__ double sh[kThreads];
     const int rows_per_pass = blockDim.x / B;
 #pragma unroll
-    for (int k = 0; k < 2 * MAXM; k++) {
-        if (k < 2 * m) {
-            sh[threadIdx.x] = acc[k];
+    for (int k = 0; k < 2 * MAXM + 1; k++) {
+        if (k <= 2 * m) {
+            sh[threadIdx.x] = (k == 2 * m) ? ff : acc[k];
             __syncthreads();
             if ((int)threadIdx.x < B) {
                 double sum = 0.0;
@@ -636,7 +640,7 @@ void launch_aa_save(int64_t nx, int B, const double* x, const double* z, double*
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-int64_t aa_partial_size(int64_t nx, int B, int m) { return (int64_t)2 * m * spmv_grid(2 * nx, B) * B; }
+int64_t aa_partial_size(int64_t nx, int B, int m) { return (int64_t)(2 * m + 1) * spmv_grid(2 * nx, B) * B; }
 
 void launch_aa_update(int64_t nx, int B, int m, const double* x, const double* z, const double* w, double* fprev,
                       double* gprev, double* dF, double* dG, const int* mode, const int* slot, double* partial,
@@ -650,7 +654,7 @@ void launch_aa_update(int64_t nx, int B, int m, const double* x, const double* z
         aa_update_kernel<kAndersonMax><<<g, kThreads, 0, s>>>(nx, B, m, x, z, w, fprev, gprev, dF, dG, mode, slot,
                                                                partial);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    reduce_stage2_multi<<<2 * m * B, kThreads, 0, s>>>(g, B, partial, dots);
+    reduce_stage2_multi<<<(2 * m + 1) * B, kThreads, 0, s>>>(g, B, partial, dots);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -219,6 +219,10 @@ struct Problem {
 
 namespace {
 
+// The Anderson history restarts when the fixed-point residual |f| grows by
+// more than this factor from one outer iteration to the next.
+constexpr double kAndersonGuard = 2.0;
+
 // Host half of the Anderson acceleration: per instance, the Gram matrix of
 // its difference columns dF (indexed by ring slot) and the small solve.
 struct AndersonGram {
@@ -317,7 +321,7 @@ class GroupRun {
             adG_.alloc(2 * X * aa_m_);
             agam_.alloc((size_t)B_ * aa_m_);
             apart_.alloc(aa_partial_size(nx_, B_, aa_m_));
-            adots_.alloc((size_t)2 * aa_m_ * B_);
+            adots_.alloc((size_t)(2 * aa_m_ + 1) * B_);
             amode_.alloc(B_);
             aslot_.alloc(B_);
             amix_.alloc(B_);
@@ -532,6 +536,7 @@ class GroupRun {
         // Anderson acceleration, per instance: f and g stored, valid columns,
         // newest ring slot, this iteration's kernel mode, mu changed
         std::vector<int> aa_have(B_, 0), aa_count(B_, 0), aa_slot(B_, 0), aa_mode(B_, 0), mu_changed(B_, 0);
+        std::vector<double> aa_fnorm(B_, -1.0);  // |f| of the instance's previous Anderson step
         AndersonGram gram(B_, aa_m_);
         int it = 0;
         while (true) {
@@ -544,6 +549,7 @@ class GroupRun {
                         recover[b] = 0;
                         ycount[b] = 0;
                         aa_have[b] = aa_count[b] = 0;
+                        aa_fnorm[b] = -1.0;
                     }
                 warm_ = false;  // every large block of the group starts its projection cold again
             }
@@ -666,7 +672,7 @@ class GroupRun {
                     active[b] = 0;
                 }
             }
-            if (aa_m_ > 0) anderson(active, recover, mu_changed, aa_have, aa_count, aa_slot, aa_mode, gram);
+            if (aa_m_ > 0) anderson(active, recover, mu_changed, aa_have, aa_count, aa_slot, aa_mode, aa_fnorm, gram);
             it++;
         }
         CK(cudaEventRecord(e2, s_));
@@ -686,14 +692,15 @@ class GroupRun {
     }
 
     // Anderson acceleration after a step: f = g - w enters the history of every
-    // instance still iterating with anderson_memory > 0 (after a mu change the
-    // history restarts from this f), and an instance with at least one
-    // difference column continues from g - sum_j gamma_j dG_j, where gamma
-    // minimises |f - sum_j gamma_j dF_j| (a Tikhonov term of 1e-10 tr(dF^T dF)
-    // keeps the small system regular).
+    // instance still iterating with anderson_memory > 0, and an instance with
+    // at least one difference column continues from g - sum_j gamma_j dG_j,
+    // where gamma minimises |f - sum_j gamma_j dF_j| (a Tikhonov term of
+    // 1e-10 tr(dF^T dF) keeps the small system regular).  The history restarts
+    // from this f after a mu change and when |f| more than doubled since the
+    // previous step (the step went the wrong way; that step is not mixed).
     void anderson(const std::vector<int>& active, const std::vector<int>& recover, const std::vector<int>& mu_changed,
                   std::vector<int>& have, std::vector<int>& count, std::vector<int>& slot, std::vector<int>& mode,
-                  AndersonGram& gram) {
+                  std::vector<double>& fnorm, AndersonGram& gram) {
         bool any = false;
         for (int b = 0; b < B_; b++) {
             const int mb = P_[b]->opt.anderson_memory;
@@ -715,14 +722,23 @@ class GroupRun {
         CK(cudaMemcpyAsync(aslot_.p, slot.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
         launch_aa_update(nx_, B_, aa_m_, x_.p, z_.p, aw_.p, af_.p, ag_.p, adF_.p, adG_.p, amode_.p, aslot_.p,
                          apart_.p, adots_.p, s_);
-        std::vector<double> dots((size_t)2 * aa_m_ * B_);
+        std::vector<double> dots((size_t)(2 * aa_m_ + 1) * B_);
         CK(cudaMemcpyAsync(dots.data(), adots_.p, dots.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
         CK(cudaStreamSynchronize(s_));
         std::vector<double> gamma((size_t)B_ * aa_m_, 0.0);
         std::vector<int> mix(B_, 0);
         bool anymix = false;
         for (int b = 0; b < B_; b++) {
+            if (mode[b] == 0) continue;
+            const double fn = std::sqrt(dots[(size_t)(2 * aa_m_) * B_ + b]);
+            const bool grew = fnorm[b] >= 0.0 && fn > kAndersonGuard * fnorm[b];
+            fnorm[b] = fn;
             if (mode[b] != 2) continue;
+            if (grew) {
+                // this f starts a new history: f and g are stored, the column is dropped
+                count[b] = 0;
+                continue;
+            }
             if (gram.solve(b, P_[b]->opt.anderson_memory, slot[b], count[b], dots, &gamma[(size_t)b * aa_m_])) {
                 mix[b] = 1;
                 anymix = true;

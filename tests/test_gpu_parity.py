@@ -176,67 +176,6 @@ def test_cg_tolerance_factor_reaches_the_same_energy(v2g):
     assert s.result["iiter"] < int(g["iiter"])
 
 
-def test_cg_extrapolation_reaches_the_same_energy(v2g):
-    # cg_extrapolate: CG starts from y_k + (y_k - y_{k-1}) with the reference's
-    # stopping test, so the energy is the reference's and CG needs fewer
-    # iterations.  Solved in one group with two instances that do not
-    # extrapolate: the mode is per instance.
-    from v2rdm_casscf_b200.hamiltonian import synthetic
-
-    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
-    opts = dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]))
-    solvers = []
-    for seed, ex in ((int(g["seed"]), True), (int(g["seed"]), False), (1, False)):
-        s = v2g.V2RDMSolver.from_active_space(synthetic(4, seed), options=opts, cg_extrapolate=ex)
-        s.guess()
-        solvers.append(s)
-    res = v2g.solve_batch(solvers)
-    assert all(r["status"] == 0 for r in res)
-    assert abs(res[0]["e_total"] - float(g["e_primal"])) <= 1e-6
-    assert abs(res[1]["e_total"] - float(g["e_primal"])) <= 1e-6
-    assert res[0]["iiter"] < res[1]["iiter"]
-    g1 = load(os.path.join(GOLDEN, "solve_synthetic_n4_s1.npz"))
-    assert abs(res[2]["e_total"] - float(g1["e_primal"])) <= 1e-6
-
-
-def test_anderson_acceleration_reaches_the_same_energy(v2g):
-    # anderson_memory: the stopping test and energies are the plain step's, so
-    # the reference's energy is reached, in far fewer outer iterations.  One
-    # group holds instances with memories 10, 5 and 0 (per-instance history
-    # rings inside one allocation of 10 columns).
-    from v2rdm_casscf_b200.hamiltonian import synthetic
-
-    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
-    opts = dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]))
-    solvers = []
-    for m in (10, 5, 0):
-        s = v2g.V2RDMSolver.from_active_space(synthetic(4, int(g["seed"])), options=opts, anderson_memory=m,
-                                              cg_extrapolate=m > 0)
-        s.guess()
-        solvers.append(s)
-    res = v2g.solve_batch(solvers)
-    assert all(r["status"] == 0 for r in res)
-    for r in res:
-        assert abs(r["e_total"] - float(g["e_primal"])) <= 1e-6
-    assert res[0]["oiter"] <= 0.6 * res[2]["oiter"]
-    assert res[1]["oiter"] <= 0.8 * res[2]["oiter"]
-
-
-def test_tau_parameter_reaches_the_same_energy(v2g):
-    # TAU_PARAMETER at the top of the plugin's documented range [1.0, 1.6]
-    # (plugin.cc:94-97) changes the path, not the answer
-    from v2rdm_casscf_b200.hamiltonian import synthetic
-
-    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
-    s = v2g.V2RDMSolver.from_active_space(
-        synthetic(4, int(g["seed"])),
-        options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]), TAU_PARAMETER=1.6),
-        start="feasible")
-    e = s.compute_energy()
-    assert s.result["status"] == 0
-    assert abs(e - float(g["e_primal"])) <= 1e-6
-
-
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "pack_*.npz"))),
                          ids=lambda p: os.path.basename(p))
 def test_spatial_density_matches_reference(v2g, path):
@@ -320,6 +259,71 @@ def test_feasible_start_reaches_reference_energy(v2g, name):
     s = v2g.V2RDMSolver.from_active_space(
         a, options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"])), start="feasible",
         projection="adaptive")
+    e = s.compute_energy()
+    assert s.result["status"] == 0
+    assert abs(e - float(g["e_primal"])) <= 1e-6
+
+
+# Options beyond the reference's loop (they change the path, not the answer); last, so that
+# every parity test above runs before them.
+
+
+def test_cg_extrapolation_reaches_the_same_energy(v2g):
+    # cg_extrapolate: CG starts from y_k + (y_k - y_{k-1}) with the reference's
+    # stopping test, so the energy is the reference's and CG needs fewer
+    # iterations.  Solved in one group with two instances that do not
+    # extrapolate: the mode is per instance.
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    opts = dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]))
+    solvers = []
+    for seed, ex in ((int(g["seed"]), True), (int(g["seed"]), False), (1, False)):
+        s = v2g.V2RDMSolver.from_active_space(synthetic(4, seed), options=opts, cg_extrapolate=ex)
+        s.guess()
+        solvers.append(s)
+    res = v2g.solve_batch(solvers)
+    assert all(r["status"] == 0 for r in res)
+    assert abs(res[0]["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert abs(res[1]["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert res[0]["iiter"] < res[1]["iiter"]
+    g1 = load(os.path.join(GOLDEN, "solve_synthetic_n4_s1.npz"))
+    assert abs(res[2]["e_total"] - float(g1["e_primal"])) <= 1e-6
+
+
+def test_anderson_acceleration_reaches_the_same_energy(v2g):
+    # anderson_memory: the stopping test and energies are the plain step's, so
+    # the reference's energy is reached, in far fewer outer iterations.  One
+    # group holds instances with memories 10, 5 and 0 (per-instance history
+    # rings inside one allocation of 10 columns).
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    opts = dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]))
+    solvers = []
+    for m in (10, 5, 0):
+        s = v2g.V2RDMSolver.from_active_space(synthetic(4, int(g["seed"])), options=opts, anderson_memory=m,
+                                              cg_extrapolate=m > 0)
+        s.guess()
+        solvers.append(s)
+    res = v2g.solve_batch(solvers)
+    assert all(r["status"] == 0 for r in res)
+    for r in res:
+        assert abs(r["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert res[0]["oiter"] <= 0.6 * res[2]["oiter"]
+    assert res[1]["oiter"] <= 0.8 * res[2]["oiter"]
+
+
+def test_tau_parameter_reaches_the_same_energy(v2g):
+    # TAU_PARAMETER at the top of the plugin's documented range [1.0, 1.6]
+    # (plugin.cc:94-97) changes the path, not the answer
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    s = v2g.V2RDMSolver.from_active_space(
+        synthetic(4, int(g["seed"])),
+        options=dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]), TAU_PARAMETER=1.6),
+        start="feasible")
     e = s.compute_energy()
     assert s.result["status"] == 0
     assert abs(e - float(g["e_primal"])) <= 1e-6

@@ -95,6 +95,26 @@ def test_port_anderson_same_energy_fewer_outer_iterations(m):
     assert out["oiter"] <= 0.6 * int(g["oiter"])
 
 
+def test_port_anderson_guard_on_a_stretched_chain():
+    # H4 at 1.5 A: without the residual-growth restart, Anderson mixing needs
+    # more outer iterations than no mixing; with it (the product's rule), far
+    # fewer, at the same energy
+    from v2rdm_casscf_b200.hchain import hydrogen_chain
+
+    a = hydrogen_chain(4, 1.5)
+    L = port.Layout(a.n, a.na, a.nb)
+    A = port.build_A(L).tocsr()
+    b = port.build_b(L, A.shape[0])
+    c = port.build_c(L, a.h, a.eri())
+    w, _ = port.cg(A, np.zeros(A.shape[0]), b, 1e-10 * np.linalg.norm(b), 20000)
+    x0 = A.T @ w
+    runs = [port.solve(L, A, b, c, x0.copy(), np.zeros(A.shape[0]), np.zeros(L.dimx), 1e-6, 1e-7, cg_extrapolate=True,
+                       anderson_memory=m) for m in (0, 10)]
+    assert all(r["converged"] for r in runs)
+    assert abs(runs[1]["e_primal"] - runs[0]["e_primal"]) <= 1e-6
+    assert runs[1]["oiter"] <= 0.5 * runs[0]["oiter"]
+
+
 def test_port_agrees_with_product_table(v2g):
     L = port.Layout(5, 3, 2, 2)
     A = port.build_A(L)

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/v2rdm_gpu.h"
+#include "anderson.h"
 #include "constraints.h"
 #include "kernels.cuh"
 #include "layout.h"
@@ -218,66 +219,6 @@ struct Problem {
 };
 
 namespace {
-
-// The Anderson history restarts when the fixed-point residual |f| grows by
-// more than this factor from one outer iteration to the next.
-constexpr double kAndersonGuard = 2.0;
-
-// Host half of the Anderson acceleration: per instance, the Gram matrix of
-// its difference columns dF (indexed by ring slot) and the small solve.
-struct AndersonGram {
-    int B = 0, M = 0;
-    std::vector<double> g;  // [b][M][M]
-    AndersonGram(int nb, int m) : B(nb), M(m), g((size_t)nb * m * m, 0.0) {}
-    double& at(int b, int i, int j) { return g[((size_t)b * M + i) * M + j]; }
-    // Enters the new column at `slot` (dots[(2 j) * B + b] = dF_slot . dF_j,
-    // dots[(2 j + 1) * B + b] = dF_j . f) and solves (G + lambda I) gamma = dF^T f
-    // over the `count` valid slots of a ring of `mb`; gamma is indexed by slot.
-    // Returns false when the solution is not finite.
-    bool solve(int b, int mb, int slot, int count, const std::vector<double>& dots, double* gamma) {
-        std::vector<int> sl(count);
-        for (int i = 0; i < count; i++) sl[i] = (slot - i + mb) % mb;
-        for (int i = 0; i < count; i++) {
-            const double v = dots[(size_t)(2 * sl[i]) * B + b];
-            at(b, slot, sl[i]) = v;
-            at(b, sl[i], slot) = v;
-        }
-        const int c = count;
-        std::vector<double> a((size_t)c * c), r(c);
-        double tr = 0.0;
-        for (int i = 0; i < c; i++) tr += at(b, sl[i], sl[i]);
-        const double lambda = 1e-10 * tr + 1e-300;
-        for (int i = 0; i < c; i++) {
-            for (int k = 0; k < c; k++) a[(size_t)i * c + k] = at(b, sl[i], sl[k]) + (i == k ? lambda : 0.0);
-            r[i] = dots[(size_t)(2 * sl[i] + 1) * B + b];
-        }
-        // Gaussian elimination with partial pivoting (c <= 16)
-        for (int k = 0; k < c; k++) {
-            int piv = k;
-            for (int i = k + 1; i < c; i++)
-                if (std::fabs(a[(size_t)i * c + k]) > std::fabs(a[(size_t)piv * c + k])) piv = i;
-            if (!(std::fabs(a[(size_t)piv * c + k]) > 0.0)) return false;
-            if (piv != k) {
-                for (int j = 0; j < c; j++) std::swap(a[(size_t)k * c + j], a[(size_t)piv * c + j]);
-                std::swap(r[k], r[piv]);
-            }
-            for (int i = k + 1; i < c; i++) {
-                const double f = a[(size_t)i * c + k] / a[(size_t)k * c + k];
-                for (int j = k; j < c; j++) a[(size_t)i * c + j] -= f * a[(size_t)k * c + j];
-                r[i] -= f * r[k];
-            }
-        }
-        std::vector<double> x(c);
-        for (int k = c - 1; k >= 0; k--) {
-            double s = r[k];
-            for (int j = k + 1; j < c; j++) s -= a[(size_t)k * c + j] * x[j];
-            x[k] = s / a[(size_t)k * c + k];
-            if (!std::isfinite(x[k])) return false;
-        }
-        for (int i = 0; i < c; i++) gamma[sl[i]] = x[i];
-        return true;
-    }
-};
 
 // Lock-step solve of B instances that share one layout.
 class GroupRun {
@@ -535,9 +476,8 @@ class GroupRun {
         std::vector<int> ycount(B_, 0), exmode(B_, 0);
         // Anderson acceleration, per instance: f and g stored, valid columns,
         // newest ring slot, this iteration's kernel mode, mu changed
-        std::vector<int> aa_have(B_, 0), aa_count(B_, 0), aa_slot(B_, 0), aa_mode(B_, 0), mu_changed(B_, 0);
-        std::vector<double> aa_fnorm(B_, -1.0);  // |f| of the instance's previous Anderson step
-        AndersonGram gram(B_, aa_m_);
+        std::vector<int> mu_changed(B_, 0);
+        AndersonState aa(B_, aa_m_);
         int it = 0;
         while (true) {
             if (std::find(recover.begin(), recover.end(), 1) != recover.end()) {
@@ -548,8 +488,7 @@ class GroupRun {
                         iiter[b] += cs[b].iter;
                         recover[b] = 0;
                         ycount[b] = 0;
-                        aa_have[b] = aa_count[b] = 0;
-                        aa_fnorm[b] = -1.0;
+                        aa.restart(b);
                     }
                 warm_ = false;  // every large block of the group starts its projection cold again
             }
@@ -562,8 +501,8 @@ class GroupRun {
             CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
             if (aa_m_ > 0) {
                 // w = the (x, z) this step starts from
-                for (int b = 0; b < B_; b++) aa_mode[b] = (active[b] && opt(b).anderson_memory > 0) ? 1 : 0;
-                CK(cudaMemcpyAsync(amode_.p, aa_mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+                for (int b = 0; b < B_; b++) aa.mode[b] = (active[b] && opt(b).anderson_memory > 0) ? 1 : 0;
+                CK(cudaMemcpyAsync(amode_.p, aa.mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
                 launch_aa_save(nx_, B_, x_.p, z_.p, aw_.p, amode_.p, s_);
             }
             std::fill(mu_changed.begin(), mu_changed.end(), 0);
@@ -672,7 +611,7 @@ class GroupRun {
                     active[b] = 0;
                 }
             }
-            if (aa_m_ > 0) anderson(active, recover, mu_changed, aa_have, aa_count, aa_slot, aa_mode, aa_fnorm, gram);
+            if (aa_m_ > 0) anderson(active, recover, mu_changed, aa);
             it++;
         }
         CK(cudaEventRecord(e2, s_));
@@ -699,27 +638,16 @@ class GroupRun {
     // from this f after a mu change and when |f| more than doubled since the
     // previous step (the step went the wrong way; that step is not mixed).
     void anderson(const std::vector<int>& active, const std::vector<int>& recover, const std::vector<int>& mu_changed,
-                  std::vector<int>& have, std::vector<int>& count, std::vector<int>& slot, std::vector<int>& mode,
-                  std::vector<double>& fnorm, AndersonGram& gram) {
+                  AndersonState& aa) {
         bool any = false;
         for (int b = 0; b < B_; b++) {
-            const int mb = P_[b]->opt.anderson_memory;
-            mode[b] = 0;
-            if (!active[b] || mb == 0 || recover[b]) continue;
-            if (mu_changed[b]) have[b] = count[b] = 0;
-            if (have[b]) {
-                slot[b] = count[b] == 0 ? 0 : (slot[b] + 1) % mb;
-                count[b] = std::min(count[b] + 1, mb);
-                mode[b] = 2;
-            } else {
-                mode[b] = 1;
-                have[b] = 1;
-            }
-            any = true;
+            aa.mode[b] = 0;
+            if (!active[b] || recover[b]) continue;
+            if (aa.begin(b, P_[b]->opt.anderson_memory, mu_changed[b] != 0)) any = true;
         }
         if (!any) return;
-        CK(cudaMemcpyAsync(amode_.p, mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
-        CK(cudaMemcpyAsync(aslot_.p, slot.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(amode_.p, aa.mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(aslot_.p, aa.slot.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
         launch_aa_update(nx_, B_, aa_m_, x_.p, z_.p, aw_.p, af_.p, ag_.p, adF_.p, adG_.p, amode_.p, aslot_.p,
                          apart_.p, adots_.p, s_);
         std::vector<double> dots((size_t)(2 * aa_m_ + 1) * B_);
@@ -729,21 +657,9 @@ class GroupRun {
         std::vector<int> mix(B_, 0);
         bool anymix = false;
         for (int b = 0; b < B_; b++) {
-            if (mode[b] == 0) continue;
-            const double fn = std::sqrt(dots[(size_t)(2 * aa_m_) * B_ + b]);
-            const bool grew = fnorm[b] >= 0.0 && fn > kAndersonGuard * fnorm[b];
-            fnorm[b] = fn;
-            if (mode[b] != 2) continue;
-            if (grew) {
-                // this f starts a new history: f and g are stored, the column is dropped
-                count[b] = 0;
-                continue;
-            }
-            if (gram.solve(b, P_[b]->opt.anderson_memory, slot[b], count[b], dots, &gamma[(size_t)b * aa_m_])) {
+            if (aa.finish(b, P_[b]->opt.anderson_memory, dots, &gamma[(size_t)b * aa_m_])) {
                 mix[b] = 1;
                 anymix = true;
-            } else {
-                have[b] = count[b] = 0;  // a singular or non-finite system restarts the history
             }
         }
         if (!anymix) return;

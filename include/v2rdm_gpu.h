@@ -105,6 +105,9 @@ typedef struct v2g_result {
     double t_cg;         /* device seconds in the CG phase (iiter_time_) */
     double t_xz;         /* device seconds in Update_xz (oiter_time_) */
     double t_total;      /* device seconds for the whole solve */
+    long cg_stalls;      /* CG solves stopped because the residual grew 100x above its
+                            minimum (a right-hand side with a component in the null space of
+                            A^T above the CG tolerance; the plugin's CG would diverge there) */
 } v2g_result;
 
 void v2g_default_options(v2g_options* opt);

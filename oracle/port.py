@@ -324,20 +324,34 @@ def update_xz(A, L, x, y, c, mu):
     return xn, zn
 
 
-def cg(A, y, rhs, tol, maxiter):
-    """CGSolver::solve, cg_solver.cc:125-177."""
+def cg(A, y, rhs, tol, maxiter, growth_stop=None):
+    """CGSolver::solve, cg_solver.cc:125-177.
+
+    growth_stop: the product's safeguard (None = the reference's CG): stop,
+    keeping y, when p.Ap <= 0 or when r.r exceeds growth_stop times its
+    smallest value in this solve (A A^T is singular, and a right-hand side
+    with a null-space component above tol makes the plain iteration diverge).
+    """
     r = rhs - A @ (A.T @ y)
     p = r.copy()
     it = 0
+    rrmin = r @ r
     while True:
         Ap = A @ (A.T @ p)
         rr = r @ r
-        alpha = rr / (p @ Ap)
+        pap = p @ Ap
+        if growth_stop is not None and not pap > 0.0:
+            break
+        alpha = rr / pap
         y = y + alpha * p
         r = r - alpha * Ap
         rrnew = r @ r
         if math.sqrt(rrnew) < tol:
             break
+        if growth_stop is not None:
+            if rrnew > growth_stop * rrmin:
+                break
+            rrmin = min(rrmin, rrnew)
         p = (rrnew / rr) * p + r
         it += 1
         if it >= maxiter:
@@ -346,7 +360,7 @@ def cg(A, y, rhs, tol, maxiter):
 
 
 def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_maxiter=10000, tau=1.0,
-          mu_update_frequency=500, cg_extrapolate=False, anderson_memory=0):
+          mu_update_frequency=500, cg_extrapolate=False, anderson_memory=0, cg_growth_stop=None):
     """The outer loop of v2rdm_solver.cc:1778-1908 (no orbital optimisation).
 
     cg_extrapolate: the product's option of that name; from the third outer
@@ -381,7 +395,7 @@ def solve(L, A, b, c, x, y, z, r_conv, e_conv, maxiter=10000, cg_conv=1e-9, cg_m
             starts.append(y)
         else:
             y0 = y
-        y, k = cg(A, y0, B, tol, cg_maxiter)
+        y, k = cg(A, y0, B, tol, cg_maxiter, growth_stop=cg_growth_stop)
         iiter += k
         w = np.concatenate([x_in, z_in]) if anderson_memory else None
         x, z = update_xz(A, L, x, y, c, mu)

@@ -327,3 +327,12 @@ def test_tau_parameter_reaches_the_same_energy(v2g):
     e = s.compute_energy()
     assert s.result["status"] == 0
     assert abs(e - float(g["e_primal"])) <= 1e-6
+
+
+def test_cg_growth_stop_does_not_fire_in_converging_solves(v2g):
+    # the CG safeguard against a right-hand side in the null space of A^T
+    # (kCgGrowth, csrc/kernels.cuh) must never fire in a converging solve
+    g, s = _solve_golden(v2g, "synthetic_n5_s2")
+    e = s.compute_energy()
+    assert s.result["status"] == 0 and s.result["cg_stalls"] == 0
+    assert abs(e - float(g["e_primal"])) <= 1e-6

@@ -102,6 +102,7 @@ class Result(ctypes.Structure):
         ("t_cg", ctypes.c_double),
         ("t_xz", ctypes.c_double),
         ("t_total", ctypes.c_double),
+        ("cg_stalls", ctypes.c_long),
     ]
 
     def as_dict(self):

@@ -70,11 +70,21 @@ void launch_set_rows(int64_t n, int B, const double* row, double* out, const int
 // CG pieces (cg_solver.cc:125-177), per instance with cg_active masks.
 struct CgScalars {
     double rr, pap, alpha, beta, rrnew, tol;
-    int active;   // still iterating
-    int iter;     // iter_ of the reference
-    int do_p;     // p update pending this iteration
+    double rrmin;  // smallest r.r of this solve
+    int active;    // still iterating
+    int iter;      // iter_ of the reference
+    int do_p;      // p update pending this iteration
     int maxiter;
+    int stalled;   // stopped because r.r grew past kCgGrowth * rrmin
 };
+// A A^T is singular (the constraint rows are dependent), so a right-hand side
+// with a component in the null space of A^T above the CG tolerance (rounding
+// in A(c - z) and A x) cannot be met: r stalls at that component and CG then
+// diverges, with y growing without bound.  A converging CG never lets r.r rise
+// by more than ~30x above its running minimum (|r| 5.3x in the BPSDP runs
+// measured); a rise past this factor stops the instance's CG with the current
+// y instead.
+constexpr double kCgGrowth = 1e4;
 // r = rhs - Ap ; p = r
 void launch_cg_init(int64_t n, int B, const double* rhs, const double* Ap, double* r, double* p, const CgScalars* cs,
                     cudaStream_t s);

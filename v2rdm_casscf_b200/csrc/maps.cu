@@ -475,6 +475,7 @@ __global__ void cg_set_rr_kernel(int B, CgScalars* cs, const double* rr, int* n_
     for (int b = threadIdx.x; b < B; b += blockDim.x) {
         if (cs[b].active) {
             cs[b].rr = rr[b];
+            cs[b].rrmin = rr[b];
             cnt++;
         }
     }
@@ -486,6 +487,13 @@ __global__ void cg_alpha_kernel(int B, CgScalars* cs, const double* pap) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B || !cs[b].active) return;
     cs[b].pap = pap[b];
+    if (!(pap[b] > 0.0)) {
+        // p has no component outside the null space of A^T (or r = 0): no step
+        cs[b].alpha = 0.0;
+        cs[b].active = 0;
+        cs[b].stalled = 1;
+        return;
+    }
     cs[b].alpha = cs[b].rr / pap[b];
 }
 
@@ -525,11 +533,18 @@ __global__ void cg_beta_kernel(int B, CgScalars* cs, const double* rrnew, int* n
             const double nrm = sqrt(rn);
             c.rrnew = rn;
             if (!(nrm < c.tol)) {
-                c.beta = rn / c.rr;
-                c.rr = rn;
-                c.do_p = 1;
-                c.iter += 1;
-                if (c.iter >= c.maxiter) c.active = 0;
+                if (rn > kCgGrowth * c.rrmin) {
+                    // diverging on the null space of A^T: keep the current y (kernels.cuh)
+                    c.active = 0;
+                    c.stalled = 1;
+                } else {
+                    c.beta = rn / c.rr;
+                    c.rr = rn;
+                    c.rrmin = fmin(c.rrmin, rn);
+                    c.do_p = 1;
+                    c.iter += 1;
+                    if (c.iter >= c.maxiter) c.active = 0;
+                }
             } else {
                 c.active = 0;
             }

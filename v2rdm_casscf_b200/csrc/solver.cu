@@ -442,7 +442,7 @@ class GroupRun {
         res.assign(B_, v2g_result{});
         std::vector<double> mu(B_), ep(B_, 0.0), ed(B_, 0.0), egap(B_, 0.0);
         std::vector<int> active(B_, 1), oiter(B_, 0);
-        std::vector<long> iiter(B_, 0);
+        std::vector<long> iiter(B_, 0), stalls(B_, 0);
         std::vector<double> coef(B_);
         for (int b = 0; b < B_; b++) {
             mu[b] = P_[b]->mu;
@@ -467,6 +467,7 @@ class GroupRun {
                     if (fs[b]) {
                         mu[b] = 1.0;
                         iiter[b] += cs[b].iter;
+                        stalls[b] += cs[b].stalled;
                     }
             }
         }
@@ -486,6 +487,7 @@ class GroupRun {
                     if (recover[b]) {
                         mu[b] = 1.0;
                         iiter[b] += cs[b].iter;
+                        stalls[b] += cs[b].stalled;
                         recover[b] = 0;
                         ycount[b] = 0;
                         aa.restart(b);
@@ -567,6 +569,7 @@ class GroupRun {
                 const double e_p = hscal_[2 * B_ + b], e_d = hscal_[3 * B_ + b];
                 const long ii = cs[b].iter;
                 iiter[b] += ii;
+                stalls[b] += cs[b].stalled;
                 if (oiter[b] % o.mu_update_frequency == 0 && oiter[b] > 0) {
                     mu[b] = mu[b] * ep[b] / ed[b];
                     mu_changed[b] = 1;
@@ -584,6 +587,7 @@ class GroupRun {
                 res[b].mu = mu[b];
                 res[b].oiter = oiter[b];
                 res[b].iiter = iiter[b];
+                res[b].cg_stalls = stalls[b];
                 res[b].efzc = P.efzc;
                 res[b].enuc = P.enuc;
                 if (!std::isfinite(ep[b]) || !std::isfinite(ed[b]) || !std::isfinite(e_p)) {

@@ -252,10 +252,11 @@ def run_gpu(args):
         launches, h2d, d2h = int(t[0]), float(t[1]), float(t[2])
     conv = [r["status"] == 0 for r in results]
     n_conv = int(sum(conv))
-    if world > 1:  # instances converged on all ranks
-        t = torch.tensor([float(n_conv)], dtype=torch.float64, device=f"cuda:{dev}")
+    n_stall = int(sum(r["cg_stalls"] for r in results))
+    if world > 1:  # instances converged and CG stops on all ranks
+        t = torch.tensor([float(n_conv), float(n_stall)], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        n_conv = int(t[0])
+        n_conv, n_stall = int(t[0]), int(t[1])
     if rank == 0:
         oiters = {}
         for i, r in zip(mine, results):
@@ -325,6 +326,7 @@ def run_gpu(args):
             "launches_timed": map_n,
         },
         "converged": n_conv,
+        "cg_stalls": n_stall,
         "unconverged": [{"instance": int(mine[k]), "n": int(all_spaces[mine[k]].n), "status": int(r["status"]),
                          "oiter": int(r["oiter"])} for k, r in enumerate(results) if r["status"] != 0],
         "wall_s": wall,

@@ -202,6 +202,17 @@ int v2g_read_checkpoint(v2g_handle* h, const char* path);
 /* The full BPSDP solve from the handle's current state. */
 int v2g_solve(v2g_handle* h, v2g_result* res);
 
+/* One-step orbital optimisation runs the BPSDP loop with RotateOrbitals (focas)
+ * every ORBOPT_FREQUENCY outer iterations inside it (v2rdm_solver.cc:1855-1873):
+ * mu, the outer-iteration count (the mu schedule), the last eps(p) / eps(d)
+ * (the next CG tolerance) and x, y, z carry on across the rotations.  This
+ * continues the handle's loop where the previous v2g_solve / v2g_solve_continue
+ * stopped, for at most max_outer outer iterations, so the caller can rotate the
+ * orbitals and call v2g_set_hamiltonian between segments.  Returns
+ * V2G_ERR_NOT_CONVERGED when the segment ended unconverged (res->oiter counts
+ * from the start of the loop; res->iiter counts this segment). */
+int v2g_solve_continue(v2g_handle* h, int max_outer, v2g_result* res);
+
 /* Solves count independent problems in one GPU run.  Handles with the same
  * layout share index tables; each keeps its own convergence test and stops
  * independently.  Returns V2G_OK when every instance converged. */

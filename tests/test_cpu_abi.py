@@ -39,3 +39,23 @@ def test_ctypes_struct_matches_header(cname, pyname):
     size, offsets = _c_layout(cname, fields)
     assert ctypes.sizeof(cls) == size
     assert [getattr(cls, f).offset for f in fields] == offsets
+
+
+def test_solve_continue_checks_its_arguments():
+    # v2g_solve_continue (one-step orbital optimisation segments): bad
+    # arguments are refused before any device work; without a GPU the
+    # solve reports V2G_ERR_NO_DEVICE instead of falling back to the CPU
+    import ctypes
+
+    import torch
+
+    import v2rdm_casscf_b200 as V
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    L = V.lib()
+    r = V.Result()
+    assert L.v2g_solve_continue(None, 10, ctypes.byref(r)) == V.V2G_ERR_ARG
+    s = V.V2RDMSolver.from_active_space(synthetic(4, 0))
+    assert L.v2g_solve_continue(s.h, 0, ctypes.byref(r)) == V.V2G_ERR_ARG
+    if not torch.cuda.is_available():
+        assert L.v2g_solve_continue(s.h, 10, ctypes.byref(r)) == V.V2G_ERR_NO_DEVICE

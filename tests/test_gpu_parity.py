@@ -336,3 +336,34 @@ def test_cg_growth_stop_does_not_fire_in_converging_solves(v2g):
     e = s.compute_energy()
     assert s.result["status"] == 0 and s.result["cg_stalls"] == 0
     assert abs(e - float(g["e_primal"])) <= 1e-6
+
+
+def test_segmented_solve_continues_the_loop(v2g):
+    # one-step orbital optimisation runs the loop in segments with focas
+    # between them (v2rdm_solver.cc:1855-1873): v2g_solve_continue carries
+    # mu, the outer-iteration count (the mu schedule), eps(p) / eps(d) and
+    # x, y, z across segments, so segments of 100 outer iterations with the
+    # (here unchanged) integrals set again in between reach the reference's
+    # energy in about the outer iterations of one solve
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    g = load(os.path.join(GOLDEN, "solve_synthetic_n4_s0.npz"))
+    a = synthetic(4, int(g["seed"]))
+    opts = dict(R_CONVERGENCE=float(g["r_conv"]), E_CONVERGENCE=float(g["e_conv"]))
+    s1 = v2g.V2RDMSolver.from_active_space(a, options=opts)
+    s1.guess()
+    s1.compute_energy()
+    s = v2g.V2RDMSolver.from_active_space(a, options=opts)
+    s.guess()
+    segments = 0
+    while True:
+        r = s.solve_continue(100)
+        segments += 1
+        if r["status"] == 0:
+            break
+        assert r["status"] == v2g.V2G_ERR_NOT_CONVERGED and segments < 100
+        assert r["oiter"] == 100 * segments
+        s.set_hamiltonian(a.oei_packed, a.qmo, a.nq, a.enuc)
+    assert segments > 1
+    assert abs(r["e_total"] - float(g["e_primal"])) <= 1e-6
+    assert abs(r["oiter"] - s1.result["oiter"]) <= 0.05 * s1.result["oiter"]

@@ -35,7 +35,7 @@ EXPORTS = [
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
     "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density",
-    "v2g_write_checkpoint", "v2g_read_checkpoint", "v2g_set_active_orbital_energies",
+    "v2g_write_checkpoint", "v2g_read_checkpoint", "v2g_set_active_orbital_energies", "v2g_solve_continue",
 ]
 
 
@@ -152,6 +152,7 @@ def lib():
         L.v2g_set_active_orbital_energies.argtypes = [P, DP]
         L.v2g_read_checkpoint.argtypes = [P, ctypes.c_char_p]
         L.v2g_solve.argtypes = [P, ctypes.POINTER(Result)]
+        L.v2g_solve_continue.argtypes = [P, I, ctypes.POINTER(Result)]
         L.v2g_solve_batch.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(Result)]
         L.v2g_export_A.argtypes = [P, LP, IP, DP]
         L.v2g_trace.restype = L_
@@ -413,6 +414,18 @@ class V2RDMSolver:
             raise V2GError(code, "v2RDM did not converge.")
         _check(code)
         return r.e_total
+
+    def solve_continue(self, max_outer):
+        """Continues the BPSDP loop for at most max_outer outer iterations
+        (v2g_solve_continue: one-step orbital optimisation segments); returns
+        the result dict, with status V2G_ERR_NOT_CONVERGED when the segment
+        ended unconverged."""
+        r = Result()
+        code = lib().v2g_solve_continue(self.h, int(max_outer), ctypes.byref(r))
+        self.result = r.as_dict()
+        if code not in (V2G_OK, V2G_ERR_NOT_CONVERGED):
+            _check(code)
+        return self.result
 
     def trace(self):
         L = lib()

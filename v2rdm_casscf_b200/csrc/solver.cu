@@ -39,6 +39,9 @@ thread_local std::string g_last_error;
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+struct NoDevice : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
 
 #define CK(call)                                                                                         \
     do {                                                                                                 \
@@ -211,6 +214,13 @@ struct Problem {
     std::shared_ptr<DeviceTables> T;
     std::vector<std::array<double, 8>> trace;
     std::vector<double> energies;  // active orbital energies, if the caller gave them
+    // Loop state carried by v2g_solve_continue: outer iterations done and the
+    // last eps(p), eps(d) (they set the next CG tolerance); every solve
+    // updates them.  resume > 0 makes the next solve continue the loop for at
+    // most that many outer iterations.
+    long oiter_done = 0;
+    double last_ep = 0.0, last_ed = 0.0;
+    int resume = 0;
 
     DeviceTables& tables() {
         if (!T) T = get_tables(L, device);
@@ -444,10 +454,20 @@ class GroupRun {
         std::vector<int> active(B_, 1), oiter(B_, 0);
         std::vector<long> iiter(B_, 0), stalls(B_, 0);
         std::vector<double> coef(B_);
+        // the last outer iteration of this call: MAXITER, or the end of a
+        // continued segment
+        std::vector<int> limit(B_);
         for (int b = 0; b < B_; b++) {
             mu[b] = P_[b]->mu;
             P_[b]->trace.clear();
             res[b].status = V2G_ERR_NOT_CONVERGED;
+            limit[b] = opt(b).maxiter;
+            if (P_[b]->resume > 0) {
+                oiter[b] = (int)P_[b]->oiter_done;
+                ep[b] = P_[b]->last_ep;
+                ed[b] = P_[b]->last_ed;
+                limit[b] = oiter[b] + P_[b]->resume;
+            }
         }
         cudaEvent_t e0, e1, e2, e3;
         CK(cudaEventCreate(&e0));
@@ -460,7 +480,8 @@ class GroupRun {
         {
             std::vector<int> fs(B_);
             bool any = false;
-            for (int b = 0; b < B_; b++) any |= (fs[b] = opt(b).feasible_start ? 1 : 0) != 0;
+            for (int b = 0; b < B_; b++)
+                any |= (fs[b] = (opt(b).feasible_start && P_[b]->resume == 0) ? 1 : 0) != 0;
             if (any) {
                 feasible_start(fs, cs);
                 for (int b = 0; b < B_; b++)
@@ -604,7 +625,7 @@ class GroupRun {
                     active[b] = 0;
                     continue;
                 }
-                if (oiter[b] == o.maxiter) {
+                if (oiter[b] == limit[b]) {
                     res[b].status = V2G_ERR_NOT_CONVERGED;
                     active[b] = 0;
                     continue;
@@ -627,6 +648,9 @@ class GroupRun {
             res[b].t_xz = t_xz;
             res[b].t_total = ms_tot * 1e-3;
             P_[b]->mu = mu[b];
+            P_[b]->oiter_done = oiter[b];
+            P_[b]->last_ep = ep[b];
+            P_[b]->last_ed = ed[b];
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -979,6 +1003,8 @@ template <class F>
 int guarded(F&& f) {
     try {
         return f();
+    } catch (const NoDevice& e) {
+        return fail(V2G_ERR_NO_DEVICE, e.what());
     } catch (const CudaError& e) {
         return fail(V2G_ERR_CUDA, e.what());
     } catch (const std::invalid_argument& e) {
@@ -990,7 +1016,7 @@ int guarded(F&& f) {
 
 void require_device() {
     int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw CudaError("no CUDA device visible");
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw NoDevice("no CUDA device visible");
 }
 
 }  // namespace
@@ -1485,6 +1511,14 @@ int v2g_last_batch_stats(v2g_batch_stats* out) {
 }
 
 int v2g_solve(v2g_handle* h, v2g_result* res) { return v2g_solve_batch(&h, 1, res); }
+
+int v2g_solve_continue(v2g_handle* h, int max_outer, v2g_result* res) {
+    if (!h || !res || max_outer < 1) return v2g::fail(V2G_ERR_ARG, "bad arguments to v2g_solve_continue");
+    h->P.resume = max_outer;
+    const int st = v2g_solve_batch(&h, 1, res);  // guarded: returns a status, never throws
+    h->P.resume = 0;
+    return st;
+}
 
 long v2g_A_nnz(v2g_handle* h) {
     if (!h) return -1;

@@ -529,6 +529,8 @@ def main():
                     help="Anderson acceleration of the outer iteration with this memory (0 = off)")
     ap.add_argument("--cg-extrapolate", action="store_true",
                     help="start each CG from y_k + (y_k - y_k-1) instead of y_k (same stopping test)")
+    ap.add_argument("--accelerated", action="store_true",
+                    help="Anderson acceleration (memory 10), extrapolated CG start, MU_UPDATE_FREQUENCY 250")
     ap.add_argument("--plain", action="store_true",
                     help="reference algorithm, options and start: exact projection, CG factor 0.01, "
                          "mu update every 500, random start")
@@ -540,6 +542,10 @@ def main():
     ap.add_argument("--roofline-only", action="store_true",
                     help="run only the timed A / A^T launches of the roofline (for profiling)")
     args = ap.parse_args()
+    if args.accelerated and args.plain:
+        ap.error("--accelerated and --plain exclude each other")
+    if args.accelerated:
+        args.anderson, args.cg_extrapolate, args.mu_freq = 10, True, 250
     if args.plain:
         args.projection, args.cg_factor, args.mu_freq, args.start = "exact", 0.01, 500, "state"
         args.cg_extrapolate, args.tau, args.anderson = False, 1.0, 0

@@ -29,6 +29,12 @@ the batch take several GB), so no L2 flush is needed between steps.
             sample of sizes and extrapolated to the batch with the iteration
             counts of the same instances
 
+Loop options: --accelerated runs the solver's Anderson acceleration (memory 10)
+with the extrapolated CG start and MU_UPDATE_FREQUENCY 250 (each also on its
+own: --anderson, --cg-extrapolate, --mu-update-frequency, --tau); the line's
+config names the options used, and the default is the reference's loop from
+the feasible start with the adaptive projection.
+
 Multi-GPU (torchrun): instances are dealt to ranks by a longest-first bin-pack
 on a per-iteration cost model (v2rdm_casscf_b200/shard.py), with no exchange
 during the solve; value is the max over ranks.  `--impl reference` times the

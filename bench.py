@@ -88,7 +88,20 @@ def workload(name, count):
         from v2rdm_casscf_b200.hchain import hydrogen_scan
 
         return hydrogen_scan(20, 0.6, 3.0, count if count != 256 else 64)
+    if name == "h20t2":  # linear H20, 1.0 A, (20e,20o), DQGT2 (T2 blocks of 11,800 and 3,800)
+        from v2rdm_casscf_b200.hchain import hydrogen_chain
+
+        return [hydrogen_chain(20, 1.0)]
+    if name == "h50":  # linear H50, 1.2 A, (50e,50o), DQG (G2aa blocks of 5,000)
+        from v2rdm_casscf_b200.hchain import hydrogen_chain
+
+        return [hydrogen_chain(50, 1.2)]
     raise SystemExit(f"unknown workload {name}")
+
+
+def workload_positivity(name):
+    """POSITIVITY of a workload (DQG unless it names T2)."""
+    return "DQGT2" if name == "h20t2" else "DQG"
 
 
 def workload_text(args, count):
@@ -99,6 +112,11 @@ def workload_text(args, count):
         return "h10: linear H10, 0.9 A, STO-3G RHF orbitals, (10e,10o) all active, " + opts
     if args.workload == "h20scan":
         return f"h20scan: {count} linear H20 geometries, spacing 0.6..3.0 A, STO-3G RHF orbitals, (20e,20o), " + opts
+    if args.workload == "h20t2":
+        return ("h20t2: linear H20, 1.0 A, STO-3G RHF orbitals, (20e,20o) all active, "
+                + opts.replace("DQG", "DQGT2"))
+    if args.workload == "h50":
+        return "h50: linear H50, 1.2 A, STO-3G RHF orbitals, (50e,50o) all active, " + opts
     return f"{args.workload}: {count} synthetic active spaces, " + opts
 
 
@@ -183,7 +201,8 @@ def run_gpu(args):
 
     mine = partition(workload_costs(all_spaces), world)[rank] if world > 1 else list(range(len(all_spaces)))
     def make(maxiter):
-        opts = dict(OPTIONS, MU_UPDATE_FREQUENCY=args.mu_freq, TAU_PARAMETER=args.tau)
+        opts = dict(OPTIONS, MU_UPDATE_FREQUENCY=args.mu_freq, TAU_PARAMETER=args.tau,
+                    POSITIVITY=workload_positivity(args.workload))
         if maxiter:
             opts["MAXITER"] = maxiter
         return [V.V2RDMSolver.from_active_space(all_spaces[i], options=opts, device=dev, profile=True,
@@ -366,7 +385,8 @@ def run_gpu(args):
             # the reference runs from its own random start: its iteration counts are
             # those of a solve from that start (recorded), else this run's
             oiters, src = reference_iterations(args, [results[k]["oiter"] for k in range(len(results))])
-            out["cpu_baseline"] = cpu_baseline(all_spaces, oiters, args.cpu_sample)
+            out["cpu_baseline"] = cpu_baseline(all_spaces, oiters, args.cpu_sample,
+                                               workload_positivity(args.workload))
             out["cpu_baseline"]["sample"] += "; iteration counts: " + src
         if args.save_iterations and world == 1 and not args.max_outer and args.start == "state":
             os.makedirs(os.path.dirname(ITER_FILE), exist_ok=True)
@@ -416,20 +436,22 @@ def roofline_pass(V, solvers, spaces, mine, dev, torch, reps=20):
     return total_b / total_t / 1e9, out
 
 
-def ref_time_per_iteration(space, iters, threads):
+def ref_time_per_iteration(space, iters, threads, positivity="DQG"):
     """Seconds per outer iteration of the reference on one instance (after one warm-up iteration)."""
     from oracle import ref as R
 
     R.set_threads(threads)
     r = R.RefSolver([space.n], [space.nb], soccpi=[space.na - space.nb], multiplicity=space.multiplicity,
-                    positivity="DQG", r_convergence=OPTIONS["R_CONVERGENCE"], e_convergence=OPTIONS["E_CONVERGENCE"])
+                    positivity=positivity, r_convergence=OPTIONS["R_CONVERGENCE"],
+                    e_convergence=OPTIONS["E_CONVERGENCE"])
     r.set_integrals(space.oei_packed, space.qmo, space.nq)
     r.guess()
     r.build_constraints()
     out = r.solve(max_outer=iters + 1, trace_cap=0)
     t1 = out["t_total"]
     r2 = R.RefSolver([space.n], [space.nb], soccpi=[space.na - space.nb], multiplicity=space.multiplicity,
-                     positivity="DQG", r_convergence=OPTIONS["R_CONVERGENCE"], e_convergence=OPTIONS["E_CONVERGENCE"])
+                     positivity=positivity, r_convergence=OPTIONS["R_CONVERGENCE"],
+                     e_convergence=OPTIONS["E_CONVERGENCE"])
     r2.set_integrals(space.oei_packed, space.qmo, space.nq)
     r2.guess()
     r2.build_constraints()
@@ -446,7 +468,7 @@ def reference_iterations(args, fallback):
     return fallback, "outer-iteration counts of this run"
 
 
-def cpu_baseline(spaces, oiters, sample_sizes):
+def cpu_baseline(spaces, oiters, sample_sizes, positivity="DQG"):
     """Reference CPU time for the batch, extrapolated from a timed sample."""
     from oracle import ref as R
 
@@ -461,7 +483,7 @@ def cpu_baseline(spaces, oiters, sample_sizes):
     per_it = {}
     for n in sample:
         iters = 1 if n >= 16 else (2 if n >= 12 else 3)
-        per_it[n] = ref_time_per_iteration(by_n[n], iters, threads)
+        per_it[n] = ref_time_per_iteration(by_n[n], iters, threads, positivity)
     # power-law fit t(n) = a n^p over the sampled sizes for the others
     xs = np.log(np.array(sample, dtype=float))
     ys = np.log(np.array([per_it[n] for n in sample]))
@@ -496,7 +518,7 @@ def run_reference(args):
     vals = []
     base = None
     for _ in range(args.warmup + args.steps):
-        base = cpu_baseline(spaces, oiters, args.cpu_sample)
+        base = cpu_baseline(spaces, oiters, args.cpu_sample, workload_positivity(args.workload))
         vals.append(base["value"])
     value = float(np.mean(vals[args.warmup:]))
     base["value"] = value

@@ -17,6 +17,7 @@ stated tolerance.
 import math
 
 import numpy as np
+from scipy.special import erf
 
 from .hamiltonian import ActiveSpace
 
@@ -31,7 +32,7 @@ def _boys0(t):
     small = t < 1e-12
     out[small] = 1.0 - t[small] / 3.0
     ts = t[~small]
-    out[~small] = 0.5 * np.sqrt(np.pi / ts) * np.vectorize(math.erf)(np.sqrt(ts))
+    out[~small] = 0.5 * np.sqrt(np.pi / ts) * erf(np.sqrt(ts))
     return out
 
 

@@ -480,8 +480,9 @@ class GroupRun {
         {
             std::vector<int> fs(B_);
             bool any = false;
+            // a continued loop keeps its state; its first segment starts like a solve
             for (int b = 0; b < B_; b++)
-                any |= (fs[b] = (opt(b).feasible_start && P_[b]->resume == 0) ? 1 : 0) != 0;
+                any |= (fs[b] = (opt(b).feasible_start && oiter[b] == 0) ? 1 : 0) != 0;
             if (any) {
                 feasible_start(fs, cs);
                 for (int b = 0; b < B_; b++)

@@ -121,3 +121,23 @@ def test_port_agrees_with_product_table(v2g):
     s = v2g.V2RDMSolver([5], 3, 2, 2)
     P = csr_of(s)
     assert (A - P).count_nonzero() == 0 or abs(A - P).max() <= 1e-15
+
+
+def test_port_accelerated_configuration_on_a_chain():
+    # the bench's --accelerated loop options (Anderson memory 10, extrapolated
+    # CG start, MU_UPDATE_FREQUENCY 250) on H4 at 1.0 A: the plain loop's
+    # energy in a fraction of its outer and CG iterations
+    from v2rdm_casscf_b200.hchain import hydrogen_chain
+
+    a = hydrogen_chain(4, 1.0)
+    L = port.Layout(a.n, a.na, a.nb)
+    A = port.build_A(L).tocsr()
+    b = port.build_b(L, A.shape[0])
+    c = port.build_c(L, a.h, a.eri())
+    w, _ = port.cg(A, np.zeros(A.shape[0]), b, 1e-10 * np.linalg.norm(b), 20000)
+    runs = [port.solve(L, A, b, c, A.T @ w, np.zeros(A.shape[0]), np.zeros(L.dimx), 1e-6, 1e-7, **kw)
+            for kw in ({}, dict(anderson_memory=10, cg_extrapolate=True, mu_update_frequency=250))]
+    assert all(r["converged"] for r in runs)
+    assert abs(runs[1]["e_primal"] - runs[0]["e_primal"]) <= 1e-6
+    assert runs[1]["oiter"] <= 0.6 * runs[0]["oiter"]
+    assert runs[1]["iiter"] <= 0.6 * runs[0]["iiter"]

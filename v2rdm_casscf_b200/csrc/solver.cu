@@ -263,24 +263,11 @@ class GroupRun {
             yprev_.alloc(C);
             ex_.alloc(B_);
         }
-        for (auto* p : P_) aa_m_ = std::max(aa_m_, p->opt.anderson_memory);
-        if (aa_m_ > 0) {
-            aw_.alloc(2 * X);
-            af_.alloc(2 * X);
-            ag_.alloc(2 * X);
-            adF_.alloc(2 * X * aa_m_);
-            adG_.alloc(2 * X * aa_m_);
-            agam_.alloc((size_t)B_ * aa_m_);
-            apart_.alloc(aa_partial_size(nx_, B_, aa_m_));
-            adots_.alloc((size_t)(2 * aa_m_ + 1) * B_);
-            amode_.alloc(B_);
-            aslot_.alloc(B_);
-            amix_.alloc(B_);
-        }
         CK(cudaMallocHost(&hscal_, sizeof(double) * 4 * B_));
         CK(cudaMallocHost(&hnact_, sizeof(int) * 8));
         build_projection_plan();
         upload_state();
+        alloc_anderson(X);
         for (auto* p : P_) profile_ = profile_ || p->profile;
         if (profile_) {
             prof_ev_.resize(256);
@@ -525,7 +512,7 @@ class GroupRun {
             CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
             if (aa_m_ > 0) {
                 // w = the (x, z) this step starts from
-                for (int b = 0; b < B_; b++) aa.mode[b] = (active[b] && opt(b).anderson_memory > 0) ? 1 : 0;
+                for (int b = 0; b < B_; b++) aa.mode[b] = (active[b] && aa_memory(b) > 0) ? 1 : 0;
                 CK(cudaMemcpyAsync(amode_.p, aa.mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
                 launch_aa_save(nx_, B_, x_.p, z_.p, aw_.p, amode_.p, s_);
             }
@@ -659,6 +646,37 @@ class GroupRun {
         cudaEventDestroy(e3);
     }
 
+    // The Anderson history of the group (after every other buffer): (3 + 2 m)
+    // state vectors.  m shrinks to what 80 % of the free device memory holds,
+    // or the acceleration is switched off for this group, with a note on stderr.
+    void alloc_anderson(size_t X) {
+        for (auto* p : P_) aa_m_ = std::max(aa_m_, p->opt.anderson_memory);
+        if (aa_m_ <= 0) return;
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        const double vec = 2.0 * (double)X * sizeof(double);
+        const int fit = (int)std::floor((0.8 * (double)free_b / vec - 3.0) / 2.0);
+        if (fit < aa_m_) {
+            std::fprintf(stderr, "v2g: Anderson memory %d does not fit in device memory next to this group; using %d\n",
+                         aa_m_, std::max(fit, 0));
+            aa_m_ = std::max(fit, 0);
+            if (aa_m_ == 0) return;
+        }
+        aw_.alloc(2 * X);
+        af_.alloc(2 * X);
+        ag_.alloc(2 * X);
+        adF_.alloc(2 * X * aa_m_);
+        adG_.alloc(2 * X * aa_m_);
+        agam_.alloc((size_t)B_ * aa_m_);
+        apart_.alloc(aa_partial_size(nx_, B_, aa_m_));
+        adots_.alloc((size_t)(2 * aa_m_ + 1) * B_);
+        amode_.alloc(B_);
+        aslot_.alloc(B_);
+        amix_.alloc(B_);
+    }
+    // An instance's history length: its anderson_memory within the group's allocation.
+    int aa_memory(int b) const { return std::min(P_[b]->opt.anderson_memory, aa_m_); }
+
     // Anderson acceleration after a step: f = g - w enters the history of every
     // instance still iterating with anderson_memory > 0, and an instance with
     // at least one difference column continues from g - sum_j gamma_j dG_j,
@@ -672,7 +690,7 @@ class GroupRun {
         for (int b = 0; b < B_; b++) {
             aa.mode[b] = 0;
             if (!active[b] || recover[b]) continue;
-            if (aa.begin(b, P_[b]->opt.anderson_memory, mu_changed[b] != 0)) any = true;
+            if (aa.begin(b, aa_memory(b), mu_changed[b] != 0)) any = true;
         }
         if (!any) return;
         CK(cudaMemcpyAsync(amode_.p, aa.mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
@@ -686,7 +704,7 @@ class GroupRun {
         std::vector<int> mix(B_, 0);
         bool anymix = false;
         for (int b = 0; b < B_; b++) {
-            if (aa.finish(b, P_[b]->opt.anderson_memory, dots, &gamma[(size_t)b * aa_m_])) {
+            if (aa.finish(b, aa_memory(b), dots, &gamma[(size_t)b * aa_m_])) {
                 mix[b] = 1;
                 anymix = true;
             }

@@ -465,6 +465,10 @@ def reference_iterations(args, fallback):
         d = json.load(open(ITER_FILE))
         return d["outer_iterations"], ("outer-iteration counts of the same instances solved on the GPU from the "
                                        "reference's random start with its loop options (profiles/)")
+    golden = os.path.join(ROOT, "tests", "golden", "solve_h10_chain.npz")
+    if args.workload == "h10" and os.path.exists(golden):
+        return [int(np.load(golden)["oiter"])], ("the outer-iteration count of the compiled reference's own solve of "
+                                                 "this input from its random start (tests/golden/solve_h10_chain.npz)")
     plain = (args.start == "state" and args.anderson == 0 and not args.cg_extrapolate and args.tau == 1.0
              and args.mu_freq == 500)
     if plain:
@@ -518,7 +522,7 @@ def run_reference(args):
         return
     spaces = workload(args.workload, args.count)
     oiters, src = reference_iterations(args, [2500] * len(spaces))
-    if not (args.workload == "batch256" and args.count == 256 and os.path.exists(ITER_FILE)):
+    if not (args.workload == "batch256" and args.count == 256 and os.path.exists(ITER_FILE)) and args.workload != "h10":
         src = "2500 outer iterations per instance (no recorded counts for this workload)"
     vals = []
     base = None

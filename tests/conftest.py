@@ -10,6 +10,7 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
+    config.addinivalue_line("markers", "late: runs after every other test (options beyond the reference's loop)")
 
 
 def _has_gpu():
@@ -22,6 +23,9 @@ def _has_gpu():
 
 
 def pytest_collection_modifyitems(config, items):
+    # tests of options beyond the reference's loop run last, so that a stop at
+    # the first failure (-x) never hides a parity result
+    items[:] = [i for i in items if "late" not in i.keywords] + [i for i in items if "late" in i.keywords]
     if _has_gpu():
         return
     skip = pytest.mark.skip(reason="no CUDA device")

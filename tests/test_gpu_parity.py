@@ -264,10 +264,11 @@ def test_feasible_start_reaches_reference_energy(v2g, name):
     assert abs(e - float(g["e_primal"])) <= 1e-6
 
 
-# Options beyond the reference's loop (they change the path, not the answer); last, so that
-# every parity test above runs before them.
+# Options beyond the reference's loop (they change the path, not the answer); marked late,
+# so that they run after every other test.
 
 
+@pytest.mark.late
 def test_cg_extrapolation_reaches_the_same_energy(v2g):
     # cg_extrapolate: CG starts from y_k + (y_k - y_{k-1}) with the reference's
     # stopping test, so the energy is the reference's and CG needs fewer
@@ -291,6 +292,7 @@ def test_cg_extrapolation_reaches_the_same_energy(v2g):
     assert abs(res[2]["e_total"] - float(g1["e_primal"])) <= 1e-6
 
 
+@pytest.mark.late
 def test_anderson_acceleration_reaches_the_same_energy(v2g):
     # anderson_memory: the stopping test and energies are the plain step's, so
     # the reference's energy is reached, in far fewer outer iterations.  One
@@ -314,6 +316,7 @@ def test_anderson_acceleration_reaches_the_same_energy(v2g):
     assert res[1]["oiter"] <= 0.8 * res[2]["oiter"]
 
 
+@pytest.mark.late
 def test_tau_parameter_reaches_the_same_energy(v2g):
     # TAU_PARAMETER at the top of the plugin's documented range [1.0, 1.6]
     # (plugin.cc:94-97) changes the path, not the answer
@@ -329,6 +332,7 @@ def test_tau_parameter_reaches_the_same_energy(v2g):
     assert abs(e - float(g["e_primal"])) <= 1e-6
 
 
+@pytest.mark.late
 def test_cg_growth_stop_does_not_fire_in_converging_solves(v2g):
     # the CG safeguard against a right-hand side in the null space of A^T
     # (kCgGrowth, csrc/kernels.cuh) must never fire in a converging solve
@@ -338,6 +342,7 @@ def test_cg_growth_stop_does_not_fire_in_converging_solves(v2g):
     assert abs(e - float(g["e_primal"])) <= 1e-6
 
 
+@pytest.mark.late
 def test_segmented_solve_continues_the_loop(v2g):
     # one-step orbital optimisation runs the loop in segments with focas
     # between them (v2rdm_solver.cc:1855-1873): v2g_solve_continue carries

@@ -89,6 +89,14 @@ typedef struct v2g_options {
                                    stopping test and the energies are taken on the un-accelerated
                                    step as in the plugin; the history restarts when mu changes;
                                    0 = off, at most 16 (0) */
+    int mixed_precision;        /* 1: while an instance's adaptive projection tolerance (see
+                                   adaptive_projection) is at least 1e-5, the dense products of the
+                                   projection of its large blocks (refinement residuals, eigenvector
+                                   updates, x = V D+ V^T and z = V D- V^T) run on the tensor cores as
+                                   3xTF32 products with FP32 accumulation (FP32 accuracy); below it
+                                   they run in FP64, whose first refinement sweeps take the
+                                   eigenvectors from FP32 to FP64 accuracy.  Maps, CG, errors and
+                                   energies stay FP64.  Needs adaptive_projection (0) */
 } v2g_options;
 
 typedef struct v2g_result {
@@ -161,18 +169,32 @@ int v2g_update_xz(v2g_handle* h, double mu);
 /* The projection step of v2g_update_xz on caller-owned device vectors,
  * allocating no device memory.  No counterpart in the reference: it is for
  * host programs that cannot call cudaMalloc while they run (a pool allocator
- * that owns all device memory, a fixed device-memory budget).  Inputs c and y
- * and the in/out x (dimx, dimx and nconstraints doubles, device memory);
- * output z (dimx).  Limits: every block of dimension <= 64 and dimx <= 65536,
+ * that owns all device memory, a fixed device-memory budget).  Device memory
+ * in: d_c (dimx doubles) and d_y (nconstraints doubles); in/out: d_x (dimx);
+ * out: d_z (dimx).  Limits: every block of dimension <= 64 and dimx <= 65536,
  * else V2G_ERR_ARG; the handle's device tables must exist (v2g_update_xz, a
  * map call or a solve builds them).  Scratch is a static device array of
  * about 0.5 MiB that every GPU loading the library holds until exit; the
  * first call on a device looks up its address, so make that call before any
- * stream capture.  Calls share the array: calls that overlap on the GPU
- * (other streams or host threads) race.  Asynchronous on the given stream
- * (NULL: the legacy default stream). */
+ * stream capture.  mu and the block list reach the device as a kernel
+ * argument: no host memory is copied.  Calls share the array: calls that
+ * overlap on the GPU (other streams or host threads) race.  Asynchronous on
+ * the given stream (NULL: the legacy default stream); the caller's current
+ * device is left as it was. */
 int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const double* d_y, double* d_x, double* d_z,
                           void* stream);
+
+/* The dense product of the projection on caller-owned device buffers, for
+ * tests and inspection: for nblocks symmetric blocks of dimensions dims[i]
+ * (each padded to np_i = dims rounded up to a multiple of 64 and stored
+ * row-major np_i x np_i, one after the other), C_i = op(A_i) diag(d_i) op(B_i)
+ * with op = transpose where trans* is set and d (np_i per block, one after the
+ * other) optional.  tensor_cores = 1 runs the 3xTF32 tcgen05 kernel of the
+ * mixed-precision projection, 0 the FP64 kernel.  Synchronous; returns
+ * V2G_ERR_CUDA when a tensor-core pipeline wait ran out.  No counterpart in
+ * the reference (it calls F_DGEMM, v2rdm_solver.cc:3273,3286). */
+int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int transA, const double* B, int transB,
+                          const double* d, double* C, int tensor_cores, int device);
 
 /* The RDMs handed to the orbital optimiser, as PackSpatialDensity
  * (v2rdm_solver.cc:3664-3773), from the handle's x: d1 = spin-summed 1-RDM,

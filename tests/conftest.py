@@ -23,9 +23,14 @@ def _has_gpu():
 
 
 def pytest_collection_modifyitems(config, items):
-    # tests of options beyond the reference's loop run last, so that a stop at
-    # the first failure (-x) never hides a parity result
-    items[:] = [i for i in items if "late" not in i.keywords] + [i for i in items if "late" in i.keywords]
+    # tests of options beyond the reference's loop run after the parity tests,
+    # so that a stop at the first failure (-x) never hides a parity result; the
+    # allocation-free entry point's file (test_zz_*) stays the very last
+    def rank(it):
+        last = os.path.basename(str(it.fspath)).startswith("test_zz_")
+        return (2 if last else (1 if "late" in it.keywords else 0))
+
+    items[:] = sorted(items, key=rank)
     if _has_gpu():
         return
     skip = pytest.mark.skip(reason="no CUDA device")

@@ -14,8 +14,17 @@ inputs and outputs as .npz files:
   solve_<case>.npz  a full BPSDP solve (random start, srand(0)) of a seeded
                     synthetic active space: final energies, iteration counts,
                     the per-iteration trace and the final x, y, z
+  mapsum_<case>.npz A u and A^T w at sizes too large to store (n = 10 and 20
+                    DQG, n = 6 and 8 DQGT2): seeded inputs, sampled outputs
+                    and projections
+  energy_<case>.npz a full BPSDP solve of an instance of the batched workload
+                    (n = 8..20, seed = its index in the batch): energies,
+                    iteration counts and CPU seconds only (the vectors of
+                    these sizes are too large for a fixture)
 
-Usage: python tests/golden/make_golden.py   (needs `make -C oracle` first)
+Usage: python tests/golden/make_golden.py [part ...]   (needs `make -C oracle` first)
+       parts: maps pack c xz solve h10 mapsum energy (default: all but mapsum
+       and energy; energy takes about an hour of CPU time)
 """
 import os
 import sys
@@ -56,6 +65,26 @@ PACK_CASES = {
     "c1_n5_doublet": ([5], [2], [1], [0.5, 0.1, 0.3, 0.3, 0.2]),
     "c2v_n6": ([2, 1, 1, 2], [1, 0, 0, 1], [0, 0, 0, 0], [0.3, 1.1, 0.2, 0.5, 0.1, 0.9]),
     "c2_n5_doublet": ([3, 2], [1, 1], [1, 0], [0.2, 0.4, 0.9, 0.3, 0.35]),
+}
+
+# map checks at sizes whose vectors are too large for a fixture: the inputs are
+# regenerated from the seed, and the fixture keeps 4096 sampled entries of A u
+# and A^T w, their largest magnitudes and two projections onto seeded vectors
+MAPSUM_CASES = {
+    # name: (n, positivity)
+    "c1_n10_dqg": (10, "DQG"),
+    "c1_n20_dqg": (20, "DQG"),
+    "c1_n6_dqgt2": (6, "DQGT2"),
+    "c1_n8_dqgt2": (8, "DQGT2"),
+}
+
+# instances of the batched workload (bench.py batch256: n = batch_sizes(256)[seed]),
+# solved by the reference to R_CONVERGENCE 1e-6 / E_CONVERGENCE 1e-7
+ENERGY_CASES = {
+    # name: (n, seed)
+    "batch_n8_s3": (8, 3),
+    "batch_n10_s40": (10, 40),
+    "batch_n12_s13": (12, 13),
 }
 
 SOLVE_CASES = {
@@ -157,6 +186,47 @@ def solve(name, spec):
                         x=r.get("x"), y=r.get("y"), z=r.get("z"))
 
 
+def mapsum_vectors(dimx, ncon, seed=2026):
+    """The seeded inputs and projection vectors of a map-checksum fixture."""
+    rng = np.random.default_rng(seed)
+    u = rng.standard_normal(dimx)
+    w = rng.standard_normal(ncon)
+    pa = rng.standard_normal(ncon)
+    pt = rng.standard_normal(dimx)
+    ia = np.sort(rng.choice(ncon, size=min(4096, ncon), replace=False))
+    it = np.sort(rng.choice(dimx, size=min(4096, dimx), replace=False))
+    return u, w, pa, pt, ia, it
+
+
+def mapsum(name, n, pos):
+    r = RefSolver([n], [n // 2], positivity=pos)
+    r.build_constraints()
+    u, w, pa, pt, ia, it = mapsum_vectors(r.dimx, r.ncon)
+    au, atw = r.Au(u), r.ATu(w)
+    np.savez_compressed(os.path.join(HERE, f"mapsum_{name}.npz"), n=n, positivity=pos, dimx=r.dimx, ncon=r.ncon,
+                        block_dims=r.block_dims, idx_a=ia, au=au[ia], idx_t=it, atw=atw[it],
+                        au_max=np.abs(au).max(), atw_max=np.abs(atw).max(), au_dot=au @ pa, atw_dot=atw @ pt,
+                        au_norm=np.linalg.norm(au), atw_norm=np.linalg.norm(atw))
+
+
+def solve_energy(name, n, seed):
+    """Reference solve of one batched-workload instance; energies and counts only."""
+    from v2rdm_casscf_b200.hamiltonian import batch_sizes
+
+    assert int(batch_sizes(256)[seed]) == n, "seed is not an n-orbital instance of the batch"
+    a = synthetic(n, seed)
+    r = RefSolver([n], [a.nb], soccpi=[a.na - a.nb], multiplicity=a.multiplicity, positivity="DQG",
+                  r_convergence=1e-6, e_convergence=1e-7)
+    r.set_integrals(a.oei_packed, a.qmo, a.nq)
+    r.guess()
+    r.build_constraints()
+    out = r.solve()
+    np.savez_compressed(os.path.join(HERE, f"energy_{name}.npz"), n=n, seed=seed, r_conv=1e-6, e_conv=1e-7,
+                        electrons=a.na + a.nb, e_primal=out["e_primal"], e_dual=out["e_dual"], ep=out["ep"],
+                        ed=out["ed"], oiter=out["oiter"], iiter=out["iiter"], converged=out["converged"],
+                        t_total=out["t_total"], threads=int(os.environ.get("OMP_NUM_THREADS", "4")))
+
+
 def solve_hchain(name, natoms, spacing):
     """Reference solve of an all-active H chain (STO-3G RHF orbitals, CD integrals)."""
     from v2rdm_casscf_b200.hchain import hydrogen_chain
@@ -177,13 +247,26 @@ def solve_hchain(name, natoms, spacing):
 
 if __name__ == "__main__":
     set_threads(int(os.environ.get("OMP_NUM_THREADS", "4")))
-    for k, v in MAP_CASES.items():
-        maps(k, v)
-    for k, v in PACK_CASES.items():
-        pack(k, v)
-    cvec()
-    xz()
-    for k, v in SOLVE_CASES.items():
-        solve(k, v)
-    solve_hchain("h10_chain", 10, 0.9)
+    parts = sys.argv[1:] or ["maps", "pack", "c", "xz", "solve", "h10"]
+    if "maps" in parts:
+        for k, v in MAP_CASES.items():
+            maps(k, v)
+    if "pack" in parts:
+        for k, v in PACK_CASES.items():
+            pack(k, v)
+    if "c" in parts:
+        cvec()
+    if "xz" in parts:
+        xz()
+    if "solve" in parts:
+        for k, v in SOLVE_CASES.items():
+            solve(k, v)
+    if "h10" in parts:
+        solve_hchain("h10_chain", 10, 0.9)
+    if "mapsum" in parts:
+        for k, v in MAPSUM_CASES.items():
+            mapsum(k, *v)
+    if "energy" in parts:
+        for k, v in ENERGY_CASES.items():
+            solve_energy(k, *v)
     print("golden fixtures written to", HERE)

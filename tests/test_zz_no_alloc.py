@@ -1,6 +1,10 @@
 """The allocation-free projection entry point (v2g_update_xz_noalloc) against
 v2g_update_xz, through the C ABI, on consecutive calls that share its static
-scratch.  Same tolerance as the projection tests: 1e-10 relative."""
+scratch.  Same tolerance as the projection tests: 1e-10 relative.
+
+Callers of this entry point run under a pool allocator or a fixed device-memory
+budget and cannot allocate, so the test also checks that the call leaves the
+device's free memory unchanged and the caller's current device as it was."""
 import numpy as np
 import pytest
 
@@ -39,19 +43,34 @@ def test_noalloc_projection_matches_update_xz(v2g):
         d_x = torch.from_numpy(x).to(dev)
         d_z = torch.full((s.dimx,), float("nan"), dtype=torch.float64, device=dev)
         stream = torch.cuda.current_stream(dev)
+        torch.cuda.synchronize(dev)
+        free0, _ = torch.cuda.mem_get_info(dev)
         s.update_xz_noalloc(mu, d_c.data_ptr(), d_y.data_ptr(), d_x.data_ptr(), d_z.data_ptr(),
                             stream.cuda_stream)
         torch.cuda.synchronize(dev)
+        free1, _ = torch.cuda.mem_get_info(dev)
         x_out, z_out = d_x.cpu().numpy(), d_z.cpu().numpy()
         scale = max(np.abs(x_ref).max(), np.abs(z_ref).max())
         assert np.isfinite(x_out).all() and np.isfinite(z_out).all()
         assert np.abs(x_out - x_ref).max() <= 1e-10 * scale
         assert np.abs(z_out - z_ref).max() <= 1e-10 * scale
+        assert free1 == free0, f"device free memory changed by {free0 - free1} bytes during the call"
+        assert torch.cuda.current_device() == 0
 
 
 def test_noalloc_rejects_large_blocks(v2g):
+    import torch
+
+    dev = torch.device("cuda:0")
     s = v2g.V2RDMSolver([6], 3, 3)  # G2aa block of 72
     rng = np.random.default_rng(0)
     s.ATu(rng.standard_normal(s.nconstraints))  # builds the device tables
+    # real buffers of the right sizes: a regression of the size check fails the
+    # assertion below instead of reading through bad pointers
+    d_c = torch.zeros(s.dimx, dtype=torch.float64, device=dev)
+    d_y = torch.zeros(s.nconstraints, dtype=torch.float64, device=dev)
+    d_x = torch.zeros(s.dimx, dtype=torch.float64, device=dev)
+    d_z = torch.zeros(s.dimx, dtype=torch.float64, device=dev)
     with pytest.raises(v2g.V2GError, match="exceeds the maximum of 64"):
-        s.update_xz_noalloc(1.0, 1, 1, 1, 1)
+        s.update_xz_noalloc(1.0, d_c.data_ptr(), d_y.data_ptr(), d_x.data_ptr(), d_z.data_ptr())
+    torch.cuda.synchronize(dev)

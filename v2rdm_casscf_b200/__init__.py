@@ -34,7 +34,7 @@ EXPORTS = [
     "v2g_guess_random", "v2g_set_state", "v2g_get_state", "v2g_apply_A", "v2g_apply_AT", "v2g_apply_A_device",
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
-    "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density",
+    "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density", "v2g_block_gemm_device",
     "v2g_write_checkpoint", "v2g_read_checkpoint", "v2g_set_active_orbital_energies", "v2g_solve_continue",
 ]
 
@@ -63,6 +63,7 @@ class Options(ctypes.Structure):
         ("start", ctypes.c_int),
         ("cg_extrapolate", ctypes.c_int),
         ("anderson_memory", ctypes.c_int),
+        ("mixed_precision", ctypes.c_int),
     ]
 
 
@@ -160,6 +161,7 @@ def lib():
         L.v2g_last_batch_stats.argtypes = [ctypes.POINTER(BatchStats)]
         for f in ("v2g_apply_A_batched_device", "v2g_apply_AT_batched_device"):
             getattr(L, f).argtypes = [P, I, P, P, P]
+        L.v2g_block_gemm_device.argtypes = [I, IP, P, I, P, I, P, P, I, I]
         _lib = L
     return _lib
 
@@ -217,13 +219,16 @@ class V2RDMSolver:
     stopping test, fewer CG iterations).  ``anderson_memory=m`` (1..16)
     accelerates the outer iteration on (x, z) with the last m step
     differences (Anderson's method; the stopping test and energies are those
-    of the plain step).
+    of the plain step).  ``mixed_precision=True`` (with the adaptive
+    projection) runs the dense products of the large blocks' projection on
+    the tensor cores (3xTF32, FP32 accuracy) while the projection tolerance is
+    at least 1e-5, and in FP64 after that.
     """
 
     def __init__(self, active, nalpha, nbeta, multiplicity=1, frozen_docc=None, restricted_docc=None,
                  restricted_uocc=None, frozen_uocc=None, options=None, device=0, record_trace=False,
                  profile=False, projection="exact", cg_tolerance_factor=0.01, start="state",
-                 cg_extrapolate=False, anderson_memory=0):
+                 cg_extrapolate=False, anderson_memory=0, mixed_precision=False):
         L = lib()
         self.active = list(active)
         opts = dict(DEFAULT_OPTIONS)
@@ -262,6 +267,7 @@ class V2RDMSolver:
         o.start = int(start == "feasible")
         o.cg_extrapolate = int(bool(cg_extrapolate))
         o.anderson_memory = int(anderson_memory)
+        o.mixed_precision = int(bool(mixed_precision))
         nirrep = len(active)
         zero = [0] * nirrep
         arrs = [np.ascontiguousarray(v if v is not None else zero, dtype=np.int32)
@@ -433,6 +439,15 @@ class V2RDMSolver:
         rows = np.zeros(8 * max(n, 1))
         L.v2g_trace(self.h, _dp(rows), n)
         return rows[: 8 * n].reshape(n, 8)
+
+
+def block_gemm_device(dims, d_a, d_b, d_c, trans_a=False, trans_b=False, d_d=None, tensor_cores=True, device=0):
+    """C_i = op(A_i) diag(d_i) op(B_i) for padded blocks on the device (pointers); see v2g_block_gemm_device."""
+    dims = np.ascontiguousarray(dims, dtype=np.int32)
+    _check(lib().v2g_block_gemm_device(len(dims), _ip(dims), ctypes.c_void_p(d_a), int(bool(trans_a)),
+                                       ctypes.c_void_p(d_b), int(bool(trans_b)),
+                                       ctypes.c_void_p(d_d) if d_d else None, ctypes.c_void_p(d_c),
+                                       int(bool(tensor_cores)), int(device)))
 
 
 def last_batch_stats():

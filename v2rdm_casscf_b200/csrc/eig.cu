@@ -17,6 +17,9 @@
 // clustered and exactly degenerate spectra these blocks have.
 #include <cfloat>
 
+#include <mutex>
+#include <vector>
+
 #include "kernels.cuh"
 
 namespace v2g {
@@ -632,9 +635,11 @@ __global__ void oa_lambda_kernel(const BlockTask* __restrict__ tasks, const doub
 __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ S,
                                 const double* __restrict__ G, const double* __restrict__ lam,
                                 const double* __restrict__ scale, const int* __restrict__ bmask,
-                                int* __restrict__ partner, int* __restrict__ hard) {
+                                int* __restrict__ partner, int* __restrict__ hard,
+                                unsigned long long* __restrict__ gdev, int* __restrict__ restart) {
     __shared__ double sr[256];
     __shared__ int sj[256];
+    __shared__ double sg[256];
     const int task = blockIdx.y;
     if (bmask && !bmask[task]) return;
     const BlockTask t = tasks[task];
@@ -642,12 +647,14 @@ __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const doubl
     if (i >= t.np) return;
     double best = -1.0;
     int bj = -1;
+    double gd = 0.0;  // max_j |G_ij - delta_ij| of this row: how far V is from orthonormal
     if (i < t.n) {
         const double negligible = 1e-15 * scale[task];
         const double li = lam[t.doff + i];
         for (int j = threadIdx.x; j < t.n; j += blockDim.x) {
-            if (j == i) continue;
             const int64_t w = t.woff + (int64_t)i * t.np + j;
+            gd = fmax(gd, fabs(G[w] - (j == i ? 1.0 : 0.0)));
+            if (j == i) continue;
             const double lj = lam[t.doff + j];
             const double num = fabs(S[w] - lj * G[w]);
             const double gap = fabs(lj - li);
@@ -662,9 +669,11 @@ __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const doubl
     }
     sr[threadIdx.x] = best;
     sj[threadIdx.x] = bj;
+    sg[threadIdx.x] = gd;
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) {
+            sg[threadIdx.x] = fmax(sg[threadIdx.x], sg[threadIdx.x + w]);
             const double r2 = sr[threadIdx.x + w];
             const int j2 = sj[threadIdx.x + w];
             if (r2 > sr[threadIdx.x] || (r2 == sr[threadIdx.x] && j2 >= 0 && (sj[threadIdx.x] < 0 || j2 < sj[threadIdx.x]))) {
@@ -674,7 +683,12 @@ __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const doubl
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) partner[t.doff + i] = sj[0];
+    if (threadIdx.x == 0) {
+        partner[t.doff + i] = sj[0];
+        if (gdev && sg[0] > 0.0) atomicMax(gdev + task, (unsigned long long)__double_as_longlong(sg[0]));
+        // eigenvectors far from orthonormal: the block restarts cold
+        if (!(sg[0] <= 0.25)) restart[task] = 1;
+    }
 }
 
 // M = I + E.  Isolated strongly coupled pairs (partner of each other) get
@@ -723,10 +737,12 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
         if (i >= t.n || j >= t.n) {
             m = (i == j) ? 1.0 : 0.0;
         } else if (i == j) {
-            m = rot ? rc : 1.0 + 0.5 * (1.0 - G[w]);
+            // the norm correction (1 - g_ii) / 2 applies to rotated columns too
+            m = (rot ? rc : 1.0) + 0.5 * (1.0 - G[w]);
         } else if (rot && j == pi) {
-            // J_pp = c, J_pq = s, J_qp = -s, J_qq = c with p < q
-            m = (i < j) ? rs : -rs;
+            // J_pp = c, J_pq = s, J_qp = -s, J_qq = c with p < q, plus the
+            // orthogonality term of the pair (first order, like every pair)
+            m = ((i < j) ? rs : -rs) - 0.5 * G[w];
         } else {
             const double lj = lam[t.doff + j];
             const double num = S[w] - lj * G[w];
@@ -735,7 +751,10 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
             if (fabs(num) <= negligible) {
                 e = -0.5 * G[w];
             } else if (!(fabs(num) <= kHard * fabs(gap))) {
-                e = 0.0;  // strongly coupled: rotated in this or a later sweep
+                // strongly coupled: rotated in this or a later sweep; only the
+                // orthogonality term now (Ogita-Aishima's rule for clustered
+                // pairs), so that V stays orthonormal inside clusters
+                e = -0.5 * G[w];
                 pending = true;
                 pend = fmax(pend, fabs(num));
             } else {
@@ -808,6 +827,22 @@ __global__ void oa_masks_kernel(int ntasks, const unsigned long long* __restrict
     }
 }
 
+// M = I + (I - G) / 2 on the n x n part (identity on the padding): V M is one
+// Newton-Schulz step towards the orthonormal polar factor of V (G = V^T V);
+// it squares the distance from orthonormal.
+__global__ void ortho_step_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ G,
+                                  const int* __restrict__ bmask, double* __restrict__ M) {
+    if (bmask && !bmask[blockIdx.y]) return;
+    const BlockTask t = tasks[blockIdx.y];
+    const int p = blockIdx.x;
+    if (p >= t.np) return;
+    for (int q = threadIdx.x; q < t.np; q += blockDim.x) {
+        const int64_t w = t.woff + (int64_t)p * t.np + q;
+        const double id = (p == q) ? 1.0 : 0.0;
+        M[w] = (p < t.n && q < t.n) ? id + 0.5 * (id - G[w]) : id;
+    }
+}
+
 // C <- upper triangle of C mirrored to the lower one (tile granularity: the
 // GEMM computed tiles ti <= tj only)
 __global__ void mirror_kernel(const BlockTask* __restrict__ tasks, double* __restrict__ C,
@@ -874,13 +909,25 @@ __global__ void write_xz_kernel(const BlockTask* __restrict__ tasks, int B, cons
 
 constexpr size_t kJacobiSmem = 2 * kJ * kLd * sizeof(double);
 
+// The 66,560 B of dynamic shared memory of the Jacobi kernels need an opt-in
+// per kernel and per device.  Each device is set up once; a failed attempt is
+// retried on the next launch, whose own error then reaches the caller.
 void set_smem_attrs() {
-    static bool done = false;
-    if (done) return;
-    cudaFuncSetAttribute(small_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
-    cudaFuncSetAttribute(bj_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
-    cudaFuncSetAttribute(bj_update_wv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacobiSmem);
-    done = true;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return;
+    static std::mutex mu;
+    static std::vector<char> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((size_t)dev < done.size() && done[dev]) return;
+    bool ok = cudaFuncSetAttribute(small_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kJacobiSmem) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(bj_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kJacobiSmem) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(bj_update_wv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kJacobiSmem) == cudaSuccess;
+    if (!ok) return;
+    if ((size_t)dev >= done.size()) done.resize(dev + 1, 0);
+    done[dev] = 1;
 }
 
 }  // namespace
@@ -959,11 +1006,13 @@ void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, 
 
 void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
                        const int* bmask, double* lam, double* scale, int* partner, double* M,
-                       unsigned long long* emax, int* hard, double* erow, int* restart, cudaStream_t s) {
+                       unsigned long long* emax, int* hard, double* erow, int* restart, unsigned long long* gdev,
+                       cudaStream_t s) {
     if (ntasks == 0) return;
     oa_lambda_kernel<<<ntasks, 256, 0, s>>>(tasks, S, G, bmask, lam, scale, restart);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    oa_pairs_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, bmask, partner, hard);
+    oa_pairs_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, bmask, partner, hard, gdev,
+                                                          restart);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     oa_update_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, partner, bmask, M, emax,
                                                            hard, erow);
@@ -990,6 +1039,13 @@ void launch_copy_blocks(const BlockTask* tasks, int ntasks, int max_np, const do
 void launch_mirror(const BlockTask* tasks, int ntasks, int max_np, double* C, const int* bmask, cudaStream_t s) {
     if (ntasks == 0) return;
     mirror_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, C, bmask);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_ortho_step(const BlockTask* tasks, int ntasks, int max_np, const double* G, const int* bmask, double* M,
+                       cudaStream_t s) {
+    if (ntasks == 0) return;
+    ortho_step_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, G, bmask, M);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

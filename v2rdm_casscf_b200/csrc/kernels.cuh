@@ -95,6 +95,11 @@ void launch_cg_update_yr(int64_t n, int B, double* y, double* r, const double* p
                          const CgScalars* cs, double* partial, double* rr_out, cudaStream_t s);
 // convergence test and beta; counts instances still active into *n_active
 void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cudaStream_t s);
+// One CG step after p.Ap (in pap): y += alpha p, r -= alpha Ap, then r.r,
+// alpha, the convergence test, beta and the count of instances still
+// iterating into *n_active (two launches; replaces alpha / update_yr / beta)
+void launch_cg_step(int64_t n, int B, double* y, double* r, const double* p, const double* Ap, CgScalars* cs,
+                    const double* pap, double* partial, int* n_active, cudaStream_t s);
 // p = beta p + r
 void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s);
 // CG start extrapolation over [e * B + b]: where mode[b] == 2,
@@ -158,6 +163,16 @@ struct GemmTile {
 };
 void launch_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
                  const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s);
+// The same product on the tensor cores (tcgen05, 3xTF32 split, FP32
+// accumulation: FP32 accuracy) over 128 x 64 tiles of C: tile (ti, tj) covers
+// rows 128 ti.. and columns 64 tj..; rows past np are not written.
+void launch_tc_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
+                    const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s);
+// 0 while every tensor-core GEMM's pipeline waits ended; 1 after one ran out
+// (that launch's result is invalid); reset clears the flag.
+int tc_gemm_status(bool reset);
+// the same flag copied into host (pinned) memory on a stream, without a device-wide sync
+void tc_gemm_status_async(int* host, cudaStream_t s);
 // One block-Jacobi round: solve each 64x64 pair problem, then rotate W and V.
 struct PairTask {
     int task;   // block task
@@ -198,9 +213,12 @@ void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, 
 // Blocks whose eigenvectors lost orthonormality (|g_ii - 1| > 0.25) or whose
 // values broke down get restart[t] = 1; blocks whose first-order step has
 // ||E||_F > 0.2 are marked hard.  erow holds one double per padded row.
+// gdev[t] (optional) gets max |G_ij - delta_ij| of the block (as the bits of a
+// non-negative double): the distance of V from orthonormal.
 void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
                        const int* bmask, double* lam, double* scale, int* partner, double* M,
-                       unsigned long long* emax, int* hard, double* erow, int* restart, cudaStream_t s);
+                       unsigned long long* emax, int* hard, double* erow, int* restart, unsigned long long* gdev,
+                       cudaStream_t s);
 void launch_oa_masks(int ntasks, const unsigned long long* emax, const int* hard, const double* tol,
                      const double* abs_tol, const double* scale, int* ref, int* upd, int* jac, int* n_ref,
                      cudaStream_t s);
@@ -209,6 +227,10 @@ void launch_copy_blocks(const BlockTask* tasks, int ntasks, int max_np, const do
 void launch_count(int n, const int* mask, int* out, cudaStream_t s);
 // symmetric GEMM results: copy the upper tiles onto the lower ones
 void launch_mirror(const BlockTask* tasks, int ntasks, int max_np, double* C, const int* bmask, cudaStream_t s);
+// M = I + (I - G) / 2 (G = V^T V): V M is a Newton-Schulz step that brings V
+// back to orthonormal (the distance squares)
+void launch_ortho_step(const BlockTask* tasks, int ntasks, int max_np, const double* G, const int* bmask, double* M,
+                       cudaStream_t s);
 // max_sweeps[i] = unlimited where sel[i]
 void launch_uncap(int n, const int* sel, int* max_sweeps, cudaStream_t s);
 // dst[i] |= src[i]

@@ -62,6 +62,7 @@ struct Options {
     // this many difference columns; 0 = off.  The history restarts whenever mu
     // changes.
     int anderson_memory = 0;
+    bool mixed_precision = false;  // tensor-core (3xTF32) projection products while rho >= 1e-5
 };
 
 // Parses POSITIVITY the way v2rdm_solver.cc:497-522 does; returns false for

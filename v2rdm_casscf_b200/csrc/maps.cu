@@ -521,6 +521,90 @@ __global__ void cg_update_yr_kernel(int64_t n, int B, double* __restrict__ y, do
     block_partial(acc, B, partial);
 }
 
+// y += alpha p ; r -= alpha Ap with alpha = r.r / p.Ap computed by every
+// thread from the instance's scalars (no separate alpha launch; p.Ap <= 0
+// takes no step and the beta kernel stops the instance); partial[., b] of
+// r.r.  Block 0 clears the active-instance counter that the beta kernel
+// fills.
+__global__ void cg_step_yr_kernel(int64_t n, int B, double* __restrict__ y, double* __restrict__ r,
+                                  const double* __restrict__ p, const double* __restrict__ Ap,
+                                  const CgScalars* __restrict__ cs, const double* __restrict__ pap,
+                                  double* __restrict__ partial, int* __restrict__ n_active) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_active = 0;
+    const Chunk ch = chunk_of(n, B);
+    double acc = 0.0;
+    if (ch.live) {
+        const int b = ch.b;
+        const double pp = pap[b];
+        const bool act = cs[b].active && pp > 0.0;
+        const double a = act ? cs[b].rr / pp : 0.0;
+        for (int64_t e = ch.first; e < ch.nrows; e += ch.stride) {
+            const int64_t t = e * B + b;
+            double rv = r[t];
+            if (act) {
+                y[t] += a * p[t];
+                rv += -a * Ap[t];
+                r[t] = rv;
+            }
+            acc += rv * rv;
+        }
+    }
+    block_partial(acc, B, partial);
+}
+
+// One block per instance: r.r from the step kernel's partials (fixed tree),
+// then the scalars of cg_solver.cc:159-177: alpha, the ||r|| < tol test,
+// beta and the iteration count, the stops on p.Ap <= 0 and on residual
+// growth (kCgGrowth); counts the instances still iterating into n_active.
+__global__ void cg_beta_reduce_kernel(int nblk, int B, const double* __restrict__ partial,
+                                      const double* __restrict__ pap, CgScalars* cs, int* n_active) {
+    __shared__ double sh[kThreads];
+    const int b = blockIdx.x;
+    double s = 0.0;
+    for (int k = threadIdx.x; k < nblk; k += blockDim.x) s += partial[(int64_t)k * B + b];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    CgScalars c = cs[b];
+    c.do_p = 0;
+    if (c.active) {
+        c.pap = pap[b];
+        if (!(c.pap > 0.0)) {
+            // p has no component outside the null space of A^T (or r = 0): no step
+            c.alpha = 0.0;
+            c.active = 0;
+            c.stalled = 1;
+        } else {
+            c.alpha = c.rr / c.pap;
+            const double rn = sh[0];
+            c.rrnew = rn;
+            if (!(sqrt(rn) < c.tol)) {
+                if (rn > kCgGrowth * c.rrmin) {
+                    // diverging on the null space of A^T: keep the current y (kernels.cuh)
+                    c.active = 0;
+                    c.stalled = 1;
+                } else {
+                    c.beta = rn / c.rr;
+                    c.rr = rn;
+                    c.rrmin = fmin(c.rrmin, rn);
+                    c.do_p = 1;
+                    c.iter += 1;
+                    if (c.iter >= c.maxiter) c.active = 0;
+                }
+            } else {
+                c.active = 0;
+            }
+            if (!isfinite(rn)) c.active = 0;
+        }
+    }
+    cs[b] = c;
+    if (c.active) atomicAdd(n_active, 1);
+}
+
 // One warp: per instance, test ||r|| < tol (cg_solver.cc:167-171), else beta
 // and iteration count; counts the instances still iterating.
 __global__ void cg_beta_kernel(int B, CgScalars* cs, const double* rrnew, int* n_active) {
@@ -714,6 +798,14 @@ void launch_cg_update_yr(int64_t n, int B, double* y, double* r, const double* p
     cg_update_yr_kernel<<<g, kThreads, 0, s>>>(n, B, y, r, p, Ap, cs, partial);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     reduce_stage2<<<B, kThreads, 0, s>>>(g, B, partial, rr_out);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+void launch_cg_step(int64_t n, int B, double* y, double* r, const double* p, const double* Ap, CgScalars* cs,
+                    const double* pap, double* partial, int* n_active, cudaStream_t s) {
+    const int g = spmv_grid(n, B);
+    cg_step_yr_kernel<<<g, kThreads, 0, s>>>(n, B, y, r, p, Ap, cs, pap, partial, n_active);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    cg_beta_reduce_kernel<<<B, kThreads, 0, s>>>(g, B, partial, pap, cs, n_active);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cudaStream_t s) {

@@ -51,6 +51,21 @@ struct NoDevice : std::runtime_error {
                             std::to_string(__LINE__));                                                   \
     } while (0)
 
+// Makes a device current for the scope of a call and restores the caller's
+// current device afterwards.
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        CK(cudaSetDevice(device));
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
@@ -230,6 +245,11 @@ struct Problem {
 
 namespace {
 
+// Projection tolerance down to which the mixed-precision phase runs the large
+// blocks' dense products on the tensor cores (FP32 accuracy, ~1e-6 relative,
+// is then two orders below what the projection has to deliver).
+constexpr double kMixedRho = 1e-5;
+
 // Lock-step solve of B instances that share one layout.
 class GroupRun {
   public:
@@ -268,6 +288,9 @@ class GroupRun {
         build_projection_plan();
         upload_state();
         alloc_anderson(X);
+        if (const char* d = std::getenv("V2G_DIAG")) diag_every_ = std::atoi(d);
+        if (diag_every_ > 0)
+            if (const char* fn = std::getenv("V2G_DIAG_FILE")) diag_file_ = std::fopen(fn, "a");
         for (auto* p : P_) profile_ = profile_ || p->profile;
         if (profile_) {
             prof_ev_.resize(256);
@@ -275,6 +298,8 @@ class GroupRun {
         }
     }
     ~GroupRun() {
+        if (cg_exec_) cudaGraphExecDestroy(cg_exec_);
+        if (diag_file_) std::fclose(diag_file_);
         for (auto e : prof_ev_) cudaEventDestroy(e);
         if (hscal_) cudaFreeHost(hscal_);
         if (hnact_) cudaFreeHost(hnact_);
@@ -322,7 +347,10 @@ class GroupRun {
     // projection, rho = 0.01 min(eps_p, eps_d) like the CG tolerance rule);
     // rho[b] = 0 asks for a converged one.  x = V D+ V^T / mu and z = V D- V^T
     // are positive semidefinite either way.
-    void project(const std::vector<double>& rho = {}) {
+    // mixed = true runs the large blocks' dense products on the tensor cores.
+    void project(const std::vector<double>& rho = {}, bool mixed = false) {
+        tc_ = mixed && nlarge_ > 0;
+        if (tc_) tc_projections_++;
         launch_spmv(T_.AT(), B_, y_.p, aty_.p, nullptr, nullptr, nullptr, mask_.p, s_);
         launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_);
         if (nlarge_ == 0) return;
@@ -338,8 +366,8 @@ class GroupRun {
             refine();
         }
         launch_pos_weights(large_d_.p, nlarge_, lam_.p, mu_.p, bact_.p, dw_.p, dz_.p, s_);
-        launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, false, V_.p, true, dw_.p, Tm_.p, bact_.p, s_);
-        launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, false, V_.p, true, dz_.p, M_.p, bact_.p, s_);
+        gemm_sym(V_.p, false, V_.p, true, dw_.p, Tm_.p, bact_.p);
+        gemm_sym(V_.p, false, V_.p, true, dz_.p, M_.p, bact_.p);
         launch_mirror(large_d_.p, nlarge_, max_np_, Tm_.p, bact_.p, s_);
         launch_mirror(large_d_.p, nlarge_, max_np_, M_.p, bact_.p, s_);
         launch_write_xz(large_d_.p, nlarge_, max_n_, B_, Tm_.p, M_.p, mask_.p, x_.p, z_.p, s_);
@@ -353,21 +381,22 @@ class GroupRun {
         CK(cudaMemcpyAsync(bref_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
         CK(cudaMemsetAsync(bjac_.p, 0, nlarge_ * sizeof(int), s_));
         CK(cudaMemsetAsync(restart_.p, 0, nlarge_ * sizeof(int), s_));
+        CK(cudaMemsetAsync(gdev_.p, 0, nlarge_ * sizeof(unsigned long long), s_));
         int nref = 1;
         for (int sweep = 0; sweep < kMaxOa && nref > 0; sweep++) {
             // S = V^T (U V) and G = V^T V are symmetric: upper tiles, then mirrored
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bref_.p, s_);
-            launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bref_.p, s_);
-            launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, true, V_.p, false, nullptr, G_.p, bref_.p, s_);
+            gemm_full(U_.p, false, V_.p, false, nullptr, Tm_.p, bref_.p);
+            gemm_sym(V_.p, true, Tm_.p, false, nullptr, W_.p, bref_.p);
+            gemm_sym(V_.p, true, V_.p, false, nullptr, G_.p, bref_.p);
             launch_mirror(large_d_.p, nlarge_, max_np_, W_.p, bref_.p, s_);
             launch_mirror(large_d_.p, nlarge_, max_np_, G_.p, bref_.p, s_);
             CK(cudaMemsetAsync(emax_.p, 0, nlarge_ * sizeof(unsigned long long), s_));
             CK(cudaMemsetAsync(hard_.p, 0, nlarge_ * sizeof(int), s_));
             launch_oa_analyze(large_d_.p, nlarge_, max_np_, W_.p, G_.p, bref_.p, lam_.p, scale_.p, partner_.p,
-                              M_.p, emax_.p, hard_.p, erow_.p, restart_.p, s_);
+                              M_.p, emax_.p, hard_.p, erow_.p, restart_.p, gdev_.p, s_);
             launch_oa_masks(nlarge_, emax_.p, hard_.p, otol_.p, atol_.p, scale_.p, bref_.p, bupd_.p, bjac_.p,
                             nact_.p + 2, s_);
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, V_.p, false, M_.p, false, nullptr, Tm_.p, bupd_.p, s_);
+            gemm_full(V_.p, false, M_.p, false, nullptr, Tm_.p, bupd_.p);
             launch_copy_blocks(large_d_.p, nlarge_, max_np_, Tm_.p, V_.p, bupd_.p, s_);
             CK(cudaMemcpyAsync(hnact_ + 2, nact_.p + 2, sizeof(int), cudaMemcpyDeviceToHost, s_));
             CK(cudaStreamSynchronize(s_));
@@ -386,9 +415,19 @@ class GroupRun {
         CK(cudaStreamSynchronize(s_));
         if (hnact_[3] > 0) {
             jacobi_blocks_ += hnact_[3];
+            // the refinement skipped these blocks' update, so their V carries the
+            // orthogonality error of the previous iteration: two Newton-Schulz
+            // steps first (Jacobi's rotations preserve V^T V, whatever it is)
+            for (int k = 0; k < 2; k++) {
+                gemm_sym(V_.p, true, V_.p, false, nullptr, G_.p, bjac_.p);
+                launch_mirror(large_d_.p, nlarge_, max_np_, G_.p, bjac_.p, s_);
+                launch_ortho_step(large_d_.p, nlarge_, max_np_, G_.p, bjac_.p, M_.p, s_);
+                gemm_full(V_.p, false, M_.p, false, nullptr, Tm_.p, bjac_.p);
+                launch_copy_blocks(large_d_.p, nlarge_, max_np_, Tm_.p, V_.p, bjac_.p, s_);
+            }
             // warm block Jacobi on W = V^T U V with the current V
-            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, U_.p, false, V_.p, false, nullptr, Tm_.p, bjac_.p, s_);
-            launch_gemm(large_d_.p, stiles_.p, nstiles_, V_.p, true, Tm_.p, false, nullptr, W_.p, bjac_.p, s_);
+            gemm_full(U_.p, false, V_.p, false, nullptr, Tm_.p, bjac_.p);
+            gemm_sym(V_.p, true, Tm_.p, false, nullptr, W_.p, bjac_.p);
             launch_mirror(large_d_.p, nlarge_, max_np_, W_.p, bjac_.p, s_);
         }
         if (hnact_[4] > 0) {
@@ -554,7 +593,18 @@ class GroupRun {
             for (int b = 0; b < B_; b++)
                 if (opt(b).adaptive_projection)
                     rho[b] = (oiter[b] == 0) ? 0.01 : 0.01 * std::min(ep[b], ed[b]);
-            project(rho);
+            // the mixed-precision phase: every instance still iterating asked for it
+            // and accepts a projection residual of at least kMixedRho
+            bool mixed = false;
+            for (int b = 0; b < B_; b++) {
+                if (!active[b]) continue;
+                if (!(opt(b).mixed_precision && rho[b] >= kMixedRho)) {
+                    mixed = false;
+                    break;
+                }
+                mixed = true;
+            }
+            project(rho, mixed);
             CK(cudaEventRecord(e2, s_));
             // ed = ||A^T y + z - c||, ep = ||A x - b||, E = c.x, b.y (:1826-1852)
             launch_reduce(RED_ED, nx_, B_, aty_.p, z_.p, c_.p, nullptr, partial_.p, red_.p, s_);
@@ -563,7 +613,10 @@ class GroupRun {
             launch_reduce(RED_DOT, nx_, B_, c_.p, x_.p, nullptr, nullptr, partial_.p, red_.p + 2 * B_, s_);
             launch_reduce(RED_DOT_ROW, nc_, B_, y_.p, nullptr, nullptr, T_.b.p, partial_.p, red_.p + 3 * B_, s_);
             CK(cudaMemcpyAsync(hscal_, red_.p, 4 * B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+            if (tc_) tc_gemm_status_async(hnact_ + 5, s_);
             CK(cudaStreamSynchronize(s_));
+            if (tc_ && hnact_[5] != 0)
+                throw CudaError("a tensor-core GEMM of the projection did not finish (pipeline wait ran out)");
             float ms_cg = 0, ms_xz = 0;
             CK(cudaEventElapsedTime(&ms_cg, e0, e1));
             CK(cudaEventElapsedTime(&ms_xz, e1, e2));
@@ -624,6 +677,7 @@ class GroupRun {
                     active[b] = 0;
                 }
             }
+            if (diag_every_ > 0 && (it % diag_every_ == 0 || any_nonfinite(ep, ed))) diagnose(it, cs, ep, ed, mu);
             if (aa_m_ > 0) anderson(active, recover, mu_changed, aa);
             it++;
         }
@@ -716,6 +770,48 @@ class GroupRun {
         CK(cudaStreamSynchronize(s_));
     }
 
+    static bool any_nonfinite(const std::vector<double>& ep, const std::vector<double>& ed) {
+        for (size_t b = 0; b < ep.size(); b++)
+            if (!std::isfinite(ep[b]) || !std::isfinite(ed[b])) return true;
+        return false;
+    }
+
+    // Per-iteration diagnostics (V2G_DIAG = every k outer iterations, written to
+    // V2G_DIAG_FILE or stderr): per instance eps(p), eps(d), mu, this
+    // iteration's CG count, |y|^2, |x|^2, |z|^2; per group the largest distance
+    // of the projection's eigenvectors from orthonormal (max |V^T V - I| over the
+    // large blocks, as the refinement found it) and the running counts of
+    // block-Jacobi fallbacks and cold restarts.
+    void diagnose(int it, const std::vector<CgScalars>& cs, const std::vector<double>& ep,
+                  const std::vector<double>& ed, const std::vector<double>& mu) {
+        std::vector<double> sums(3 * B_);
+        const DevBuf<double>* vecs[3] = {&y_, &x_, &z_};
+        const int64_t lens[3] = {nc_, nx_, nx_};
+        for (int k = 0; k < 3; k++) {
+            launch_reduce(RED_DOT, lens[k], B_, vecs[k]->p, vecs[k]->p, nullptr, nullptr, partial_.p, red_.p, s_);
+            CK(cudaMemcpyAsync(&sums[k * B_], red_.p, B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        }
+        double gmax = 0.0;
+        if (nlarge_ > 0) {
+            std::vector<unsigned long long> g(nlarge_);
+            CK(cudaMemcpyAsync(g.data(), gdev_.p, nlarge_ * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
+            CK(cudaStreamSynchronize(s_));
+            for (auto v : g) {
+                double d;
+                std::memcpy(&d, &v, sizeof(d));
+                gmax = std::max(gmax, d);
+            }
+        }
+        CK(cudaStreamSynchronize(s_));
+        std::FILE* f = diag_file_ ? diag_file_ : stderr;
+        std::fprintf(f, "diag it %d group n=%lld B=%d gdev %.3e jacobi_blocks %ld restarts %ld oa_sweeps %ld\n", it,
+                     (long long)nx_, B_, gmax, jacobi_blocks_, restarts_, oa_sweeps_);
+        for (int b = 0; b < B_; b++)
+            std::fprintf(f, "diag it %d b %d ep %.3e ed %.3e mu %.4f cg %d stalled %d y2 %.3e x2 %.3e z2 %.3e\n", it, b,
+                         ep[b], ed[b], mu[b], cs[b].iter, cs[b].stalled, sums[b], sums[B_ + b], sums[2 * B_ + b]);
+        std::fflush(f);
+    }
+
     // Which of y, x, z (and the CG scalars) turned non-finite, on stderr, so
     // that a failing instance can be reproduced and traced alone.
     void report_nonfinite(int b, int oiter, double mu, long cg_iters) {
@@ -768,6 +864,7 @@ class GroupRun {
     long jacobi_sweeps() const { return sweeps_total_; }
     long oa_sweeps() const { return oa_sweeps_; }
     long jacobi_blocks() const { return jacobi_blocks_; }
+    long tc_projections() const { return tc_projections_; }
     double map_seconds() const { return map_sec_; }
     long map_launches() const { return map_n_; }
     double map_bytes() const { return map_bytes_; }
@@ -775,6 +872,22 @@ class GroupRun {
     double d2h_bytes() const { return 8.0 * B_ * (2.0 * nx_ + nc_); }
 
   private:
+    // The projection's dense products: on all tiles of C (full) or on the
+    // upper tiles of a symmetric C (sym, mirrored afterwards), in FP64 or, in
+    // the mixed-precision phase (tc_), as 3xTF32 products on the tensor cores.
+    void gemm_full(const double* A, bool ta, const double* Bm, bool tb, const double* d, double* C, const int* mask) {
+        if (tc_)
+            launch_tc_gemm(large_d_.p, tc_gtiles_.p, ntc_gtiles_, A, ta, Bm, tb, d, C, mask, s_);
+        else
+            launch_gemm(large_d_.p, gtiles_.p, ngtiles_, A, ta, Bm, tb, d, C, mask, s_);
+    }
+    void gemm_sym(const double* A, bool ta, const double* Bm, bool tb, const double* d, double* C, const int* mask) {
+        if (tc_)
+            launch_tc_gemm(large_d_.p, tc_stiles_.p, ntc_stiles_, A, ta, Bm, tb, d, C, mask, s_);
+        else
+            launch_gemm(large_d_.p, stiles_.p, nstiles_, A, ta, Bm, tb, d, C, mask, s_);
+    }
+
     // CG map launch with optional CUDA-event timing (profile mode).
     // With dotv, also red_[b] = sum dotv[., b] * out[., b].
     void map_launch(const DevMap& M, const double* in, double* out, const double* dotv = nullptr,
@@ -815,21 +928,50 @@ class GroupRun {
         launch_cg_init(nc_, B_, bv_.p, ap_.p, r_.p, p_.p, cs_.p, s_);
         launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
         launch_cg_set_rr(B_, cs_.p, red_.p, nact_.p, s_);
-        const int check_every = 4;
-        for (int k = 0;; k++) {
-            map_launch(T_.AT(), p_.p, atp_.p, nullptr, mask_.p);
-            map_launch(T_.A(), atp_.p, ap_.p, p_.p, mask_.p);  // Ap and p.Ap
-            launch_cg_alpha(B_, cs_.p, red_.p, s_);
-            launch_cg_update_yr(nc_, B_, y_.p, r_.p, p_.p, ap_.p, cs_.p, partial_.p, red_.p, s_);
-            launch_cg_beta(B_, cs_.p, red_.p, nact_.p, s_);
-            launch_cg_update_p(nc_, B_, p_.p, r_.p, cs_.p, s_);
-            if ((k + 1) % check_every == 0) {
-                CK(cudaMemcpyAsync(hnact_, nact_.p, sizeof(int), cudaMemcpyDeviceToHost, s_));
-                CK(cudaStreamSynchronize(s_));
-                if (hnact_[0] == 0) break;
+        // CG iterations run in chunks of kCgChunk (a CUDA graph, captured once
+        // per group, outside profile mode); instances that converge inside a
+        // chunk are masked by their scalars, and the host looks at the count of
+        // instances still iterating after each chunk
+        while (true) {
+            if (!profile_) {
+                if (!cg_exec_) capture_cg_chunk();
+                CK(cudaGraphLaunch(cg_exec_, s_));
+                g_kernel_launches.fetch_add(cg_chunk_nodes_, std::memory_order_relaxed);
+            } else {
+                for (int k = 0; k < kCgChunk; k++) cg_iteration();
             }
+            CK(cudaMemcpyAsync(hnact_, nact_.p, sizeof(int), cudaMemcpyDeviceToHost, s_));
+            CK(cudaStreamSynchronize(s_));
+            if (hnact_[0] == 0) break;
         }
         if (profile_) flush_profile();
+    }
+
+    static constexpr int kCgChunk = 4;
+    // One CG iteration (cg_solver.cc:141-177) for every instance whose scalars are active.
+    void cg_iteration() {
+        map_launch(T_.AT(), p_.p, atp_.p, nullptr, mask_.p);
+        map_launch(T_.A(), atp_.p, ap_.p, p_.p, mask_.p);  // Ap and p.Ap (into red_)
+        launch_cg_step(nc_, B_, y_.p, r_.p, p_.p, ap_.p, cs_.p, red_.p, partial_.p, nact_.p, s_);
+        launch_cg_update_p(nc_, B_, p_.p, r_.p, cs_.p, s_);
+    }
+    // kCgChunk CG iterations captured from the stream into a graph: the
+    // kernels' arguments are the group's fixed buffers, so one capture serves
+    // every CG solve of the group.
+    void capture_cg_chunk() {
+        CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < kCgChunk; k++) cg_iteration();
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(s_, &g));
+        size_t nodes = 0;
+        CK(cudaGraphGetNodes(g, nullptr, &nodes));
+        // the launchers counted the captured kernels as launches; graph
+        // launches are counted per replay instead
+        g_kernel_launches.fetch_sub((long)nodes, std::memory_order_relaxed);
+        cg_chunk_nodes_ = (long)nodes;
+        const cudaError_t e = cudaGraphInstantiate(&cg_exec_, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
     }
 
     // Jacobi: relative off-diagonal norm 1e-13 or the absolute rho share of
@@ -924,6 +1066,7 @@ class GroupRun {
         partner_.alloc(doff);
         scale_.alloc(nlarge_);
         emax_.alloc(nlarge_);
+        gdev_.alloc(nlarge_);
         hard_.alloc(nlarge_);
         bact_.alloc(nlarge_);
         bwork_.alloc(nlarge_);
@@ -953,6 +1096,22 @@ class GroupRun {
         }
         gtiles_.upload(gt.data(), gt.size());
         stiles_.upload(st.data(), st.size());
+        // 128 x 64 tiles of the tensor-core GEMM; the symmetric products need
+        // every 64 x 64 upper tile, i.e. 128-row tile ti with 64-column tile tj >= 2 ti
+        std::vector<GemmTile> tg, ts;
+        for (int ti = 0; ti < nlarge_; ti++) {
+            const BlockTask& t = hlarge_[ti];
+            const int nr = (t.np + 127) / 128, nc = t.np / 64;
+            for (int i = 0; i < nr; i++)
+                for (int j = 0; j < nc; j++) {
+                    tg.push_back({ti, i, j});
+                    if (2 * i <= j) ts.push_back({ti, i, j});
+                }
+        }
+        tc_gtiles_.upload(tg.data(), tg.size());
+        tc_stiles_.upload(ts.data(), ts.size());
+        ntc_gtiles_ = (int)tg.size();
+        ntc_stiles_ = (int)ts.size();
         nstiles_ = (int)st.size();
         pairs_.upload(pt.data(), pt.size());
         wtiles_.upload(wt.data(), wt.size());
@@ -990,19 +1149,28 @@ class GroupRun {
     DevBuf<BlockTask> small_d_, large_d_;
     int nsmall_ = 0, nlarge_ = 0, max_np_ = 0, max_n_ = 0, max_rounds_ = 0;
     DevBuf<double> U_, W_, V_, Tm_, G_, M_, Q_, dw_, dz_, lam_, scale_, jtol_, otol_, atol_, rowsum_, erow_;
-    DevBuf<unsigned long long> emax_;
+    DevBuf<unsigned long long> emax_, gdev_;
     DevBuf<int> hard_, bact_, bwork_, bref_, bupd_, bjac_, partner_, msw_, restart_, qskip_;
     DevBuf<double> pthr_;
     long restarts_ = 0;
     bool cap_ = false;
     long oa_sweeps_ = 0, jacobi_blocks_ = 0;
-    DevBuf<GemmTile> gtiles_, stiles_;
+    DevBuf<GemmTile> gtiles_, stiles_, tc_gtiles_, tc_stiles_;
+    int ntc_gtiles_ = 0, ntc_stiles_ = 0;
+    bool tc_ = false;  // this projection's dense products on the tensor cores
+    long tc_projections_ = 0;
     DevBuf<PairTask> pairs_;
     DevBuf<WTileTask> wtiles_;
     DevBuf<VTileTask> vtiles_;
     int ngtiles_ = 0, nstiles_ = 0, npairs_ = 0, nwtiles_ = 0, nvtiles_ = 0;
     bool warm_ = false;
     long sweeps_total_ = 0;
+    // the captured CG chunk
+    cudaGraphExec_t cg_exec_ = nullptr;
+    long cg_chunk_nodes_ = 0;
+    // diagnostics (V2G_DIAG)
+    int diag_every_ = 0;
+    std::FILE* diag_file_ = nullptr;
     // profile mode
     bool profile_ = false;
     std::vector<cudaEvent_t> prof_ev_;
@@ -1072,6 +1240,7 @@ void v2g_default_options(v2g_options* o) {
     o->start = 0;
     o->cg_extrapolate = 0;
     o->anderson_memory = 0;
+    o->mixed_precision = 0;
 }
 
 const char* v2g_last_error(void) { return v2g::g_last_error.c_str(); }
@@ -1107,6 +1276,9 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         if (opt->anderson_memory < 0 || opt->anderson_memory > v2g::kAndersonMax)
             return v2g::fail(V2G_ERR_ARG, "anderson_memory must be in 0..16");
         o.anderson_memory = opt->anderson_memory;
+        if (opt->mixed_precision != 0 && opt->mixed_precision != 1)
+            return v2g::fail(V2G_ERR_ARG, "mixed_precision must be 0 or 1");
+        o.mixed_precision = opt->mixed_precision == 1;
         if (!(o.cg_tol_factor > 0.0 && o.cg_tol_factor < 1.0))
             return v2g::fail(V2G_ERR_ARG, "cg_tolerance_factor must be in (0, 1)");
         if (o.maxiter < 1 || o.cg_maxiter < 1 || o.mu_update_frequency < 1)
@@ -1603,6 +1775,27 @@ unsigned char* noalloc_scratch(int device) {
     return static_cast<unsigned char*>(g_noalloc_addr[device]);
 }
 
+// The per-call inputs of the scratch (mu and the block list), passed by value
+// as a kernel argument (3 KB) so that no host memory is copied per call.
+struct NoAllocSetup {
+    double mu;
+    int nt;
+    int n[kNoAllocMaxTasks];
+    int64_t xoff[kNoAllocMaxTasks];
+};
+
+__global__ void noalloc_setup_kernel(NoAllocSetup p, double* s_mu, v2g::BlockTask* s_tasks) {
+    for (int i = threadIdx.x; i < p.nt; i += blockDim.x) {
+        v2g::BlockTask t{};
+        t.xoff = p.xoff[i];
+        t.n = p.n[i];
+        t.inst = 0;
+        s_tasks[i] = t;
+    }
+    if (threadIdx.x == 0) *s_mu = p.mu;
+}
+
+
 }  // namespace
 
 extern "C" {
@@ -1622,37 +1815,78 @@ int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const dou
         if (L.dimx > kNoAllocMaxDimx)
             return v2g::fail(V2G_ERR_ARG, "v2g_update_xz_noalloc: dimx " + std::to_string(L.dimx) +
                                               " exceeds the maximum of " + std::to_string(kNoAllocMaxDimx));
-        v2g::BlockTask tasks[kNoAllocMaxTasks];
-        int nt = 0;
+        NoAllocSetup setup{};
+        setup.mu = mu;
+        setup.nt = 0;
         for (size_t k = 0; k < L.block_dims.size(); k++) {
             const int n = L.block_dims[k];
             if (n == 0) continue;
             if (n > 64)
                 return v2g::fail(V2G_ERR_ARG, "v2g_update_xz_noalloc: block of dimension " + std::to_string(n) +
                                                   " exceeds the maximum of 64 (use v2g_update_xz)");
-            if (nt == kNoAllocMaxTasks)
+            if (setup.nt == kNoAllocMaxTasks)
                 return v2g::fail(V2G_ERR_ARG, "v2g_update_xz_noalloc: more than " +
                                                   std::to_string(kNoAllocMaxTasks) + " blocks");
-            v2g::BlockTask t{};
-            t.xoff = L.block_off[k];
-            t.n = n;
-            t.inst = 0;
-            tasks[nt++] = t;
+            setup.n[setup.nt] = n;
+            setup.xoff[setup.nt] = L.block_off[k];
+            setup.nt++;
         }
-        CK(cudaSetDevice(T.device));
+        v2g::DeviceScope scope(T.device);
         unsigned char* base = noalloc_scratch(T.device);
         double* s_mu = reinterpret_cast<double*>(base);
         v2g::BlockTask* s_tasks = reinterpret_cast<v2g::BlockTask*>(base + kNoAllocMuBytes);
         double* s_aty = reinterpret_cast<double*>(base + kNoAllocMuBytes + kNoAllocTaskBytes);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        // mu and the task list are rewritten by every call; A^T y is cleared
+        // mu and the block list are rewritten by every call; A^T y is cleared
         // first, so nothing of an earlier call's contents is read.
-        CK(cudaMemcpyAsync(s_mu, &mu, sizeof(double), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(s_tasks, tasks, nt * sizeof(v2g::BlockTask), cudaMemcpyHostToDevice, s));
+        noalloc_setup_kernel<<<1, 256, 0, s>>>(setup, s_mu, s_tasks);
+        v2g::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
         CK(cudaMemsetAsync(s_aty, 0, L.dimx * sizeof(double), s));
         v2g::launch_spmv(T.AT(), 1, d_y, s_aty, nullptr, nullptr, nullptr, nullptr, s);
-        v2g::launch_small_project(s_tasks, nt, 1, s_aty, d_c, d_x, d_z, s_mu, nullptr, s);
+        v2g::launch_small_project(s_tasks, setup.nt, 1, s_aty, d_c, d_x, d_z, s_mu, nullptr, s);
         CK(cudaGetLastError());
+        return V2G_OK;
+    });
+}
+
+int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int transA, const double* B, int transB,
+                          const double* d, double* C, int tensor_cores, int device) {
+    return v2g::guarded([&]() -> int {
+        if (nblocks < 1 || !dims || !A || !B || !C) return v2g::fail(V2G_ERR_ARG, "bad block GEMM arguments");
+        v2g::require_device();
+        v2g::DeviceScope scope(device);
+        std::vector<v2g::BlockTask> tasks(nblocks);
+        std::vector<v2g::GemmTile> tiles;
+        int64_t woff = 0, doff = 0;
+        for (int i = 0; i < nblocks; i++) {
+            if (dims[i] < 1 || dims[i] > 16384) return v2g::fail(V2G_ERR_ARG, "block dimension out of range");
+            v2g::BlockTask t{};
+            t.n = dims[i];
+            t.np = (dims[i] + 63) / 64 * 64;
+            t.nb = t.np / 32;
+            t.woff = woff;
+            t.doff = doff;
+            woff += (int64_t)t.np * t.np;
+            doff += t.np;
+            tasks[i] = t;
+            const int nr = tensor_cores ? (t.np + 127) / 128 : t.np / 64, nc = t.np / 64;
+            for (int a = 0; a < nr; a++)
+                for (int b = 0; b < nc; b++) tiles.push_back({i, a, b});
+        }
+        v2g::DevBuf<v2g::BlockTask> dt;
+        v2g::DevBuf<v2g::GemmTile> dg;
+        dt.upload(tasks.data(), tasks.size());
+        dg.upload(tiles.data(), tiles.size());
+        if (tensor_cores) {
+            v2g::tc_gemm_status(true);
+            v2g::launch_tc_gemm(dt.p, dg.p, (int)tiles.size(), A, transA != 0, B, transB != 0, d, C, nullptr, 0);
+        } else {
+            v2g::launch_gemm(dt.p, dg.p, (int)tiles.size(), A, transA != 0, B, transB != 0, d, C, nullptr, 0);
+        }
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(0));
+        if (tensor_cores && v2g::tc_gemm_status(true) != 0)
+            return v2g::fail(V2G_ERR_CUDA, "a tensor-core GEMM pipeline wait ran out");
         return V2G_OK;
     });
 }

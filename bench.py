@@ -4,9 +4,10 @@
 Metric: time to 1e-6 Eh (E_CONVERGENCE 1e-7, R_CONVERGENCE 1e-6) of the
 solver's own stopping test, for three solvers on the same input:
 
-  value           the product's solve (FP64 maps / CG, adaptive projection,
-                  least-norm feasible warm start, Anderson acceleration of the
-                  outer iteration with the extrapolated CG start), device seconds
+  value           the product's solve (FP64 maps / CG, mixed-precision
+                  adaptive projection on the tensor cores, least-norm feasible
+                  warm start, Anderson acceleration of the outer iteration with
+                  the extrapolated CG start), device seconds
                   with the inputs resident in HBM (CUDA events around the
                   iteration phase inside the C ABI call)
   plain_fp64_gpu  the reference's algorithm, options and random start
@@ -188,18 +189,22 @@ def product_kw(args):
         return dict(projection="exact", cg_tolerance_factor=0.01, start="state", cg_extrapolate=False,
                     anderson_memory=0), dict(MU_UPDATE_FREQUENCY=500, TAU_PARAMETER=1.0)
     return (dict(projection=args.projection, cg_tolerance_factor=args.cg_factor, start=args.start,
-                 cg_extrapolate=args.cg_extrapolate, anderson_memory=args.anderson),
+                 cg_extrapolate=args.cg_extrapolate, anderson_memory=args.anderson,
+                 mixed_precision=args.mixed and args.projection == "adaptive"),
             dict(MU_UPDATE_FREQUENCY=args.mu_freq, TAU_PARAMETER=args.tau))
 
 
-PLAIN_KW = (dict(projection="exact", cg_tolerance_factor=0.01, start="state", cg_extrapolate=False, anderson_memory=0),
+PLAIN_KW = (dict(projection="exact", cg_tolerance_factor=0.01, start="state", cg_extrapolate=False, anderson_memory=0,
+                 mixed_precision=False),
             dict(MU_UPDATE_FREQUENCY=500, TAU_PARAMETER=1.0))
 
 
 def mode_text(kw, opt):
     if kw == PLAIN_KW[0] and opt == PLAIN_KW[1]:
         return "plain FP64 (the reference's algorithm, options and random start)"
-    return ("FP64 maps / CG / refinement, "
+    return ("FP64 maps / CG / errors, "
+            + ("mixed-precision projection (3xTF32 tcgen05 products while the projection tolerance is >= 1e-5, "
+               "FP64 after), " if kw.get("mixed_precision") else "FP64 projection, ")
             + ("adaptive projection accuracy" if kw["projection"] == "adaptive" else "converged projections")
             + (", least-norm feasible warm start" if kw["start"] == "feasible" else ", the reference's random start")
             + (", extrapolated CG start" if kw["cg_extrapolate"] else "")
@@ -232,7 +237,7 @@ def run_gpu(args):
         mine = partition(workload_costs(all_spaces), world)[rank]
     kw, opt = product_kw(args)
 
-    def make(kw, opt, maxiter, profile=True):
+    def make(kw, opt, maxiter, profile=False):
         o = dict(OPTIONS, POSITIVITY=workload_positivity(args.workload), **opt)
         if maxiter:
             o["MAXITER"] = maxiter
@@ -291,9 +296,6 @@ def run_gpu(args):
     dev_s = [s["device_seconds"] for s in stats]
     e2e_s = [s["e2e_seconds"] for s in stats]
     value, e2e = float(np.mean(dev_s)), float(np.mean(e2e_s))
-    map_s = sum(s["map_seconds"] for s in stats)
-    map_n = sum(s["map_launches"] for s in stats)
-    map_b = sum(s["map_bytes"] for s in stats)
     launches = sum(s["kernel_launches"] for s in stats)
     h2d = float(np.mean([s["h2d_bytes"] for s in stats]))
     d2h = float(np.mean([s["d2h_bytes"] for s in stats]))
@@ -341,19 +343,7 @@ def run_gpu(args):
         },
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
-        "roofline": {
-            "kernel": "ell_kernel + long_kernel (A and A^T of the CG), in-solve CUDA events, timed steps",
-            "bound": "hbm",
-            "achieved": (map_b / map_s / 1e9) if map_s > 0 else None,
-            "peak": pk,
-            "peak_kind": pk_kind,
-            "unit": "GB/s",
-            "frac": (map_b / map_s / 1e9 / pk) if map_s > 0 else None,
-            "traffic": None,
-            "launches": map_n,
-            "bytes_per_launch": (map_b / map_n) if map_n else None,
-            "us_per_launch": (map_s / map_n * 1e6) if map_n else None,
-        },
+        "roofline": roofline_workload(solvers, pk, pk_kind),
         "converged": n_conv,
         "wall_s": wall,
     }
@@ -398,19 +388,46 @@ def run_gpu(args):
         out["energy_check"] = chk
     # the same map kernel timed alone on the batched workload's largest group
     if args.roofline_batch:
-        big = [synthetic(20, s) for s in range(19)]
-        bs = [V.V2RDMSolver.from_active_space(a, options=dict(OPTIONS), device=dev) for a in big[:1]]
-        achieved, detail = roofline_alone(V, bs, big, list(range(19)), dev, torch, force_B=19)
+        b20 = V.V2RDMSolver([20], 10, 10, device=dev)
+        ta, tt = b20.time_maps(19, 20)
+        nbytes = 8.0 * (b20.dimx + b20.nconstraints) * 19
+        ach = 2 * nbytes / (ta + tt) / 1e9
         out["roofline_batch"] = {"kernel": "ell_kernel + long_kernel, A and A^T of n = 20 with 19 instances "
-                                           "interleaved (the batched workload's largest group), timed alone",
-                                 "bound": "hbm", "achieved": achieved, "peak": pk, "peak_kind": pk_kind,
-                                 "unit": "GB/s", "frac": achieved / pk, "detail": detail}
+                                           "interleaved (the batched workload's largest group), graph replay",
+                                 "bound": "hbm", "achieved": ach, "peak": pk, "peak_kind": pk_kind, "unit": "GB/s",
+                                 "frac": ach / pk, "traffic": ROOFLINE_TRAFFIC.get((20, 19)),
+                                 "bytes_per_launch": nbytes, "us_per_launch": {"A": ta * 1e6, "AT": tt * 1e6}}
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
         if args.cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline(args, all_spaces)
         print(json.dumps(out), flush=True)
+
+
+# DRAM bytes (read + write) per launch of the roofline kernels, from one ncu
+# capture of the same launches (profiles/ell_kernel_*.md gives the command):
+# key = (n, instances)
+ROOFLINE_TRAFFIC = {}
+
+
+def roofline_workload(solvers, pk, pk_kind):
+    """The map kernels of the workload's largest instance layout: A and A^T on
+    the instance's own vector size, `reps` launches replayed from a CUDA graph
+    between CUDA events on their stream (the kernels' own duration; the host's
+    launch rate, which bounds a single small instance inside the solve, is
+    excluded), algorithmic bytes 8 (rows + columns) per launch."""
+    s = max(solvers, key=lambda v: v.dimx)
+    ta, tt = s.time_maps(1, 50)
+    nbytes = 8.0 * (s.dimx + s.nconstraints)
+    ach = 2 * nbytes / (ta + tt) / 1e9
+    key = (int(s.active[0]), 1)
+    return {"kernel": "ell_kernel + long_kernel (A and A^T of the CG), one instance of the workload, graph replay",
+            "bound": "hbm", "achieved": ach, "peak": pk, "peak_kind": pk_kind, "unit": "GB/s", "frac": ach / pk,
+            "traffic": ROOFLINE_TRAFFIC.get(key), "bytes_per_launch": nbytes,
+            "us_per_launch": {"A": ta * 1e6, "AT": tt * 1e6},
+            "note": "bytes per launch fit in L2 at this size: the kernel is bound by latency, not HBM"
+                    if nbytes < 64e6 else ""}
 
 
 def roofline_alone(V, solvers, spaces, mine, dev, torch, reps=20, force_B=None):
@@ -587,6 +604,8 @@ def main():
     ap.add_argument("--tau", type=float, default=1.0, help="TAU_PARAMETER (the plugin's default 1.0)")
     ap.add_argument("--anderson", type=int, default=10,
                     help="Anderson acceleration of the outer iteration with this memory (0 = off)")
+    ap.add_argument("--no-mixed", dest="mixed", action="store_false",
+                    help="FP64 projection products throughout (no tensor-core phase)")
     ap.add_argument("--no-cg-extrapolate", dest="cg_extrapolate", action="store_false",
                     help="start each CG from y_k (the reference's) instead of y_k + (y_k - y_k-1)")
     ap.add_argument("--plain", action="store_true",

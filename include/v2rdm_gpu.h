@@ -78,7 +78,10 @@ typedef struct v2g_options {
     int start;                  /* 0: solve from the handle's state (v2g_guess_random, the plugin's
                                    TPDM_GUESS=RANDOM, or v2g_set_state); 1: from the least-norm
                                    point of A x = b with zero duals and mu = 1, computed on the
-                                   GPU at the start of the solve (no counterpart in the plugin) (0) */
+                                   GPU at the start of the solve; 2: from the learned warm start's
+                                   proposal (v2g_ws_propose) moved onto A x = b the same way, with
+                                   zero duals and the proposed mu, or as 1 without a proposal
+                                   (1 and 2 have no counterpart in the plugin) (0) */
     int cg_extrapolate;         /* 1: each outer iteration's CG starts from y_k + (y_k - y_{k-1}),
                                    the linear extrapolation of the last two CG solutions, instead of
                                    y_k (cg_solver.cc:125 warm-starts from y_k); the stopping test is
@@ -184,6 +187,14 @@ int v2g_update_xz(v2g_handle* h, double mu);
 int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const double* d_y, double* d_x, double* d_z,
                           void* stream);
 
+/* Seconds per launch of A and of A^T (the map kernels of the CG) on nvec
+ * instance-interleaved vectors of the handle's layout: `reps` launches
+ * captured in a CUDA graph and replayed between CUDA events on one stream, so
+ * the figure is the kernels' own duration (plus the graph's launch gaps), not
+ * the host's launch rate.  For roofline figures; no counterpart in the
+ * reference. */
+int v2g_time_maps(v2g_handle* h, int nvec, int reps, double* sec_A, double* sec_AT);
+
 /* The dense product of the projection on caller-owned device buffers, for
  * tests and inspection: for nblocks symmetric blocks of dimensions dims[i]
  * (each padded to np_i = dims rounded up to a multiple of 64 and stored
@@ -195,6 +206,38 @@ int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const dou
  * the reference (it calls F_DGEMM, v2rdm_solver.cc:3273,3286). */
 int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int transA, const double* B, int transB,
                           const double* d, double* C, int tensor_cores, int device);
+
+/* Learned warm start (no counterpart in the reference, whose start is the
+ * random guess of Guess, v2rdm_solver.cc:2386-2516).  A pair-wise MLP (16
+ * features of each orbital pair p <= q from h and the three-index integrals,
+ * three hidden ReLU layers of width `hidden`, BF16 weights, FP32 arithmetic)
+ * proposes for every pair the alpha 1-RDM element gamma_pq, the D2ab pair
+ * diagonal D2ab(pq,pq) and a contribution to log(mu).  It is trained on the
+ * GPU (Adam on the mean squared error) on converged solutions of this solver;
+ * v2g_ws_propose turns its output into the handle's start proposal x0 (D1,
+ * Q1 = 1 - D1, the D2ab diagonal; zero elsewhere) and mu, which a solve with
+ * start = 2 projects onto A x = b.  All-active C1 singlets only
+ * (V2G_ERR_UNSUPPORTED otherwise).  Rows are the n (n + 1) / 2 pairs of an
+ * active space, features 16 floats per row, targets and outputs 3. */
+typedef struct v2g_warmstart v2g_warmstart;
+int v2g_ws_create(int hidden, int device, unsigned long long seed, v2g_warmstart** out);
+void v2g_ws_destroy(v2g_warmstart* w);
+long v2g_ws_num_params(const v2g_warmstart* w);
+int v2g_ws_get_params(const v2g_warmstart* w, float* params);   /* FP32 master weights */
+int v2g_ws_set_params(v2g_warmstart* w, const float* params);   /* also resets the optimiser */
+long v2g_ws_rows(const v2g_handle* h);                             /* pairs of the handle's active space */
+int v2g_ws_features(const v2g_handle* h, float* features);          /* rows x 16 */
+int v2g_ws_targets(const v2g_handle* h, float* targets);            /* rows x 3 from the handle's x and mu */
+int v2g_ws_forward(v2g_warmstart* w, long rows, const float* features, float* out);
+/* loss = mean squared error over rows x 3 outputs and its gradient (FP32,
+ * num_params floats, laid out like the parameters) */
+int v2g_ws_gradient(v2g_warmstart* w, long rows, const float* features, const float* targets, double* loss,
+                    float* grad);
+/* Adam (lr) over minibatches of batch_rows rows in the given order, `epochs`
+ * passes; loss = the last epoch's mean */
+int v2g_ws_train(v2g_warmstart* w, long rows, const float* features, const float* targets, int epochs,
+                 int batch_rows, float lr, double* loss);
+int v2g_ws_propose(v2g_warmstart* w, v2g_handle* h);
 
 /* The RDMs handed to the orbital optimiser, as PackSpatialDensity
  * (v2rdm_solver.cc:3664-3773), from the handle's x: d1 = spin-summed 1-RDM,

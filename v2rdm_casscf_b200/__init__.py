@@ -35,7 +35,10 @@ EXPORTS = [
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
     "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density", "v2g_block_gemm_device",
+    "v2g_time_maps",
     "v2g_write_checkpoint", "v2g_read_checkpoint", "v2g_set_active_orbital_energies", "v2g_solve_continue",
+    "v2g_ws_create", "v2g_ws_destroy", "v2g_ws_num_params", "v2g_ws_get_params", "v2g_ws_set_params", "v2g_ws_rows",
+    "v2g_ws_features", "v2g_ws_targets", "v2g_ws_forward", "v2g_ws_gradient", "v2g_ws_train", "v2g_ws_propose",
 ]
 
 
@@ -162,6 +165,22 @@ def lib():
         for f in ("v2g_apply_A_batched_device", "v2g_apply_AT_batched_device"):
             getattr(L, f).argtypes = [P, I, P, P, P]
         L.v2g_block_gemm_device.argtypes = [I, IP, P, I, P, I, P, P, I, I]
+        L.v2g_time_maps.argtypes = [P, I, I, DP, DP]
+        FP = ctypes.POINTER(ctypes.c_float)
+        L.v2g_ws_create.argtypes = [I, I, ctypes.c_ulonglong, ctypes.POINTER(P)]
+        L.v2g_ws_destroy.argtypes = [P]
+        L.v2g_ws_num_params.restype = L_
+        L.v2g_ws_num_params.argtypes = [P]
+        L.v2g_ws_get_params.argtypes = [P, FP]
+        L.v2g_ws_set_params.argtypes = [P, FP]
+        L.v2g_ws_rows.restype = L_
+        L.v2g_ws_rows.argtypes = [P]
+        L.v2g_ws_features.argtypes = [P, FP]
+        L.v2g_ws_targets.argtypes = [P, FP]
+        L.v2g_ws_forward.argtypes = [P, L_, FP, FP]
+        L.v2g_ws_gradient.argtypes = [P, L_, FP, FP, DP, FP]
+        L.v2g_ws_train.argtypes = [P, L_, FP, FP, I, I, ctypes.c_float, DP]
+        L.v2g_ws_propose.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -262,9 +281,9 @@ class V2RDMSolver:
         o.spin_adapt_g2 = int(bool(opts["SPIN_ADAPT_G2"]))
         o.constrain_d3 = int(bool(opts["CONSTRAIN_D3"]))
         o.constrain_d4 = int(bool(opts["CONSTRAIN_D4"]))
-        if start not in ("state", "feasible"):
-            raise ValueError("start is 'state' (guess()/set_state) or 'feasible'")
-        o.start = int(start == "feasible")
+        if start not in ("state", "feasible", "learned"):
+            raise ValueError("start is 'state' (guess()/set_state), 'feasible' or 'learned'")
+        o.start = {"state": 0, "feasible": 1, "learned": 2}[start]
         o.cg_extrapolate = int(bool(cg_extrapolate))
         o.anderson_memory = int(anderson_memory)
         o.mixed_precision = int(bool(mixed_precision))
@@ -373,6 +392,12 @@ class V2RDMSolver:
         _check(f(self.h, int(nvec), ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
                  ctypes.c_void_p(stream) if stream else None))
 
+    def time_maps(self, nvec=1, reps=50):
+        """(seconds per launch of A, of A^T) on nvec interleaved vectors (graph replay, CUDA events)."""
+        a, t = ctypes.c_double(), ctypes.c_double()
+        _check(lib().v2g_time_maps(self.h, int(nvec), int(reps), ctypes.byref(a), ctypes.byref(t)))
+        return a.value, t.value
+
     def update_xz(self, mu):
         _check(lib().v2g_update_xz(self.h, float(mu)))
 
@@ -448,6 +473,80 @@ def block_gemm_device(dims, d_a, d_b, d_c, trans_a=False, trans_b=False, d_d=Non
                                        ctypes.c_void_p(d_b), int(bool(trans_b)),
                                        ctypes.c_void_p(d_d) if d_d else None, ctypes.c_void_p(d_c),
                                        int(bool(tensor_cores)), int(device)))
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class WarmStart:
+    """The learned warm start (v2g_ws_*): a pair-wise MLP trained on converged
+    solutions of this solver that proposes D1, the D2ab pair diagonal and mu;
+    a solver created with ``start="learned"`` projects the proposal onto
+    A x = b at the start of its solve."""
+
+    def __init__(self, hidden=224, device=0, seed=0):
+        h = ctypes.c_void_p()
+        _check(lib().v2g_ws_create(int(hidden), int(device), ctypes.c_ulonglong(seed), ctypes.byref(h)))
+        self.h = h
+        self.nparams = lib().v2g_ws_num_params(h)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.v2g_ws_destroy(h)
+            self.h = None
+
+    @property
+    def params(self):
+        out = np.zeros(self.nparams, dtype=np.float32)
+        _check(lib().v2g_ws_get_params(self.h, _fp(out)))
+        return out
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.nparams
+        _check(lib().v2g_ws_set_params(self.h, _fp(p)))
+
+    @staticmethod
+    def features(solver):
+        rows = lib().v2g_ws_rows(solver.h)
+        out = np.zeros((rows, 16), dtype=np.float32)
+        _check(lib().v2g_ws_features(solver.h, _fp(out)))
+        return out
+
+    @staticmethod
+    def targets(solver):
+        rows = lib().v2g_ws_rows(solver.h)
+        out = np.zeros((rows, 3), dtype=np.float32)
+        _check(lib().v2g_ws_targets(solver.h, _fp(out)))
+        return out
+
+    def forward(self, features):
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros((f.shape[0], 3), dtype=np.float32)
+        _check(lib().v2g_ws_forward(self.h, f.shape[0], _fp(f), _fp(out)))
+        return out
+
+    def gradient(self, features, targets):
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = ctypes.c_double()
+        _check(lib().v2g_ws_gradient(self.h, f.shape[0], _fp(f), _fp(t), ctypes.byref(loss), _fp(g)))
+        return loss.value, g
+
+    def train(self, features, targets, epochs=100, batch_rows=4096, lr=1e-3):
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        loss = ctypes.c_double()
+        _check(lib().v2g_ws_train(self.h, f.shape[0], _fp(f), _fp(t), int(epochs), int(batch_rows), float(lr),
+                                  ctypes.byref(loss)))
+        return loss.value
+
+    def propose(self, solver):
+        _check(lib().v2g_ws_propose(self.h, solver.h))
 
 
 def last_batch_stats():

@@ -17,7 +17,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libv2rdm_b200.so")
 OBJDIR = os.path.join(ROOT, "_build", "obj")
 
-CU_SOURCES = ["maps.cu", "eig.cu", "tc_gemm.cu", "solver.cu"]
+CU_SOURCES = ["maps.cu", "eig.cu", "tc_gemm.cu", "mlp.cu", "warmstart.cu", "solver.cu"]
 CPP_SOURCES = ["layout.cpp", "constraints.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

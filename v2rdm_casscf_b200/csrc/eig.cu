@@ -857,6 +857,12 @@ __global__ void mirror_kernel(const BlockTask* __restrict__ tasks, double* __res
     for (int q = threadIdx.x; q < qend; q += blockDim.x) c[(int64_t)p * t.np + q] = c[(int64_t)q * t.np + p];
 }
 
+__global__ void block_mask_kernel(const BlockTask* __restrict__ tasks, int ntasks, const int* __restrict__ mask,
+                                  int* __restrict__ bmask) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += gridDim.x * blockDim.x)
+        bmask[t] = mask[tasks[t].inst] != 0;
+}
+
 __global__ void uncap_kernel(int n, const int* __restrict__ sel, int* __restrict__ max_sweeps) {
     for (int i = threadIdx.x; i < n; i += blockDim.x)
         if (sel[i]) max_sweeps[i] = 1 << 20;
@@ -1046,6 +1052,12 @@ void launch_ortho_step(const BlockTask* tasks, int ntasks, int max_np, const dou
                        cudaStream_t s) {
     if (ntasks == 0) return;
     ortho_step_kernel<<<dim3(max_np, ntasks), 128, 0, s>>>(tasks, G, bmask, M);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_block_mask(const BlockTask* tasks, int ntasks, const int* mask, int* bmask, cudaStream_t s) {
+    if (ntasks == 0) return;
+    block_mask_kernel<<<(ntasks + 255) / 256, 256, 0, s>>>(tasks, ntasks, mask, bmask);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -38,7 +38,14 @@ struct DevMap {
     const int32_t* long_ptr = nullptr;
     const int32_t* long_col = nullptr;
     const double* long_val = nullptr;
+    // kernel variant chosen by the autotuner for one instance count (-1: the
+    // built-in rule); see kMapVariants
+    int variant = -1;
 };
+// Map kernel variants: instances per thread (2, 4, 8) and whether the table
+// loads and output stores bypass the caches (streaming hints).
+constexpr int kMapVariants = 4;  // 0: 2 plain, 1: 4 plain, 2: 4 streamed, 3: 8 streamed
+const char* map_variant_name(int v);
 
 // out[r,b] = coef[b] * (sum_k val[k] in[col[k],b] - sub[r]) + add[r,b]
 // (each of sub, coef, add optional); instances with mask[b] == 0 are skipped.
@@ -231,6 +238,8 @@ void launch_mirror(const BlockTask* tasks, int ntasks, int max_np, double* C, co
 // back to orthonormal (the distance squares)
 void launch_ortho_step(const BlockTask* tasks, int ntasks, int max_np, const double* G, const int* bmask, double* M,
                        cudaStream_t s);
+// bmask[t] = mask[tasks[t].inst] != 0
+void launch_block_mask(const BlockTask* tasks, int ntasks, const int* mask, int* bmask, cudaStream_t s);
 // max_sweeps[i] = unlimited where sel[i]
 void launch_uncap(int n, const int* sel, int* max_sweeps, cudaStream_t s);
 // dst[i] |= src[i]

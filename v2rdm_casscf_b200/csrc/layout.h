@@ -53,6 +53,10 @@ struct Options {
     // Start the solve from the least-norm point of {A x = b} (x = A^T w with
     // A A^T w = b, y = z = 0, mu = 1) instead of the handle's state.
     bool feasible_start = false;
+    // Start from the handle's proposal (the learned warm start, v2g_ws_propose)
+    // projected onto {A x = b}, y = z = 0 and the proposed mu; the least-norm
+    // feasible point when the handle has no proposal.
+    bool proposal_start = false;
     // Start each outer iteration's CG from y_k + (y_k - y_{k-1}), the linear
     // extrapolation of the last two CG solutions, instead of from y_k.  CG
     // still stops on the same residual test, so only its iteration count

@@ -664,9 +664,21 @@ static int spmv_grid(int64_t nrows, int B) {
 
 // Row tiles (kThreads slots each) per ELL bucket, proportional to its slots,
 // at most kSpmvBlocks tiles in all; every tile runs once per instance chunk.
+const char* map_variant_name(int v) {
+    static const char* names[kMapVariants] = {"2 instances/thread", "4 instances/thread",
+                                              "4 instances/thread, streamed", "8 instances/thread, streamed"};
+    return (v >= 0 && v < kMapVariants) ? names[v] : "built-in rule";
+}
+
+static int map_variant(const DevMap& M, int B) {
+    if (M.variant >= 0 && M.variant < kMapVariants) return M.variant;
+    return B <= 2 ? 0 : (B < 8 ? 1 : 2);
+}
+
 static Blocks map_blocks(const DevMap& M, int B) {
     Blocks bl{};
-    const int ch = B <= 2 ? 2 : 4;
+    const int var = map_variant(M, B);
+    const int ch = var == 0 ? 2 : (var == 3 ? 8 : 4);
     bl.nchunk = (B + ch - 1) / ch;
     int64_t tot = 0;
     for (int i = 0; i < M.nb; i++) tot += (M.nslots[i] + kThreads - 1) / kThreads;
@@ -692,12 +704,12 @@ static int run_map(const DevMap& M, int B, const double* in, double* out, const 
         // the gathered input: 7 % faster at n = 17..20 on B200, slower for
         // single instances
         const int g = bl.start[M.nb] * bl.nchunk;
-        if (B <= 2)
-            ell_kernel<2, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
-        else if (B < 8)
-            ell_kernel<4, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
-        else
-            ell_kernel<4, true><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial);
+        switch (map_variant(M, B)) {
+            case 0: ell_kernel<2, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
+            case 1: ell_kernel<4, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
+            case 2: ell_kernel<4, true><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
+            default: ell_kernel<8, true><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
+        }
         g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     }
     if (M.nlong > 0) {

@@ -22,6 +22,7 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/v2rdm_gpu.h"
@@ -29,6 +30,7 @@
 #include "constraints.h"
 #include "kernels.cuh"
 #include "layout.h"
+#include "warmstart.h"
 
 namespace v2g {
 
@@ -118,6 +120,15 @@ struct MapTable {
                 lptr.push_back((int32_t)lcol.size());
             }
         }
+        // inside a bucket, rows are ordered by their first column: rows that
+        // gather from the same region of the input run in the same CTA wave,
+        // so their gathers hit L2 (the output is written through rows[])
+        for (int w = 0; w < kMaxBuckets; w++)
+            std::stable_sort(brow[w].begin(), brow[w].end(), [&](int32_t a, int32_t b) {
+                const int32_t ca = M.rowptr[a] < M.rowptr[a + 1] ? M.col[M.rowptr[a]] : -1;
+                const int32_t cb = M.rowptr[b] < M.rowptr[b + 1] ? M.col[M.rowptr[b]] : -1;
+                return ca < cb;
+            });
         std::vector<int32_t> hrows, hcols;
         std::vector<double> hvals;
         dm = DevMap{};
@@ -229,6 +240,12 @@ struct Problem {
     std::shared_ptr<DeviceTables> T;
     std::vector<std::array<double, 8>> trace;
     std::vector<double> energies;  // active orbital energies, if the caller gave them
+    // the integrals of an all-active C1 space (h: n x n, Lq: nq x n x n), kept
+    // for the learned warm start's features
+    std::vector<double> hmat, Lq;
+    int nq = 0;
+    // a start proposal (x holds it) that a solve with start = 2 projects onto A x = b
+    bool proposal = false;
     // Loop state carried by v2g_solve_continue: outer iterations done and the
     // last eps(p), eps(d) (they set the next CG tolerance); every solve
     // updates them.  resume > 0 makes the next solve continue the loop for at
@@ -276,6 +293,8 @@ class GroupRun {
         mu_.alloc(B_);
         coef_.alloc(B_);
         mask_.alloc(B_);
+        smask1_.alloc(B_);
+        smask2_.alloc(B_);
         cs_.alloc(B_);
         nact_.alloc(8);  // counters: CG, Jacobi, refinement, fallback, restart
         for (auto* p : P_) extrapolate_ = extrapolate_ || p->opt.cg_extrapolate;
@@ -285,8 +304,14 @@ class GroupRun {
         }
         CK(cudaMallocHost(&hscal_, sizeof(double) * 4 * B_));
         CK(cudaMallocHost(&hnact_, sizeof(int) * 8));
+        CK(cudaMallocHost(&hcs_, sizeof(CgScalars) * B_));
+        stage_cap_ = 1 << 20;
+        CK(cudaMallocHost(&stage_, stage_cap_));
+        mA_ = T.A();
+        mAT_ = T.AT();
         build_projection_plan();
         upload_state();
+        tune_maps();
         alloc_anderson(X);
         if (const char* d = std::getenv("V2G_DIAG")) diag_every_ = std::atoi(d);
         if (diag_every_ > 0)
@@ -303,6 +328,9 @@ class GroupRun {
         for (auto e : prof_ev_) cudaEventDestroy(e);
         if (hscal_) cudaFreeHost(hscal_);
         if (hnact_) cudaFreeHost(hnact_);
+        if (hcs_) cudaFreeHost(hcs_);
+        if (hdots_ptr_) cudaFreeHost(hdots_ptr_);
+        if (stage_) cudaFreeHost(stage_);
         if (s_) cudaStreamDestroy(s_);
     }
 
@@ -351,7 +379,7 @@ class GroupRun {
     void project(const std::vector<double>& rho = {}, bool mixed = false) {
         tc_ = mixed && nlarge_ > 0;
         if (tc_) tc_projections_++;
-        launch_spmv(T_.AT(), B_, y_.p, aty_.p, nullptr, nullptr, nullptr, mask_.p, s_);
+        launch_spmv(mAT_, B_, y_.p, aty_.p, nullptr, nullptr, nullptr, mask_.p, s_);
         launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_);
         if (nlarge_ == 0) return;
         launch_form_u(large_d_.p, nlarge_, max_np_, B_, aty_.p, c_.p, x_.p, mu_.p, mask_.p, U_.p, s_);
@@ -406,12 +434,10 @@ class GroupRun {
         // blocks still unconverged join the Jacobi set (their OA update was applied)
         if (nref > 0) launch_merge_mask(nlarge_, bref_.p, bjac_.p, s_);
         launch_count(nlarge_, bjac_.p, nact_.p + 3, s_);
-        CK(cudaMemcpyAsync(hnact_ + 3, nact_.p + 3, sizeof(int), cudaMemcpyDeviceToHost, s_));
-        CK(cudaStreamSynchronize(s_));
         // blocks whose eigenvectors degraded restart cold (V = I, W = U) and
         // converge fully; they leave the refinement and warm Jacobi sets
         launch_count(nlarge_, restart_.p, nact_.p + 4, s_);
-        CK(cudaMemcpyAsync(hnact_ + 4, nact_.p + 4, sizeof(int), cudaMemcpyDeviceToHost, s_));
+        CK(cudaMemcpyAsync(hnact_ + 3, nact_.p + 3, 2 * sizeof(int), cudaMemcpyDeviceToHost, s_));
         CK(cudaStreamSynchronize(s_));
         if (hnact_[3] > 0) {
             jacobi_blocks_ += hnact_[3];
@@ -460,10 +486,10 @@ class GroupRun {
     }
 
     void apply_A(const double* d_in, double* d_out) {
-        launch_spmv(T_.A(), B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
+        launch_spmv(mA_, B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
     }
     void apply_AT(const double* d_in, double* d_out) {
-        launch_spmv(T_.AT(), B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
+        launch_spmv(mAT_, B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
     }
     cudaStream_t stream() const { return s_; }
     DevBuf<double>& xbuf() { return x_; }
@@ -507,13 +533,24 @@ class GroupRun {
             std::vector<int> fs(B_);
             bool any = false;
             // a continued loop keeps its state; its first segment starts like a solve
-            for (int b = 0; b < B_; b++)
-                any |= (fs[b] = (opt(b).feasible_start && oiter[b] == 0) ? 1 : 0) != 0;
+            // 1: least-norm feasible point; 2: the instance's proposal (the
+            // learned warm start) projected onto A x = b; without a proposal,
+            // start 2 falls back to 1
+            for (int b = 0; b < B_; b++) {
+                fs[b] = 0;
+                if (oiter[b] != 0) continue;
+                if (opt(b).proposal_start)
+                    fs[b] = P_[b]->proposal ? 2 : 1;
+                else if (opt(b).feasible_start)
+                    fs[b] = 1;
+                any |= fs[b] != 0;
+            }
             if (any) {
                 feasible_start(fs, cs);
                 for (int b = 0; b < B_; b++)
                     if (fs[b]) {
-                        mu[b] = 1.0;
+                        mu[b] = fs[b] == 2 ? P_[b]->mu : 1.0;
+                        P_[b]->proposal = false;  // a proposal serves one solve
                         iiter[b] += cs[b].iter;
                         stalls[b] += cs[b].stalled;
                     }
@@ -545,22 +582,22 @@ class GroupRun {
             int nactive = 0;
             for (int b = 0; b < B_; b++) nactive += active[b];
             if (nactive == 0) break;
-            CK(cudaMemcpyAsync(mask_.p, active.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+            put(mask_.p, active.data(), B_);
             for (int b = 0; b < B_; b++) coef[b] = -opt(b).tau * mu[b];
-            CK(cudaMemcpyAsync(coef_.p, coef.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
-            CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+            put(coef_.p, coef.data(), B_);
+            put(mu_.p, mu.data(), B_);
             if (aa_m_ > 0) {
                 // w = the (x, z) this step starts from
                 for (int b = 0; b < B_; b++) aa.mode[b] = (active[b] && aa_memory(b) > 0) ? 1 : 0;
-                CK(cudaMemcpyAsync(amode_.p, aa.mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+                put(amode_.p, aa.mode.data(), B_);
                 launch_aa_save(nx_, B_, x_.p, z_.p, aw_.p, amode_.p, s_);
             }
             std::fill(mu_changed.begin(), mu_changed.end(), 0);
             CK(cudaEventRecord(e0, s_));
             // Ax = -tau mu (A x - b); z <- c - z; B = A z + Ax   (:1783-1794)
-            launch_spmv(T_.A(), B_, x_.p, ax_.p, T_.b.p, coef_.p, nullptr, mask_.p, s_);
+            launch_spmv(mA_, B_, x_.p, ax_.p, T_.b.p, coef_.p, nullptr, mask_.p, s_);
             launch_c_minus_z(nx_, B_, c_.p, z_.p, mask_.p, s_);
-            launch_spmv(T_.A(), B_, z_.p, bv_.p, nullptr, nullptr, ax_.p, mask_.p, s_);
+            launch_spmv(mA_, B_, z_.p, bv_.p, nullptr, nullptr, ax_.p, mask_.p, s_);
             // CG tolerance (:1797-1805)
             for (int b = 0; b < B_; b++) {
                 const Options& o = opt(b);
@@ -575,7 +612,7 @@ class GroupRun {
                 cs[b].active = active[b];
                 cs[b].maxiter = o.cg_maxiter;
             }
-            CK(cudaMemcpyAsync(cs_.p, cs.data(), B_ * sizeof(CgScalars), cudaMemcpyHostToDevice, s_));
+            put(cs_.p, cs.data(), B_);
             // CG starts from y_k + (y_k - y_{k-1}) once two CG solutions exist
             // (mode 2); before that it only records y_k (mode 1)
             if (extrapolate_) {
@@ -583,11 +620,11 @@ class GroupRun {
                     exmode[b] = (active[b] && opt(b).cg_extrapolate) ? (ycount[b] >= 2 ? 2 : 1) : 0;
                     if (exmode[b]) ycount[b]++;
                 }
-                CK(cudaMemcpyAsync(ex_.p, exmode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+                put(ex_.p, exmode.data(), B_);
                 launch_cg_extrapolate(nc_, B_, y_.p, yprev_.p, ex_.p, s_);
             }
             cg_solve();
-            CK(cudaMemcpyAsync(cs.data(), cs_.p, B_ * sizeof(CgScalars), cudaMemcpyDeviceToHost, s_));
+            CK(cudaMemcpyAsync(hcs_, cs_.p, B_ * sizeof(CgScalars), cudaMemcpyDeviceToHost, s_));
             CK(cudaEventRecord(e1, s_));
             std::vector<double> rho(B_, 0.0);
             for (int b = 0; b < B_; b++)
@@ -608,13 +645,15 @@ class GroupRun {
             CK(cudaEventRecord(e2, s_));
             // ed = ||A^T y + z - c||, ep = ||A x - b||, E = c.x, b.y (:1826-1852)
             launch_reduce(RED_ED, nx_, B_, aty_.p, z_.p, c_.p, nullptr, partial_.p, red_.p, s_);
-            launch_spmv(T_.A(), B_, x_.p, ax_.p, nullptr, nullptr, nullptr, mask_.p, s_);
+            launch_spmv(mA_, B_, x_.p, ax_.p, nullptr, nullptr, nullptr, mask_.p, s_);
             launch_reduce(RED_EP, nc_, B_, ax_.p, nullptr, nullptr, T_.b.p, partial_.p, red_.p + B_, s_);
             launch_reduce(RED_DOT, nx_, B_, c_.p, x_.p, nullptr, nullptr, partial_.p, red_.p + 2 * B_, s_);
             launch_reduce(RED_DOT_ROW, nc_, B_, y_.p, nullptr, nullptr, T_.b.p, partial_.p, red_.p + 3 * B_, s_);
             CK(cudaMemcpyAsync(hscal_, red_.p, 4 * B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
             if (tc_) tc_gemm_status_async(hnact_ + 5, s_);
             CK(cudaStreamSynchronize(s_));
+            stage_synced();
+            std::copy(hcs_, hcs_ + B_, cs.begin());
             if (tc_ && hnact_[5] != 0)
                 throw CudaError("a tensor-core GEMM of the projection did not finish (pipeline wait ran out)");
             float ms_cg = 0, ms_xz = 0;
@@ -747,13 +786,21 @@ class GroupRun {
             if (aa.begin(b, aa_memory(b), mu_changed[b] != 0)) any = true;
         }
         if (!any) return;
-        CK(cudaMemcpyAsync(amode_.p, aa.mode.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
-        CK(cudaMemcpyAsync(aslot_.p, aa.slot.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        put(amode_.p, aa.mode.data(), B_);
+        put(aslot_.p, aa.slot.data(), B_);
         launch_aa_update(nx_, B_, aa_m_, x_.p, z_.p, aw_.p, af_.p, ag_.p, adF_.p, adG_.p, amode_.p, aslot_.p,
                          apart_.p, adots_.p, s_);
-        std::vector<double> dots((size_t)(2 * aa_m_ + 1) * B_);
-        CK(cudaMemcpyAsync(dots.data(), adots_.p, dots.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        const size_t ndots = (size_t)(2 * aa_m_ + 1) * B_;
+        if (hdots_.size() < ndots) {
+            if (hdots_ptr_) CK(cudaFreeHost(hdots_ptr_));
+            hdots_ptr_ = nullptr;
+            CK(cudaMallocHost(&hdots_ptr_, ndots * sizeof(double)));
+            hdots_.assign(ndots, 0.0);
+        }
+        CK(cudaMemcpyAsync(hdots_ptr_, adots_.p, ndots * sizeof(double), cudaMemcpyDeviceToHost, s_));
         CK(cudaStreamSynchronize(s_));
+        stage_synced();
+        std::vector<double> dots(hdots_ptr_, hdots_ptr_ + ndots);
         std::vector<double> gamma((size_t)B_ * aa_m_, 0.0);
         std::vector<int> mix(B_, 0);
         bool anymix = false;
@@ -764,10 +811,9 @@ class GroupRun {
             }
         }
         if (!anymix) return;
-        CK(cudaMemcpyAsync(agam_.p, gamma.data(), gamma.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
-        CK(cudaMemcpyAsync(amix_.p, mix.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        put(agam_.p, gamma.data(), gamma.size());
+        put(amix_.p, mix.data(), B_);
         launch_aa_mix(nx_, B_, aa_m_, x_.p, z_.p, adG_.p, agam_.p, amix_.p, s_);
-        CK(cudaStreamSynchronize(s_));
     }
 
     static bool any_nonfinite(const std::vector<double>& ep, const std::vector<double>& ed) {
@@ -829,35 +875,53 @@ class GroupRun {
                      b, B_, (long long)nx_, oiter, sums[0], sums[1], sums[2], mu, cg_iters);
     }
 
-    // Least-norm feasible start for the instances with fs[b] set: w solves
-    // A A^T w = b by the loop's CG (to 1e-10 ||b||), x = A^T w, y = z = 0,
-    // mu = 1.  A x = b is then met to the CG tolerance; the BPSDP iteration
-    // starts from a feasible primal with zero duals.
+    // Start for the instances with fs[b] set.  fs[b] = 1: the least-norm
+    // feasible point, w solves A A^T w = b by the loop's CG (to 1e-10 ||b||),
+    // x = A^T w, y = z = 0, mu = 1.  fs[b] = 2: the instance's x (a proposal)
+    // moved onto A x = b the same way, x += A^T w with A A^T w = b - A x,
+    // y = z = 0, mu = the problem's mu.  A x = b then holds to the CG
+    // tolerance and the BPSDP iteration starts from a feasible primal with
+    // zero duals.
     void feasible_start(const std::vector<int>& fs, std::vector<CgScalars>& cs) {
-        CK(cudaMemcpyAsync(mask_.p, fs.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        std::vector<int> m1(B_), m2(B_), mall(B_);
+        std::vector<double> coef(B_, 0.0), mu(B_);
+        for (int b = 0; b < B_; b++) {
+            m1[b] = fs[b] == 1;
+            m2[b] = fs[b] == 2;
+            mall[b] = fs[b] != 0;
+            coef[b] = -1.0;
+            mu[b] = P_[b]->mu;
+        }
+        CK(cudaMemcpyAsync(smask1_.p, m1.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(smask2_.p, m2.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(mask_.p, mall.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(coef_.p, coef.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
         double bn = 0.0;
         for (double v : T_.hb) bn += v * v;
         bn = std::sqrt(bn);
         for (int b = 0; b < B_; b++) {
             cs[b] = CgScalars{};
             cs[b].tol = 1e-10 * std::max(1.0, bn);
-            cs[b].active = fs[b];
+            cs[b].active = fs[b] != 0;
             cs[b].maxiter = P_[b]->opt.cg_maxiter;
         }
         CK(cudaMemcpyAsync(cs_.p, cs.data(), B_ * sizeof(CgScalars), cudaMemcpyHostToDevice, s_));
-        launch_set_rows(nc_, B_, T_.b.p, bv_.p, mask_.p, s_);  // right-hand side b
+        launch_set_rows(nc_, B_, T_.b.p, bv_.p, smask1_.p, s_);  // right-hand side b
+        // b - A x for the proposals
+        launch_spmv(mA_, B_, x_.p, bv_.p, T_.b.p, coef_.p, nullptr, smask2_.p, s_);
         launch_set_rows(nc_, B_, nullptr, y_.p, mask_.p, s_);  // w starts at 0
         cg_solve();
         CK(cudaMemcpyAsync(cs.data(), cs_.p, B_ * sizeof(CgScalars), cudaMemcpyDeviceToHost, s_));
-        launch_spmv(T_.AT(), B_, y_.p, x_.p, nullptr, nullptr, nullptr, mask_.p, s_);
+        launch_spmv(mAT_, B_, y_.p, x_.p, nullptr, nullptr, nullptr, smask1_.p, s_);
+        launch_spmv(mAT_, B_, y_.p, x_.p, nullptr, nullptr, x_.p, smask2_.p, s_);
         launch_set_rows(nc_, B_, nullptr, y_.p, mask_.p, s_);
         launch_set_rows(nx_, B_, nullptr, z_.p, mask_.p, s_);
-        std::vector<double> mu(B_);
-        CK(cudaMemcpyAsync(mu.data(), mu_.p, B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        std::vector<double> dmu(B_);
+        CK(cudaMemcpyAsync(dmu.data(), mu_.p, B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
         CK(cudaStreamSynchronize(s_));
         for (int b = 0; b < B_; b++)
-            if (fs[b]) mu[b] = 1.0;
-        CK(cudaMemcpyAsync(mu_.p, mu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+            if (fs[b]) dmu[b] = fs[b] == 2 ? mu[b] : 1.0;
+        CK(cudaMemcpyAsync(mu_.p, dmu.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
         CK(cudaStreamSynchronize(s_));
     }
 
@@ -872,6 +936,82 @@ class GroupRun {
     double d2h_bytes() const { return 8.0 * B_ * (2.0 * nx_ + nc_); }
 
   private:
+    // The autotuner of the map kernels: for this group's layout and instance
+    // count, every variant of kMapVariants is timed on A and on A^T (CUDA
+    // events around a few launches on the group's stream) and the fastest is
+    // kept for the process (the choice depends only on layout and B).
+    void tune_maps() {
+        static std::mutex mu;
+        static std::map<std::tuple<const void*, int, int>, int> chosen;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        for (int which = 0; which < 2; which++) {
+            DevMap& M = which == 0 ? mA_ : mAT_;
+            const auto key = std::make_tuple((const void*)M.rows, B_, which);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                auto it = chosen.find(key);
+                if (it != chosen.end()) {
+                    M.variant = it->second;
+                    continue;
+                }
+            }
+            if (!e0) {
+                CK(cudaEventCreate(&e0));
+                CK(cudaEventCreate(&e1));
+            }
+            const double* in = which == 0 ? x_.p : y_.p;
+            double* out = which == 0 ? ax_.p : aty_.p;
+            float best = 0.f;
+            int bestv = -1;
+            for (int v = 0; v < kMapVariants; v++) {
+                DevMap m = M;
+                m.variant = v;
+                launch_spmv(m, B_, in, out, nullptr, nullptr, nullptr, nullptr, s_);
+                CK(cudaEventRecord(e0, s_));
+                for (int k = 0; k < 5; k++) launch_spmv(m, B_, in, out, nullptr, nullptr, nullptr, nullptr, s_);
+                CK(cudaEventRecord(e1, s_));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (bestv < 0 || ms < best) {
+                    best = ms;
+                    bestv = v;
+                }
+            }
+            M.variant = bestv;
+            std::lock_guard<std::mutex> lk(mu);
+            chosen[key] = bestv;
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+
+    // Host -> device copies of per-iteration scalars go through pinned
+    // staging memory: cudaMemcpyAsync from pageable memory first drains the
+    // stream, which would stall the pipeline at every copy.  The ring restarts
+    // after a stream synchronisation (stage_synced), or synchronises itself
+    // when full.
+    template <class T>
+    void put(T* dst, const T* src, size_t n) {
+        const size_t bytes = n * sizeof(T);
+        if (bytes == 0) return;
+        size_t off = (stage_off_ + 15) & ~(size_t)15;
+        if (off + bytes > stage_cap_) {
+            CK(cudaStreamSynchronize(s_));
+            off = 0;
+            if (bytes > stage_cap_) {
+                CK(cudaFreeHost(stage_));
+                stage_ = nullptr;
+                stage_cap_ = bytes;
+                CK(cudaMallocHost(&stage_, stage_cap_));
+            }
+        }
+        std::memcpy(stage_ + off, src, bytes);
+        CK(cudaMemcpyAsync(dst, stage_ + off, bytes, cudaMemcpyHostToDevice, s_));
+        stage_off_ = off + bytes;
+    }
+    void stage_synced() { stage_off_ = 0; }
+
     // The projection's dense products: on all tiles of C (full) or on the
     // upper tiles of a symmetric C (sym, mirrored afterwards), in FP64 or, in
     // the mixed-precision phase (tc_), as 3xTF32 products on the tensor cores.
@@ -923,8 +1063,8 @@ class GroupRun {
     // CGSolver::solve for every instance whose CG scalars are active.
     void cg_solve() {
         // Ap = A A^T y ; r = B - Ap ; p = r
-        map_launch(T_.AT(), y_.p, atp_.p, nullptr, mask_.p);
-        map_launch(T_.A(), atp_.p, ap_.p, nullptr, mask_.p);
+        map_launch(mAT_, y_.p, atp_.p, nullptr, mask_.p);
+        map_launch(mA_, atp_.p, ap_.p, nullptr, mask_.p);
         launch_cg_init(nc_, B_, bv_.p, ap_.p, r_.p, p_.p, cs_.p, s_);
         launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
         launch_cg_set_rr(B_, cs_.p, red_.p, nact_.p, s_);
@@ -950,8 +1090,8 @@ class GroupRun {
     static constexpr int kCgChunk = 4;
     // One CG iteration (cg_solver.cc:141-177) for every instance whose scalars are active.
     void cg_iteration() {
-        map_launch(T_.AT(), p_.p, atp_.p, nullptr, mask_.p);
-        map_launch(T_.A(), atp_.p, ap_.p, p_.p, mask_.p);  // Ap and p.Ap (into red_)
+        map_launch(mAT_, p_.p, atp_.p, nullptr, mask_.p);
+        map_launch(mA_, atp_.p, ap_.p, p_.p, mask_.p);  // Ap and p.Ap (into red_)
         launch_cg_step(nc_, B_, y_.p, r_.p, p_.p, ap_.p, cs_.p, red_.p, partial_.p, nact_.p, s_);
         launch_cg_update_p(nc_, B_, p_.p, r_.p, cs_.p, s_);
     }
@@ -996,21 +1136,15 @@ class GroupRun {
                 cap_ = true;
             }
         }
-        CK(cudaMemcpyAsync(msw_.p, ms.data(), nlarge_ * sizeof(int), cudaMemcpyHostToDevice, s_));
-        CK(cudaMemcpyAsync(jtol_.p, jt.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
-        CK(cudaMemcpyAsync(otol_.p, ot.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
-        CK(cudaMemcpyAsync(atol_.p, at.data(), nlarge_ * sizeof(double), cudaMemcpyHostToDevice, s_));
-        CK(cudaStreamSynchronize(s_));
+        put(msw_.p, ms.data(), nlarge_);
+        put(jtol_.p, jt.data(), nlarge_);
+        put(otol_.p, ot.data(), nlarge_);
+        put(atol_.p, at.data(), nlarge_);
     }
 
     void set_block_masks() {
-        // bact[t] = mask[inst(t)], computed on the host copy of the task list
-        std::vector<int> act(B_);
-        CK(cudaMemcpyAsync(act.data(), mask_.p, B_ * sizeof(int), cudaMemcpyDeviceToHost, s_));
-        CK(cudaStreamSynchronize(s_));
-        std::vector<int> bm(nlarge_);
-        for (int t = 0; t < nlarge_; t++) bm[t] = act[hlarge_[t].inst];
-        CK(cudaMemcpyAsync(bact_.p, bm.data(), nlarge_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        // bact[t] = mask[inst(t)], on the device (no round trip through the host)
+        launch_block_mask(large_d_.p, nlarge_, mask_.p, bact_.p, s_);
     }
 
     void build_projection_plan() {
@@ -1123,12 +1257,13 @@ class GroupRun {
     }
 
     DeviceTables& T_;
+    DevMap mA_, mAT_;  // the group's copies of the maps, with the tuned kernel variant
     std::vector<Problem*> P_;
     int B_;
     int64_t nx_ = 0, nc_ = 0;
     cudaStream_t s_ = nullptr;
     DevBuf<double> c_, x_, z_, aty_, atp_, y_, ax_, bv_, r_, p_, ap_, partial_, red_, mu_, coef_;
-    DevBuf<int> mask_, nact_;
+    DevBuf<int> mask_, nact_, smask1_, smask2_;
     DevBuf<CgScalars> cs_;
     // CG start extrapolation (cg_extrapolate): the previous CG start and the
     // per-instance mode of the extrapolation kernel
@@ -1144,6 +1279,11 @@ class GroupRun {
     DevBuf<int> amode_, aslot_, amix_;
     double* hscal_ = nullptr;
     int* hnact_ = nullptr;
+    char* stage_ = nullptr;
+    size_t stage_cap_ = 0, stage_off_ = 0;
+    CgScalars* hcs_ = nullptr;  // pinned copy of the CG scalars after a CG solve
+    double* hdots_ptr_ = nullptr;  // pinned Anderson dot products
+    std::vector<double> hdots_;
     // projection plan
     std::vector<BlockTask> hlarge_;
     DevBuf<BlockTask> small_d_, large_d_;
@@ -1268,8 +1408,9 @@ int v2g_create(const v2g_options* opt, int nirrep, const int* frzcpi, const int*
         o.spin_adapt_g2 = opt->spin_adapt_g2 != 0;
         o.constrain_d4 = opt->constrain_d4 != 0;
         o.constrain_d3 = opt->constrain_d3 != 0 || o.constrain_d4;  // v2rdm_solver.cc:527-532
-        if (opt->start != 0 && opt->start != 1) return v2g::fail(V2G_ERR_ARG, "start must be 0 or 1");
+        if (opt->start < 0 || opt->start > 2) return v2g::fail(V2G_ERR_ARG, "start must be 0, 1 or 2");
         o.feasible_start = opt->start == 1;
+        o.proposal_start = opt->start == 2;
         if (opt->cg_extrapolate != 0 && opt->cg_extrapolate != 1)
             return v2g::fail(V2G_ERR_ARG, "cg_extrapolate must be 0 or 1");
         o.cg_extrapolate = opt->cg_extrapolate == 1;
@@ -1329,6 +1470,26 @@ int v2g_set_hamiltonian(v2g_handle* h, const double* oei, const double* qmo, int
         if (!err.empty()) return v2g::fail(V2G_ERR_ARG, err);
         P.enuc = enuc;
         P.have_c = true;
+        P.hmat.clear();
+        P.Lq.clear();
+        P.nq = 0;
+        int other = 0;
+        for (int hh = 0; hh < P.L.nirrep; hh++)
+            other += P.sp.frzcpi[hh] + P.sp.rstcpi[hh] + P.sp.rstvpi[hh] + P.sp.frzvpi[hh];
+        if (P.L.nirrep == 1 && other == 0) {
+            const int n = P.L.amo;
+            const size_t ntri = (size_t)n * (n + 1) / 2;
+            P.hmat.assign((size_t)n * n, 0.0);
+            P.Lq.assign((size_t)nq * n * n, 0.0);
+            for (int p = 0; p < n; p++)
+                for (int q = 0; q <= p; q++) {
+                    const size_t t = (size_t)p * (p + 1) / 2 + q;  // INDEX(p, q)
+                    P.hmat[p * n + q] = P.hmat[q * n + p] = oei[t];
+                    for (int Q = 0; Q < nq; Q++)
+                        P.Lq[((size_t)Q * n + p) * n + q] = P.Lq[((size_t)Q * n + q) * n + p] = qmo[Q * ntri + t];
+                }
+            P.nq = nq;
+        }
         return V2G_OK;
     });
 }
@@ -1360,6 +1521,7 @@ int v2g_guess_random(v2g_handle* h) {
     }
     for (int64_t i = 0; i < P.L.ncon; i++) P.y[i] = ((double)rand() / RAND_MAX - 1.0) * 2.0;
     P.mu = 1.0;
+    P.proposal = false;
     return V2G_OK;
 }
 
@@ -1370,6 +1532,7 @@ int v2g_set_state(v2g_handle* h, const double* x, const double* y, const double*
     std::copy(z, z + P.L.dimx, P.z.begin());
     std::copy(y, y + P.L.ncon, P.y.begin());
     P.mu = mu;
+    P.proposal = false;
     return V2G_OK;
 }
 
@@ -1849,6 +2012,65 @@ int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const dou
     });
 }
 
+int v2g_time_maps(v2g_handle* h, int nvec, int reps, double* sec_A, double* sec_AT) {
+    return v2g::guarded([&]() -> int {
+        if (!h || nvec < 1 || nvec > 256 || reps < 1 || reps > 10000 || !sec_A || !sec_AT)
+            return v2g::fail(V2G_ERR_ARG, "bad map timing arguments");
+        v2g::require_device();
+        v2g::DeviceTables& T = h->P.tables();
+        v2g::DeviceScope scope(T.device);
+        const int64_t nx = T.L.dimx, nc = T.L.ncon;
+        v2g::DevBuf<double> x((size_t)nx * nvec), y((size_t)nc * nvec), ox((size_t)nx * nvec), oy((size_t)nc * nvec);
+        cudaStream_t s = nullptr;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        auto cleanup = [&]() {
+            if (ex) cudaGraphExecDestroy(ex);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (s) cudaStreamDestroy(s);
+        };
+        try {
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            for (int which = 0; which < 2; which++) {
+                const v2g::DevMap& M = which == 0 ? T.A() : T.AT();
+                const double* in = which == 0 ? x.p : y.p;
+                double* out = which == 0 ? oy.p : ox.p;
+                for (int k = 0; k < 3; k++) v2g::launch_spmv(M, nvec, in, out, nullptr, nullptr, nullptr, nullptr, s);
+                CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                for (int k = 0; k < reps; k++)
+                    v2g::launch_spmv(M, nvec, in, out, nullptr, nullptr, nullptr, nullptr, s);
+                cudaGraph_t g = nullptr;
+                CK(cudaStreamEndCapture(s, &g));
+                size_t nodes = 0;
+                cudaGraphGetNodes(g, nullptr, &nodes);
+                v2g::g_kernel_launches.fetch_sub((long)nodes, std::memory_order_relaxed);
+                const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+                cudaGraphDestroy(g);
+                CK(ie);
+                CK(cudaGraphLaunch(ex, s));  // warm
+                CK(cudaEventRecord(e0, s));
+                CK(cudaGraphLaunch(ex, s));
+                CK(cudaEventRecord(e1, s));
+                CK(cudaEventSynchronize(e1));
+                v2g::g_kernel_launches.fetch_add(2 * (long)nodes, std::memory_order_relaxed);
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                (which == 0 ? *sec_A : *sec_AT) = ms * 1e-3 / reps;
+                cudaGraphExecDestroy(ex);
+                ex = nullptr;
+            }
+        } catch (...) {
+            cleanup();
+            throw;
+        }
+        cleanup();
+        return V2G_OK;
+    });
+}
+
 int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int transA, const double* B, int transB,
                           const double* d, double* C, int tensor_cores, int device) {
     return v2g::guarded([&]() -> int {
@@ -1887,6 +2109,152 @@ int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int tra
         CK(cudaStreamSynchronize(0));
         if (tensor_cores && v2g::tc_gemm_status(true) != 0)
             return v2g::fail(V2G_ERR_CUDA, "a tensor-core GEMM pipeline wait ran out");
+        return V2G_OK;
+    });
+}
+
+// ---- learned warm start (warmstart.cu) --------------------------------------
+
+namespace {
+// the all-active C1 singlet the warm start works on
+int ws_check(const Problem& P) {
+    if (P.hmat.empty()) return v2g::fail(V2G_ERR_UNSUPPORTED, "the learned warm start needs an all-active C1 space "
+                                                              "with integrals (v2g_set_hamiltonian)");
+    if (P.L.na != P.L.nb) return v2g::fail(V2G_ERR_UNSUPPORTED, "the learned warm start is built for singlets");
+    return V2G_OK;
+}
+}  // namespace
+
+int v2g_ws_create(int hidden, int device, unsigned long long seed, v2g_warmstart** out) {
+    return v2g::guarded([&]() -> int {
+        if (!out || hidden < 8 || hidden > 1024) return v2g::fail(V2G_ERR_ARG, "hidden width must be in 8..1024");
+        *out = nullptr;
+        v2g::require_device();
+        v2g::DeviceScope scope(device);
+        v2g::ws_create(hidden, device, seed, out);
+        return V2G_OK;
+    });
+}
+
+void v2g_ws_destroy(v2g_warmstart* w) {
+    if (w) v2g::ws_destroy(w);
+}
+
+long v2g_ws_num_params(const v2g_warmstart* w) { return w ? (long)v2g::ws_num_params(w) : -1; }
+
+int v2g_ws_get_params(const v2g_warmstart* w, float* params) {
+    return v2g::guarded([&]() -> int {
+        if (!w || !params) return v2g::fail(V2G_ERR_ARG, "null argument");
+        v2g::ws_get_params(w, params);
+        return V2G_OK;
+    });
+}
+
+int v2g_ws_set_params(v2g_warmstart* w, const float* params) {
+    return v2g::guarded([&]() -> int {
+        if (!w || !params) return v2g::fail(V2G_ERR_ARG, "null argument");
+        v2g::ws_set_params(w, params);
+        return V2G_OK;
+    });
+}
+
+long v2g_ws_rows(const v2g_handle* h) { return h ? (long)h->P.L.amo * (h->P.L.amo + 1) / 2 : -1; }
+
+int v2g_ws_features(const v2g_handle* h, float* features) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !features) return v2g::fail(V2G_ERR_ARG, "null argument");
+        const Problem& P = h->P;
+        if (int e = ws_check(P)) return e;
+        v2g::ws_features(P.L.amo, P.L.na, P.hmat.data(), P.Lq.data(), P.nq, features);
+        return V2G_OK;
+    });
+}
+
+int v2g_ws_targets(const v2g_handle* h, float* targets) {
+    return v2g::guarded([&]() -> int {
+        if (!h || !targets) return v2g::fail(V2G_ERR_ARG, "null argument");
+        const Problem& P = h->P;
+        if (int e = ws_check(P)) return e;
+        const v2g::Layout& L = P.L;
+        const int n = L.amo;
+        const int64_t d1 = L.off[v2g::F_D1A][0], d2 = L.off[v2g::F_D2AB][0];
+        const int64_t gab = L.gems_ab[0];
+        int r = 0;
+        for (int p = 0; p < n; p++)
+            for (int q = p; q < n; q++, r++) {
+                const int g = L.ab(0, p, q);
+                targets[r * v2g::kWsOut + 0] = (float)P.x[d1 + (int64_t)p * n + q];
+                targets[r * v2g::kWsOut + 1] = (float)P.x[d2 + (int64_t)g * gab + g];
+                targets[r * v2g::kWsOut + 2] = (float)std::log(P.mu);
+            }
+        return V2G_OK;
+    });
+}
+
+int v2g_ws_forward(v2g_warmstart* w, long rows, const float* features, float* out) {
+    return v2g::guarded([&]() -> int {
+        if (!w || rows < 1 || !features || !out) return v2g::fail(V2G_ERR_ARG, "bad forward arguments");
+        v2g::ws_forward(w, rows, features, out);
+        return V2G_OK;
+    });
+}
+
+int v2g_ws_gradient(v2g_warmstart* w, long rows, const float* features, const float* targets, double* loss,
+                    float* grad) {
+    return v2g::guarded([&]() -> int {
+        if (!w || rows < 1 || !features || !targets) return v2g::fail(V2G_ERR_ARG, "bad gradient arguments");
+        const double l = v2g::ws_gradient(w, rows, features, targets, grad);
+        if (loss) *loss = l;
+        return V2G_OK;
+    });
+}
+
+int v2g_ws_train(v2g_warmstart* w, long rows, const float* features, const float* targets, int epochs,
+                 int batch_rows, float lr, double* loss) {
+    return v2g::guarded([&]() -> int {
+        if (!w || rows < 1 || !features || !targets || epochs < 1 || batch_rows < 1 || !(lr > 0.f))
+            return v2g::fail(V2G_ERR_ARG, "bad training arguments");
+        const double l = v2g::ws_train(w, rows, features, targets, epochs, batch_rows, lr);
+        if (loss) *loss = l;
+        return V2G_OK;
+    });
+}
+
+int v2g_ws_propose(v2g_warmstart* w, v2g_handle* h) {
+    return v2g::guarded([&]() -> int {
+        if (!w || !h) return v2g::fail(V2G_ERR_ARG, "null argument");
+        Problem& P = h->P;
+        if (int e = ws_check(P)) return e;
+        const v2g::Layout& L = P.L;
+        const int n = L.amo;
+        const long rows = (long)n * (n + 1) / 2;
+        std::vector<float> feat((size_t)rows * v2g::kWsFeatures), out((size_t)rows * v2g::kWsOut);
+        v2g::ws_features(n, L.na, P.hmat.data(), P.Lq.data(), P.nq, feat.data());
+        v2g::ws_forward(w, rows, feat.data(), out.data());
+        std::fill(P.x.begin(), P.x.end(), 0.0);
+        std::fill(P.y.begin(), P.y.end(), 0.0);
+        std::fill(P.z.begin(), P.z.end(), 0.0);
+        const int64_t gab = L.gems_ab[0];
+        double lmu = 0.0;
+        int r = 0;
+        for (int p = 0; p < n; p++)
+            for (int q = p; q < n; q++, r++) {
+                const double gam = out[r * v2g::kWsOut + 0], d2 = out[r * v2g::kWsOut + 1];
+                lmu += out[r * v2g::kWsOut + 2];
+                for (int f : {v2g::F_D1A, v2g::F_D1B}) {
+                    P.x[L.off[f][0] + (int64_t)p * n + q] = gam;
+                    P.x[L.off[f][0] + (int64_t)q * n + p] = gam;
+                }
+                for (int f : {v2g::F_Q1A, v2g::F_Q1B}) {
+                    P.x[L.off[f][0] + (int64_t)p * n + q] = (p == q ? 1.0 : 0.0) - gam;
+                    P.x[L.off[f][0] + (int64_t)q * n + p] = (p == q ? 1.0 : 0.0) - gam;
+                }
+                const int g1 = L.ab(0, p, q), g2 = L.ab(0, q, p);
+                P.x[L.off[v2g::F_D2AB][0] + (int64_t)g1 * gab + g1] = d2;
+                P.x[L.off[v2g::F_D2AB][0] + (int64_t)g2 * gab + g2] = d2;
+            }
+        P.mu = std::min(10.0, std::max(0.1, std::exp(lmu / rows)));
+        P.proposal = true;
         return V2G_OK;
     });
 }

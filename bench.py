@@ -307,12 +307,10 @@ def run_gpu(args):
         t = torch.tensor([float(launches), h2d, d2h, float(n_conv)], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         launches, h2d, d2h, n_conv = int(t[0]), float(t[1]), float(t[2]), int(t[3])
-        # per-instance results of every rank reach rank 0 (energies, statuses, iterations)
-        gathered = [None] * world
-        dist.all_gather_object(gathered, [(mine[k], r["e_total"], r["status"], r["oiter"])
-                                          for k, r in enumerate(results)])
-    else:
-        gathered = [[(mine[k], r["e_total"], r["status"], r["oiter"]) for k, r in enumerate(results)]]
+    # per-instance results of every rank reach rank 0 (energies, statuses, iterations)
+    from v2rdm_casscf_b200.shard import gather_results
+
+    allres = gather_results(mine, results, world, dist if world > 1 else None)
     pk, pk_kind = peaks()
     out = {
         "metric": METRIC,
@@ -349,7 +347,6 @@ def run_gpu(args):
     }
     if clocks:
         out["clocks"] = clocks
-    allres = sorted(sum(gathered, []))
     if rank == 0:
         its = [int(r["oiter"]) for r in results]
         out["outer_iterations"] = {"max": max(its), "median": float(np.median(its)), "total": int(sum(its))}

@@ -53,7 +53,12 @@ def _rank(rank, world, port, out):
         dist.all_gather_object(got, mine)
         t = torch.tensor([float(len(mine)) + 0.5 * rank], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        out.put((rank, parts, got, float(t[0])))
+        # stub per-instance results, gathered the way bench.py gathers the solves'
+        from v2rdm_casscf_b200.shard import gather_results
+
+        stub = [dict(e_total=-1.5 * i, status=0 if i % 5 else -3, oiter=100 + i) for i in mine]
+        allres = gather_results(mine, stub, world, dist)
+        out.put((rank, parts, got, float(t[0]), allres))
     finally:
         dist.destroy_process_group()
 
@@ -73,8 +78,10 @@ def test_two_gloo_ranks_agree_and_cover_everything():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    res.sort()
-    (_, parts0, got0, m0), (_, parts1, got1, m1) = res
+    res.sort(key=lambda r: r[0])
+    (_, parts0, got0, m0, all0), (_, parts1, got1, m1, all1) = res
     assert parts0 == parts1 == got0 == got1
     assert sorted(parts0[0] + parts0[1]) == list(range(24))
     assert m0 == m1 == max(len(parts0[0]), len(parts0[1]) + 0.5)
+    # every instance's result reached both ranks, in instance order
+    assert all0 == all1 == [(i, -1.5 * i, 0 if i % 5 else -3, 100 + i) for i in range(24)]

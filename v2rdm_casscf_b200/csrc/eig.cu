@@ -68,7 +68,10 @@ __device__ double block_sum(double v, double* red) {
 // classical threshold criterion, which a relative off-norm test near the
 // rounding floor would never reach) or after max_sweeps.  On return V holds
 // the eigenvectors as columns and diag(A) the eigenvalues.
-__device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double rot_eps) {
+// With init_v = false, V already holds an orthogonal matrix (the previous
+// eigenvectors of a warm start) and the rotations accumulate onto it.
+__device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double rot_eps, bool init_v = true,
+                            double abs_tol = 0.0) {
     __shared__ double rc[kJ / 2], rs[kJ / 2];
     __shared__ int rp[kJ / 2], rq[kJ / 2];
     __shared__ double red[33];
@@ -76,7 +79,8 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
     const int tid = threadIdx.x, nt = blockDim.x;
     const int Ne = N + (N & 1);
     const int npairs = Ne / 2;
-    for (int i = tid; i < N * N; i += nt) V[(i / N) * kLd + (i % N)] = (i / N == i % N) ? 1.0 : 0.0;
+    if (init_v)
+        for (int i = tid; i < N * N; i += nt) V[(i / N) * kLd + (i % N)] = (i / N == i % N) ? 1.0 : 0.0;
     __syncthreads();
     if (N < 2) return;
     double tot = 0.0;
@@ -84,7 +88,7 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
         const double a = A[(i / N) * kLd + (i % N)];
         tot += a * a;
     }
-    const double floor_abs = 1e-17 * sqrt(block_sum(tot, red));
+    const double floor_abs = fmax(1e-17 * sqrt(block_sum(tot, red)), abs_tol);
     for (int sweep = 0; sweep < max_sweeps; sweep++) {
         if (tid == 0) rotated = 0;
         __syncthreads();
@@ -147,14 +151,22 @@ constexpr double kJacobiRotEps = 1e-15;
 constexpr int kJacobiSweeps = 20;
 constexpr int kPairSweeps = 1;
 
+// vsave (optional): the block's eigenvectors, n x n at t.woff, kept across
+// outer iterations.  With warm set, the Jacobi starts from them: A <- V^T U V
+// (nearly diagonal once the iteration settles, so one to three sweeps
+// converge it instead of ~10 from the identity) and the rotations accumulate
+// onto V.  Without warm the Jacobi starts from V = I; vsave is written either way.
 __global__ void __launch_bounds__(kJThreads) small_project_kernel(const BlockTask* __restrict__ tasks, int B,
                                                                   const double* __restrict__ aty,
                                                                   const double* __restrict__ c, double* x, double* z,
                                                                   const double* __restrict__ mu,
-                                                                  const int* __restrict__ mask) {
+                                                                  const int* __restrict__ mask,
+                                                                  double* __restrict__ vsave, int warm,
+                                                                  const double* __restrict__ stol) {
     extern __shared__ double sm[];
     double* A = sm;
     double* V = sm + kJ * kLd;
+    double* T = sm + 2 * kJ * kLd;  // only with vsave (the launch then has room for it)
     const BlockTask t = tasks[blockIdx.x];
     const int b = t.inst;
     if (mask && !mask[b]) return;
@@ -168,9 +180,44 @@ __global__ void __launch_bounds__(kJThreads) small_project_kernel(const BlockTas
         const double t2 = (aty[e2] - c[e2]) + m * x[e2];
         A[p * kLd + q] = 0.5 * (t1 + t2);
     }
+    const bool use_warm = vsave && warm;
+    if (use_warm) {
+        const double* vs = vsave + t.woff;
+        for (int i = threadIdx.x; i < N * N; i += blockDim.x) V[(i / N) * kLd + (i % N)] = vs[i];
+        __syncthreads();
+        // T = A V, then A = V^T T (symmetrised)
+        for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+            const int p = i / N, q = i % N;
+            double acc = 0.0;
+            for (int k = 0; k < N; k++) acc += A[p * kLd + k] * V[k * kLd + q];
+            T[p * kLd + q] = acc;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+            const int p = i / N, q = i % N;
+            double acc = 0.0;
+            for (int k = 0; k < N; k++) acc += V[k * kLd + p] * T[k * kLd + q];
+            A[p * kLd + q] = acc;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+            const int p = i / N, q = i % N;
+            if (p < q) {
+                const double v = 0.5 * (A[p * kLd + q] + A[q * kLd + p]);
+                A[p * kLd + q] = v;
+                A[q * kLd + p] = v;
+            }
+        }
+    }
     __syncthreads();
-    jacobi_smem(A, V, N, kJacobiSweeps, kJacobiRotEps);
+    // with stol, off-diagonal entries below the instance's share of the
+    // adaptive tolerance are left (x and z stay PSD; the residual is bounded)
+    jacobi_smem(A, V, N, kJacobiSweeps, kJacobiRotEps, !use_warm, stol ? stol[b] : 0.0);
     __syncthreads();
+    if (vsave) {
+        double* vs = vsave + t.woff;
+        for (int i = threadIdx.x; i < N * N; i += blockDim.x) vs[i] = V[(i / N) * kLd + (i % N)];
+    }
     for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
         const int p = i / N, q = i % N;
         double sx = 0.0, sz = 0.0;
@@ -914,6 +961,7 @@ __global__ void write_xz_kernel(const BlockTask* __restrict__ tasks, int B, cons
 }
 
 constexpr size_t kJacobiSmem = 2 * kJ * kLd * sizeof(double);
+constexpr size_t kJacobiWarmSmem = 3 * kJ * kLd * sizeof(double);  // + the T of a warm start
 
 // The 66,560 B of dynamic shared memory of the Jacobi kernels need an opt-in
 // per kernel and per device.  Each device is set up once; a failed attempt is
@@ -926,7 +974,7 @@ void set_smem_attrs() {
     std::lock_guard<std::mutex> lk(mu);
     if ((size_t)dev < done.size() && done[dev]) return;
     bool ok = cudaFuncSetAttribute(small_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kJacobiSmem) == cudaSuccess;
+                                   (int)kJacobiWarmSmem) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(bj_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kJacobiSmem) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(bj_update_wv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -939,10 +987,12 @@ void set_smem_attrs() {
 }  // namespace
 
 void launch_small_project(const BlockTask* tasks, int ntasks, int B, const double* aty, const double* c, double* x,
-                          double* z, const double* mu, const int* mask, cudaStream_t s) {
+                          double* z, const double* mu, const int* mask, cudaStream_t s, double* vsave, bool warm,
+                          const double* stol) {
     if (ntasks == 0) return;
     set_smem_attrs();
-    small_project_kernel<<<ntasks, kJThreads, kJacobiSmem, s>>>(tasks, B, aty, c, x, z, mu, mask);
+    small_project_kernel<<<ntasks, kJThreads, vsave ? kJacobiWarmSmem : kJacobiSmem, s>>>(
+        tasks, B, aty, c, x, z, mu, mask, vsave, warm ? 1 : 0, stol);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

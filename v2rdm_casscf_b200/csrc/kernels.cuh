@@ -152,8 +152,13 @@ struct BlockTask {
 };
 
 // Blocks with n <= 64: form U, diagonalise in shared memory, write x and z.
+// vsave (optional) keeps each block's eigenvectors (n x n at task.woff)
+// across calls; warm starts the Jacobi from them.  stol (optional, per
+// instance): off-diagonal entries below it are not rotated away (the
+// adaptive projection's tolerance share).
 void launch_small_project(const BlockTask* tasks, int ntasks, int B, const double* aty, const double* c, double* x,
-                          double* z, const double* mu, const int* mask, cudaStream_t s);
+                          double* z, const double* mu, const int* mask, cudaStream_t s, double* vsave = nullptr,
+                          bool warm = false, const double* stol = nullptr);
 
 // Large blocks (n > 64), block Jacobi on a padded np x np workspace.
 // U = sym(A^T y - c + mu x), zero padded.

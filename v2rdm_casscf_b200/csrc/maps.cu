@@ -50,8 +50,9 @@ __device__ __forceinline__ Chunk chunk_of(int64_t nrows, int B) {
     return c;
 }
 
-// Per-instance block partial of v, written to partial[block * B + b].
-__device__ __forceinline__ void block_partial(double v, int B, double* __restrict__ partial) {
+// Per-instance block partial of v, written to partial[slot * B + b] (slot is
+// the block's index among the partial sums, not always blockIdx.x).
+__device__ __forceinline__ void block_partial(double v, int B, double* __restrict__ partial, int64_t slot) {
     __shared__ double sh[kThreads];
     sh[threadIdx.x] = v;
     __syncthreads();
@@ -59,7 +60,7 @@ __device__ __forceinline__ void block_partial(double v, int B, double* __restric
         const int rows_per_pass = blockDim.x / B;
         double s = 0.0;
         for (int k = 0; k < rows_per_pass; k++) s += sh[threadIdx.x + k * B];
-        partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
+        partial[slot * B + threadIdx.x] = s;
     }
 }
 
@@ -166,10 +167,42 @@ __device__ __forceinline__ void chunk_range(int B, int nchunk, int ch, int& b0, 
     }
 }
 
+// Long rows: one CTA per row; thread t sums entries k = t / B, t / B + T / B,
+// ... for instance t % B, then a fixed-order reduction per instance.  Run by
+// the CTAs of ell_kernel past its row tiles (one launch per map).
+__device__ __forceinline__ void long_row(const DevMap& M, int B, const double* __restrict__ in, const Epi& e,
+                                         const int* __restrict__ mask, double* __restrict__ partial,
+                                         int partial_base, int lr) {
+    __shared__ double shl[kThreads];
+    const int lanes = blockDim.x / B;
+    const int b = threadIdx.x % B;
+    const int l = threadIdx.x / B;
+    const int r = M.long_rows[lr];
+    const int k0 = M.long_ptr[lr], k1 = M.long_ptr[lr + 1];
+    double s = 0.0;
+    if (threadIdx.x < lanes * B)
+        for (int k = k0 + l; k < k1; k += lanes) s += M.long_val[k] * in[(int64_t)M.long_col[k] * B + b];
+    shl[threadIdx.x] = s;
+    __syncthreads();
+    double acc = 0.0;
+    if (threadIdx.x < B) {
+        double t = 0.0;
+        for (int q = 0; q < lanes; q++) t += shl[threadIdx.x + q * B];
+        if (!(mask && !mask[threadIdx.x])) acc = epilogue(e, r, B, threadIdx.x, t);
+    }
+    __syncthreads();
+    if (partial) block_partial(threadIdx.x < B ? acc : 0.0, B, partial, (int64_t)partial_base + lr);
+}
+
 template <int CH, bool STREAM>
 __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in,
                                                        Epi e, const int* __restrict__ mask,
                                                        double* __restrict__ partial) {
+    const int ntiles = bl.start[M.nb];
+    if ((int)blockIdx.x >= ntiles * bl.nchunk) {
+        long_row(M, B, in, e, mask, partial, ntiles, blockIdx.x - ntiles * bl.nchunk);
+        return;
+    }
     const int tile = blockIdx.x / bl.nchunk;
     const int ch = blockIdx.x % bl.nchunk;
     int bi = 0;
@@ -216,31 +249,6 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int 
         for (int w = 0; w < kThreads / 32; w++) t += sh[w][threadIdx.x];
         partial[(int64_t)tile * B + b0 + threadIdx.x] = t;
     }
-}
-
-// Long rows: one CTA per row; thread t sums entries k = t / B, t / B + T / B,
-// ... for instance t % B, then a fixed-order reduction per instance.
-__global__ void long_kernel(DevMap M, int B, const double* __restrict__ in, Epi e, const int* __restrict__ mask,
-                            double* __restrict__ partial, int partial_base) {
-    __shared__ double sh[kThreads];
-    const int lanes = blockDim.x / B;
-    const int b = threadIdx.x % B;
-    const int l = threadIdx.x / B;
-    const int r = M.long_rows[blockIdx.x];
-    const int k0 = M.long_ptr[blockIdx.x], k1 = M.long_ptr[blockIdx.x + 1];
-    double s = 0.0;
-    if (threadIdx.x < lanes * B)
-        for (int k = k0 + l; k < k1; k += lanes) s += M.long_val[k] * in[(int64_t)M.long_col[k] * B + b];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    double acc = 0.0;
-    if (threadIdx.x < B) {
-        double t = 0.0;
-        for (int q = 0; q < lanes; q++) t += sh[threadIdx.x + q * B];
-        if (!(mask && !mask[threadIdx.x])) acc = epilogue(e, r, B, threadIdx.x, t);
-    }
-    __syncthreads();
-    if (partial) block_partial(threadIdx.x < B ? acc : 0.0, B, partial + (int64_t)partial_base * B);
 }
 
 // Stage 1: block g reduces a contiguous chunk of elements for every instance;
@@ -518,7 +526,7 @@ __global__ void cg_update_yr_kernel(int64_t n, int B, double* __restrict__ y, do
             acc += rv * rv;
         }
     }
-    block_partial(acc, B, partial);
+    block_partial(acc, B, partial, blockIdx.x);
 }
 
 // y += alpha p ; r -= alpha Ap with alpha = r.r / p.Ap computed by every
@@ -549,7 +557,7 @@ __global__ void cg_step_yr_kernel(int64_t n, int B, double* __restrict__ y, doub
             acc += rv * rv;
         }
     }
-    block_partial(acc, B, partial);
+    block_partial(acc, B, partial, blockIdx.x);
 }
 
 // One block per instance: r.r from the step kernel's partials (fixed tree),
@@ -698,22 +706,20 @@ static int run_map(const DevMap& M, int B, const double* in, double* out, const 
                    const double* add, const int* mask, const double* dotv, double* partial, cudaStream_t s) {
     Epi e{sub, coef, add, dotv, out};
     const Blocks bl = map_blocks(M, B);
-    if (M.nb > 0) {
-        // with 8 or more instances the table loads and the output stores are
-        // streamed past L1/L2 (cache-streaming hints), leaving the caches to
-        // the gathered input: 7 % faster at n = 17..20 on B200, slower for
-        // single instances
-        const int g = bl.start[M.nb] * bl.nchunk;
+    if (M.nb > 0 || M.nlong > 0) {
+        // one launch: the row tiles of the ELL buckets (times the instance
+        // chunks), then one CTA per long row.  Variants: with 8 or more
+        // instances the table loads and the output stores are streamed past
+        // L1/L2 (cache-streaming hints), leaving the caches to the gathered
+        // input (7 % faster at n = 17..20 on B200, slower for single
+        // instances); the autotuner of each layout group picks per map
+        const int g = bl.start[M.nb] * bl.nchunk + M.nlong;
         switch (map_variant(M, B)) {
             case 0: ell_kernel<2, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
             case 1: ell_kernel<4, false><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
             case 2: ell_kernel<4, true><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
             default: ell_kernel<8, true><<<g, kThreads, 0, s>>>(M, bl, B, in, e, mask, partial); break;
         }
-        g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    }
-    if (M.nlong > 0) {
-        long_kernel<<<M.nlong, kThreads, 0, s>>>(M, B, in, e, mask, partial, bl.start[M.nb]);
         g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     }
     return bl.start[M.nb] + M.nlong;  // partial blocks written

@@ -266,6 +266,9 @@ namespace {
 // blocks' dense products on the tensor cores (FP32 accuracy, ~1e-6 relative,
 // is then two orders below what the projection has to deliver).
 constexpr double kMixedRho = 1e-5;
+// Smallest padded block whose products go to the tensor cores in the mixed
+// phase (dimension > 448: G2aa from n = 15 on, the DQGT2 blocks, H50's blocks).
+constexpr int kMixedMinNp = 512;
 
 // Lock-step solve of B instances that share one layout.
 class GroupRun {
@@ -377,10 +380,17 @@ class GroupRun {
     // are positive semidefinite either way.
     // mixed = true runs the large blocks' dense products on the tensor cores.
     void project(const std::vector<double>& rho = {}, bool mixed = false) {
-        tc_ = mixed && nlarge_ > 0;
+        tc_ = mixed && ntc_gtiles_ > 0;
         if (tc_) tc_projections_++;
         launch_spmv(mAT_, B_, y_.p, aty_.p, nullptr, nullptr, nullptr, mask_.p, s_);
-        launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_);
+        // the small blocks start from their previous eigenvectors, except in
+        // the first projection, after a cold restart and every kSmallCold-th
+        // projection (so that rounding in the kept eigenvectors cannot build up)
+        const bool small_warm = small_warm_ && (nproj_ % kSmallCold) != 0;
+        launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_, vsmall_.p,
+                             small_warm);
+        small_warm_ = true;
+        nproj_++;
         if (nlarge_ == 0) return;
         launch_form_u(large_d_.p, nlarge_, max_np_, B_, aty_.p, c_.p, x_.p, mu_.p, mask_.p, U_.p, s_);
         set_block_masks();  // bact_ = blocks of active instances
@@ -577,7 +587,8 @@ class GroupRun {
                         ycount[b] = 0;
                         aa.restart(b);
                     }
-                warm_ = false;  // every large block of the group starts its projection cold again
+                warm_ = false;  // every block of the group starts its projection cold again
+                small_warm_ = false;
             }
             int nactive = 0;
             for (int b = 0; b < B_; b++) nactive += active[b];
@@ -1015,17 +1026,23 @@ class GroupRun {
     // The projection's dense products: on all tiles of C (full) or on the
     // upper tiles of a symmetric C (sym, mirrored afterwards), in FP64 or, in
     // the mixed-precision phase (tc_), as 3xTF32 products on the tensor cores.
+    // In the mixed phase only blocks padded to kMixedMinNp or more go to the
+    // tensor cores; smaller ones gain nothing there (a few tiles each) and stay FP64.
     void gemm_full(const double* A, bool ta, const double* Bm, bool tb, const double* d, double* C, const int* mask) {
-        if (tc_)
+        if (tc_) {
             launch_tc_gemm(large_d_.p, tc_gtiles_.p, ntc_gtiles_, A, ta, Bm, tb, d, C, mask, s_);
-        else
+            launch_gemm(large_d_.p, lo_gtiles_.p, nlo_gtiles_, A, ta, Bm, tb, d, C, mask, s_);
+        } else {
             launch_gemm(large_d_.p, gtiles_.p, ngtiles_, A, ta, Bm, tb, d, C, mask, s_);
+        }
     }
     void gemm_sym(const double* A, bool ta, const double* Bm, bool tb, const double* d, double* C, const int* mask) {
-        if (tc_)
+        if (tc_) {
             launch_tc_gemm(large_d_.p, tc_stiles_.p, ntc_stiles_, A, ta, Bm, tb, d, C, mask, s_);
-        else
+            launch_gemm(large_d_.p, lo_stiles_.p, nlo_stiles_, A, ta, Bm, tb, d, C, mask, s_);
+        } else {
             launch_gemm(large_d_.p, stiles_.p, nstiles_, A, ta, Bm, tb, d, C, mask, s_);
+        }
     }
 
     // CG map launch with optional CUDA-event timing (profile mode).
@@ -1150,7 +1167,7 @@ class GroupRun {
     void build_projection_plan() {
         const Layout& L = T_.L;
         std::vector<BlockTask> small;
-        int64_t woff = 0, qoff = 0, doff = 0;
+        int64_t woff = 0, qoff = 0, doff = 0, soff = 0;
         for (int b = 0; b < B_; b++)
             for (size_t k = 0; k < L.block_dims.size(); k++) {
                 const int n = L.block_dims[k];
@@ -1160,6 +1177,8 @@ class GroupRun {
                 t.n = n;
                 t.inst = b;
                 if (n <= 64) {
+                    t.woff = soff;  // its kept eigenvectors
+                    soff += (int64_t)n * n;
                     small.push_back(t);
                     continue;
                 }
@@ -1176,6 +1195,7 @@ class GroupRun {
         nsmall_ = (int)small.size();
         nlarge_ = (int)hlarge_.size();
         small_d_.upload(small.data(), small.size());
+        vsmall_.alloc(std::max<int64_t>(soff, 1));
         large_d_.upload(hlarge_.data(), hlarge_.size());
         if (nlarge_ == 0) return;
         U_.alloc(woff);
@@ -1232,9 +1252,19 @@ class GroupRun {
         stiles_.upload(st.data(), st.size());
         // 128 x 64 tiles of the tensor-core GEMM; the symmetric products need
         // every 64 x 64 upper tile, i.e. 128-row tile ti with 64-column tile tj >= 2 ti
-        std::vector<GemmTile> tg, ts;
+        // (blocks padded below kMixedMinNp keep FP64 tiles in the mixed phase)
+        std::vector<GemmTile> tg, ts, lg, ls;
         for (int ti = 0; ti < nlarge_; ti++) {
             const BlockTask& t = hlarge_[ti];
+            if (t.np < kMixedMinNp) {
+                const int nt = t.np / 64;
+                for (int i = 0; i < nt; i++)
+                    for (int j = 0; j < nt; j++) {
+                        lg.push_back({ti, i, j});
+                        if (i <= j) ls.push_back({ti, i, j});
+                    }
+                continue;
+            }
             const int nr = (t.np + 127) / 128, nc = t.np / 64;
             for (int i = 0; i < nr; i++)
                 for (int j = 0; j < nc; j++) {
@@ -1244,8 +1274,12 @@ class GroupRun {
         }
         tc_gtiles_.upload(tg.data(), tg.size());
         tc_stiles_.upload(ts.data(), ts.size());
+        lo_gtiles_.upload(lg.data(), lg.size());
+        lo_stiles_.upload(ls.data(), ls.size());
         ntc_gtiles_ = (int)tg.size();
         ntc_stiles_ = (int)ts.size();
+        nlo_gtiles_ = (int)lg.size();
+        nlo_stiles_ = (int)ls.size();
         nstiles_ = (int)st.size();
         pairs_.upload(pt.data(), pt.size());
         wtiles_.upload(wt.data(), wt.size());
@@ -1295,8 +1329,8 @@ class GroupRun {
     long restarts_ = 0;
     bool cap_ = false;
     long oa_sweeps_ = 0, jacobi_blocks_ = 0;
-    DevBuf<GemmTile> gtiles_, stiles_, tc_gtiles_, tc_stiles_;
-    int ntc_gtiles_ = 0, ntc_stiles_ = 0;
+    DevBuf<GemmTile> gtiles_, stiles_, tc_gtiles_, tc_stiles_, lo_gtiles_, lo_stiles_;
+    int ntc_gtiles_ = 0, ntc_stiles_ = 0, nlo_gtiles_ = 0, nlo_stiles_ = 0;
     bool tc_ = false;  // this projection's dense products on the tensor cores
     long tc_projections_ = 0;
     DevBuf<PairTask> pairs_;
@@ -1304,6 +1338,11 @@ class GroupRun {
     DevBuf<VTileTask> vtiles_;
     int ngtiles_ = 0, nstiles_ = 0, npairs_ = 0, nwtiles_ = 0, nvtiles_ = 0;
     bool warm_ = false;
+    // kept eigenvectors of the small blocks (warm Jacobi starts)
+    static constexpr long kSmallCold = 64;
+    DevBuf<double> vsmall_;
+    bool small_warm_ = false;
+    long nproj_ = 0;
     long sweeps_total_ = 0;
     // the captured CG chunk
     cudaGraphExec_t cg_exec_ = nullptr;

@@ -55,3 +55,16 @@ def workload_costs(spaces, options=None):
             cache[key] = instance_cost(s.dimx, s.nconstraints, s.dimensions)
         out.append(cache[key])
     return out
+
+
+def gather_results(mine, results, world, dist=None):
+    """Per-instance results of every rank, on every rank, sorted by instance:
+    [(instance, e_total, status, oiter), ...].  ``results`` are this rank's
+    result dicts in the order of ``mine``; with world > 1 the lists travel by
+    ``dist.all_gather_object`` (NCCL on GPUs, gloo in the CPU tests)."""
+    local = [(int(i), float(r["e_total"]), int(r["status"]), int(r["oiter"])) for i, r in zip(mine, results)]
+    if world <= 1 or dist is None:
+        return sorted(local)
+    got = [None] * world
+    dist.all_gather_object(got, local)
+    return sorted(x for part in got for x in part)

@@ -149,6 +149,7 @@ struct BlockTask {
     int nb;         // number of 32-wide column blocks (np / 32)
     int64_t qoff;   // offset of the pair-rotation buffer (large blocks)
     int64_t doff;   // offset of the np-long weight vector (large blocks)
+    int64_t toff;   // offset (32-bit words) of the split TF32 operands (tensor-core blocks)
 };
 
 // Blocks with n <= 64: form U, diagonalise in shared memory, write x and z.
@@ -176,10 +177,27 @@ struct GemmTile {
 void launch_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
                  const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s);
 // The same product on the tensor cores (tcgen05, 3xTF32 split, FP32
-// accumulation: FP32 accuracy) over 128 x 64 tiles of C: tile (ti, tj) covers
-// rows 128 ti.. and columns 64 tj..; rows past np are not written.
-void launch_tc_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
-                    const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s);
+// accumulation: FP32 accuracy) over 128 x 128 tiles of C: tile (ti, tj)
+// covers rows 128 ti.. and columns 128 tj..; rows and columns past np are not
+// written.  The operands are first split into TF32 pairs in the MMA's shared
+// memory layout, one unit (task, 128-row block) per CTA, into the plan's
+// workspaces wa and wb (tc_split_words(np) words per task, at task.toff).
+struct TcSplit {
+    int task, rb;
+};
+struct TcPlan {
+    const BlockTask* tasks = nullptr;
+    const GemmTile* tiles_full = nullptr;  // every 128 x 128 tile
+    const GemmTile* tiles_sym = nullptr;   // tiles ti <= tj (symmetric products, mirrored afterwards)
+    int n_full = 0, n_sym = 0;
+    const TcSplit* split = nullptr;
+    int nsplit = 0;
+    uint32_t* wa = nullptr;
+    uint32_t* wb = nullptr;
+};
+int64_t tc_split_words(int np);
+void launch_tc_gemm(const TcPlan& plan, bool sym, const double* A, bool transA, const double* Bm, bool transB,
+                    const double* dvec, double* C, const int* bmask, cudaStream_t s);
 // 0 while every tensor-core GEMM's pipeline waits ended; 1 after one ran out
 // (that launch's result is invalid); reset clears the flag.
 int tc_gemm_status(bool reset);

@@ -415,7 +415,10 @@ class GroupRun {
     // Ogita-Aishima sweeps from the previous eigenvectors; blocks with a hard
     // pair or without convergence after kMaxOa sweeps go to block Jacobi.
     void refine() {
-        constexpr int kMaxOa = 6;
+        // in the mixed phase the products carry FP32 rounding, so the refinement's
+        // residual floor is FP32's: a few sweeps, and blocks that stop above the
+        // (loose) tolerance are accepted as they are instead of going to Jacobi
+        const int kMaxOa = tc_ ? 3 : 6;
         CK(cudaMemcpyAsync(bref_.p, bact_.p, nlarge_ * sizeof(int), cudaMemcpyDeviceToDevice, s_));
         CK(cudaMemsetAsync(bjac_.p, 0, nlarge_ * sizeof(int), s_));
         CK(cudaMemsetAsync(restart_.p, 0, nlarge_ * sizeof(int), s_));
@@ -442,7 +445,7 @@ class GroupRun {
             oa_sweeps_++;
         }
         // blocks still unconverged join the Jacobi set (their OA update was applied)
-        if (nref > 0) launch_merge_mask(nlarge_, bref_.p, bjac_.p, s_);
+        if (nref > 0 && !tc_) launch_merge_mask(nlarge_, bref_.p, bjac_.p, s_);
         launch_count(nlarge_, bjac_.p, nact_.p + 3, s_);
         // blocks whose eigenvectors degraded restart cold (V = I, W = U) and
         // converge fully; they leave the refinement and warm Jacobi sets
@@ -1030,7 +1033,7 @@ class GroupRun {
     // tensor cores; smaller ones gain nothing there (a few tiles each) and stay FP64.
     void gemm_full(const double* A, bool ta, const double* Bm, bool tb, const double* d, double* C, const int* mask) {
         if (tc_) {
-            launch_tc_gemm(large_d_.p, tc_gtiles_.p, ntc_gtiles_, A, ta, Bm, tb, d, C, mask, s_);
+            launch_tc_gemm(tc_plan_, false, A, ta, Bm, tb, d, C, mask, s_);
             launch_gemm(large_d_.p, lo_gtiles_.p, nlo_gtiles_, A, ta, Bm, tb, d, C, mask, s_);
         } else {
             launch_gemm(large_d_.p, gtiles_.p, ngtiles_, A, ta, Bm, tb, d, C, mask, s_);
@@ -1038,7 +1041,7 @@ class GroupRun {
     }
     void gemm_sym(const double* A, bool ta, const double* Bm, bool tb, const double* d, double* C, const int* mask) {
         if (tc_) {
-            launch_tc_gemm(large_d_.p, tc_stiles_.p, ntc_stiles_, A, ta, Bm, tb, d, C, mask, s_);
+            launch_tc_gemm(tc_plan_, true, A, ta, Bm, tb, d, C, mask, s_);
             launch_gemm(large_d_.p, lo_stiles_.p, nlo_stiles_, A, ta, Bm, tb, d, C, mask, s_);
         } else {
             launch_gemm(large_d_.p, stiles_.p, nstiles_, A, ta, Bm, tb, d, C, mask, s_);
@@ -1252,10 +1255,15 @@ class GroupRun {
         stiles_.upload(st.data(), st.size());
         // 128 x 64 tiles of the tensor-core GEMM; the symmetric products need
         // every 64 x 64 upper tile, i.e. 128-row tile ti with 64-column tile tj >= 2 ti
-        // (blocks padded below kMixedMinNp keep FP64 tiles in the mixed phase)
+        // 128 x 128 tiles of the tensor-core GEMM (blocks padded to kMixedMinNp or
+        // more); the symmetric products need every 64 x 64 upper tile, which the
+        // 128-tiles ti <= tj cover; blocks below kMixedMinNp keep FP64 tiles in
+        // the mixed phase
         std::vector<GemmTile> tg, ts, lg, ls;
+        std::vector<TcSplit> sp;
+        int64_t toff = 0;
         for (int ti = 0; ti < nlarge_; ti++) {
-            const BlockTask& t = hlarge_[ti];
+            BlockTask& t = hlarge_[ti];
             if (t.np < kMixedMinNp) {
                 const int nt = t.np / 64;
                 for (int i = 0; i < nt; i++)
@@ -1265,21 +1273,39 @@ class GroupRun {
                     }
                 continue;
             }
-            const int nr = (t.np + 127) / 128, nc = t.np / 64;
-            for (int i = 0; i < nr; i++)
-                for (int j = 0; j < nc; j++) {
+            t.toff = toff;
+            toff += tc_split_words(t.np);
+            const int nr = (t.np + 127) / 128;
+            for (int i = 0; i < nr; i++) {
+                sp.push_back({ti, i});
+                for (int j = 0; j < nr; j++) {
                     tg.push_back({ti, i, j});
-                    if (2 * i <= j) ts.push_back({ti, i, j});
+                    if (i <= j) ts.push_back({ti, i, j});
                 }
+            }
+        }
+        if (toff > 0) {
+            large_d_.upload(hlarge_.data(), hlarge_.size());  // with the split offsets
+            tcwa_.alloc(toff);
+            tcwb_.alloc(toff);
         }
         tc_gtiles_.upload(tg.data(), tg.size());
         tc_stiles_.upload(ts.data(), ts.size());
+        tc_split_.upload(sp.data(), sp.size());
         lo_gtiles_.upload(lg.data(), lg.size());
         lo_stiles_.upload(ls.data(), ls.size());
         ntc_gtiles_ = (int)tg.size();
-        ntc_stiles_ = (int)ts.size();
         nlo_gtiles_ = (int)lg.size();
         nlo_stiles_ = (int)ls.size();
+        tc_plan_.tasks = large_d_.p;
+        tc_plan_.tiles_full = tc_gtiles_.p;
+        tc_plan_.tiles_sym = tc_stiles_.p;
+        tc_plan_.n_full = (int)tg.size();
+        tc_plan_.n_sym = (int)ts.size();
+        tc_plan_.split = tc_split_.p;
+        tc_plan_.nsplit = (int)sp.size();
+        tc_plan_.wa = tcwa_.p;
+        tc_plan_.wb = tcwb_.p;
         nstiles_ = (int)st.size();
         pairs_.upload(pt.data(), pt.size());
         wtiles_.upload(wt.data(), wt.size());
@@ -1330,7 +1356,10 @@ class GroupRun {
     bool cap_ = false;
     long oa_sweeps_ = 0, jacobi_blocks_ = 0;
     DevBuf<GemmTile> gtiles_, stiles_, tc_gtiles_, tc_stiles_, lo_gtiles_, lo_stiles_;
-    int ntc_gtiles_ = 0, ntc_stiles_ = 0, nlo_gtiles_ = 0, nlo_stiles_ = 0;
+    int ntc_gtiles_ = 0, nlo_gtiles_ = 0, nlo_stiles_ = 0;
+    DevBuf<TcSplit> tc_split_;
+    DevBuf<uint32_t> tcwa_, tcwb_;  // the split operands of the tensor-core products
+    TcPlan tc_plan_;
     bool tc_ = false;  // this projection's dense products on the tensor cores
     long tc_projections_ = 0;
     DevBuf<PairTask> pairs_;
@@ -2118,7 +2147,8 @@ int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int tra
         v2g::DeviceScope scope(device);
         std::vector<v2g::BlockTask> tasks(nblocks);
         std::vector<v2g::GemmTile> tiles;
-        int64_t woff = 0, doff = 0;
+        std::vector<v2g::TcSplit> split;
+        int64_t woff = 0, doff = 0, toff = 0;
         for (int i = 0; i < nblocks; i++) {
             if (dims[i] < 1 || dims[i] > 16384) return v2g::fail(V2G_ERR_ARG, "block dimension out of range");
             v2g::BlockTask t{};
@@ -2127,20 +2157,43 @@ int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int tra
             t.nb = t.np / 32;
             t.woff = woff;
             t.doff = doff;
+            t.toff = toff;
             woff += (int64_t)t.np * t.np;
             doff += t.np;
+            toff += v2g::tc_split_words(t.np);
             tasks[i] = t;
-            const int nr = tensor_cores ? (t.np + 127) / 128 : t.np / 64, nc = t.np / 64;
-            for (int a = 0; a < nr; a++)
-                for (int b = 0; b < nc; b++) tiles.push_back({i, a, b});
+            if (tensor_cores) {
+                const int nr = (t.np + 127) / 128;
+                for (int a = 0; a < nr; a++) {
+                    split.push_back({i, a});
+                    for (int b = 0; b < nr; b++) tiles.push_back({i, a, b});
+                }
+            } else {
+                const int nt = t.np / 64;
+                for (int a = 0; a < nt; a++)
+                    for (int b = 0; b < nt; b++) tiles.push_back({i, a, b});
+            }
         }
         v2g::DevBuf<v2g::BlockTask> dt;
         v2g::DevBuf<v2g::GemmTile> dg;
+        v2g::DevBuf<v2g::TcSplit> ds;
+        v2g::DevBuf<uint32_t> wa, wb;
         dt.upload(tasks.data(), tasks.size());
         dg.upload(tiles.data(), tiles.size());
         if (tensor_cores) {
+            ds.upload(split.data(), split.size());
+            wa.alloc(toff);
+            wb.alloc(toff);
+            v2g::TcPlan plan;
+            plan.tasks = dt.p;
+            plan.tiles_full = dg.p;
+            plan.n_full = (int)tiles.size();
+            plan.split = ds.p;
+            plan.nsplit = (int)split.size();
+            plan.wa = wa.p;
+            plan.wb = wb.p;
             v2g::tc_gemm_status(true);
-            v2g::launch_tc_gemm(dt.p, dg.p, (int)tiles.size(), A, transA != 0, B, transB != 0, d, C, nullptr, 0);
+            v2g::launch_tc_gemm(plan, false, A, transA != 0, B, transB != 0, d, C, nullptr, 0);
         } else {
             v2g::launch_gemm(dt.p, dg.p, (int)tiles.size(), A, transA != 0, B, transB != 0, d, C, nullptr, 0);
         }

@@ -8,17 +8,22 @@
 // A_hi B_hi + A_hi B_lo + A_lo B_hi accumulated in FP32 (the "3xTF32" split;
 // the dropped A_lo B_lo term and the splits' rounding are ~2^-22 relative).
 //
-// One CTA computes a 128 x 64 tile of C (tcgen05.mma M = 128, N = 64) with
-// its accumulator in tensor memory (64 columns).  The K dimension is walked in
-// chunks of 32 through a two-stage shared-memory ring: all 128 threads load a
-// chunk of A and B from global memory (FP64), split it and store the four
-// TF32 tiles in the canonical K-major layout without swizzle (8-row x 16-byte
-// core matrices), then one thread issues the 12 MMAs of the chunk (4 K steps
-// of 8, three products each) and commits them to the stage's mbarrier, which
-// releases the stage for the chunk after next.  The epilogue reads the
-// accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows)
-// and stores FP64.  Every wait on an mbarrier is bounded; a wait that runs out
-// sets g_tc_status and the CTA still frees its tensor memory and returns.
+// Two kernels per product:
+//   * tc_split_kernel writes each operand once as TF32 (hi, lo) tiles in the
+//     exact byte order the MMA reads from shared memory: K-major, no swizzle,
+//     8-row x 16-byte core matrices, one 128-row x 32-K tile (16 KB) per (row
+//     block, K chunk), hi then lo.  The transposes of op() and the diagonal
+//     scaling happen here (coalesced FP64 reads through shared memory).
+//   * tc_gemm_kernel computes a 128 x 128 tile of C with its accumulator in
+//     tensor memory (128 columns).  A three-stage shared-memory ring is fed by
+//     one producer thread with bulk copies (cp.async.bulk, 32 KB per operand
+//     per stage, completion counted on the stage's mbarrier); one thread
+//     issues the chunk's 12 tcgen05.mma (4 K steps of 8, three products) and
+//     commits them to the stage's "empty" mbarrier; the four warps read the
+//     accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile
+//     rows) and store FP64.
+// Every mbarrier wait is bounded; a wait that runs out sets g_tc_status, and
+// the CTA then drains what it issued (bounded) and frees its tensor memory.
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -29,28 +34,26 @@ namespace v2g {
 
 namespace {
 
-constexpr int kTcM = 128;        // rows of a C tile (MMA M)
-constexpr int kTcN = 64;         // columns of a C tile (MMA N)
-constexpr int kTcK = 32;         // K per pipeline stage
-constexpr int kTcThreads = 128;  // one thread per TMEM lane / tile row
-constexpr int kTileA = kTcM * kTcK * 4;            // bytes of one TF32 A tile (16 KB)
-constexpr int kTileB = kTcN * kTcK * 4;            // bytes of one TF32 B tile (8 KB)
-constexpr int kStage = 2 * kTileA + 2 * kTileB;    // A hi, A lo, B hi, B lo (48 KB)
-constexpr int kTcSmem = 2 * kStage + 128;          // two stages + barriers and the TMEM address
-constexpr long long kWaitLimit = 1ll << 26;        // polls of an mbarrier before giving up
+constexpr int kTcM = 128;                        // rows of a C tile (MMA M)
+constexpr int kTcN = 128;                        // columns of a C tile (MMA N)
+constexpr int kTcK = 32;                         // K per pipeline stage
+constexpr int kTcThreads = 128;                  // four warps: TMEM lanes 0..127
+constexpr int kStages = 3;
+constexpr int kTile = kTcM * kTcK * 4;           // one TF32 tile, 128 rows x 32 K (16 KB)
+constexpr int kOperand = 2 * kTile;              // hi and lo of one operand (32 KB)
+constexpr int kStage = 2 * kOperand;             // A and B (64 KB)
+constexpr int kTcSmem = kStages * kStage + 256;  // + barriers and the TMEM address
+constexpr long long kWaitLimit = 1ll << 26;      // polls of an mbarrier before giving up
 
 // 0 = fine; 1 = an mbarrier wait ran out (the result of that launch is invalid)
 __device__ int g_tc_status;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// byte offset of element (row r, k) of a K-major tile with 32 K per row, in
-// 8-row x 16-byte core matrices: core matrices adjacent in K are 128 B apart
-// (the descriptor's leading byte offset), 8-row groups 1024 B apart (its
-// stride byte offset)
-__device__ __forceinline__ uint32_t kmajor_off(int r, int k) {
-    return (uint32_t)((r >> 3) * 1024 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
-}
+// element offset (4-byte units) of (row r, k) inside a 128 x 32 K-major tile:
+// core matrices adjacent in K are 128 B apart (the descriptor's leading byte
+// offset), 8-row groups 1024 B apart (its stride byte offset)
+__device__ __forceinline__ int core_off(int r, int k) { return (r >> 3) * 256 + (k >> 2) * 32 + (r & 7) * 4 + (k & 3); }
 
 // shared-memory matrix descriptor: start address, LBO 128 B, SBO 1024 B,
 // descriptor version 1 (sm_100), no swizzle
@@ -60,7 +63,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
 }
 
 // instruction descriptor of kind::tf32: D F32, A and B TF32, both K-major,
-// N = 64, M = 128
+// N = 128, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
                             ((uint32_t)(kTcM >> 4) << 24);
 
@@ -68,13 +71,6 @@ __device__ __forceinline__ uint32_t to_tf32(float f) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
     return r;
-}
-
-// FP64 -> (TF32 high, TF32 low) with hi + lo = float(v) to ~2^-22
-__device__ __forceinline__ void split3(double v, uint32_t& hi, uint32_t& lo) {
-    const float f = (float)v;
-    hi = to_tf32(f);
-    lo = to_tf32(f - __uint_as_float(hi));
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -98,6 +94,17 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     for (long long i = 0; i < kWaitLimit; i++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// bulk copy global -> shared, completion counted on bar (16-byte aligned, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -135,99 +142,99 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// Stage chunk kc of op(A) (rows m0.., K columns kc*32..) and op(B) (K rows,
-// columns n0..) into the stage at `st` as TF32 hi / lo tiles.  Each thread
-// writes whole 16-byte core-matrix rows (4 K values); the 8 threads of a
-// store phase cover the 8 rows of one core matrix, so the stores do not
-// conflict.
-__device__ __forceinline__ void stage_chunk(unsigned char* st, const double* __restrict__ A, bool transA,
-                                            const double* __restrict__ Bm, bool transB,
-                                            const double* __restrict__ dvec, int np, int m0, int n0, int k0) {
-    unsigned char* ahi = st;
-    unsigned char* alo = st + kTileA;
-    unsigned char* bhi = st + 2 * kTileA;
-    unsigned char* blo = st + 2 * kTileA + kTileB;
-    // A: 128 rows x 8 core rows of 4 K values = 1024 pieces, 8 per thread
-#pragma unroll 2
-    for (int it = 0; it < (kTcM * kTcK / 4) / kTcThreads; it++) {
-        const int idx = it * kTcThreads + threadIdx.x;
-        const int c = (idx >> 3) & 7;              // K group of 4
-        const int r = (idx & 7) + 8 * (idx >> 6);  // tile row
-        const int row = m0 + r;
-        uint4 h = make_uint4(0, 0, 0, 0), l = make_uint4(0, 0, 0, 0);
-        if (row < np) {
-            double v[4];
-            const int k = k0 + 4 * c;
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                v[j] = transA ? __ldg(A + (int64_t)(k + j) * np + row) : __ldg(A + (int64_t)row * np + k + j);
-            split3(v[0], h.x, l.x);
-            split3(v[1], h.y, l.y);
-            split3(v[2], h.z, l.z);
-            split3(v[3], h.w, l.w);
+// One CTA per (task, 128-row block): the operand X(r, k) = rowmajor ?
+// S[r * np + k] : S[k * np + r] (times d[k] when given), rows past np zero,
+// written as TF32 hi / lo tiles: out + task.toff + (rb * nk + kc) * 2 * 4096,
+// hi then lo, each in core-matrix order.
+__global__ void __launch_bounds__(256) tc_split_kernel(const BlockTask* __restrict__ tasks,
+                                                       const TcSplit* __restrict__ units,
+                                                       const double* __restrict__ S, bool rowmajor,
+                                                       const double* __restrict__ dvec, uint32_t* __restrict__ out,
+                                                       const int* __restrict__ bmask) {
+    __shared__ double tile[kTcM][kTcK + 1];
+    const TcSplit u = units[blockIdx.x];
+    if (bmask && !bmask[u.task]) return;
+    const BlockTask t = tasks[u.task];
+    const int np = t.np, nk = np / kTcK;
+    const double* src = S + t.woff;
+    const double* d = dvec ? dvec + t.doff : nullptr;
+    for (int kc = 0; kc < nk; kc++) {
+        const int k0 = kc * kTcK;
+        if (rowmajor) {
+            // a warp reads 32 consecutive K of one row
+            for (int it = threadIdx.x; it < kTcM * kTcK; it += 256) {
+                const int r = it / kTcK, k = it % kTcK;
+                const int row = u.rb * kTcM + r;
+                double v = 0.0;
+                if (row < np) v = src[(int64_t)row * np + k0 + k];
+                if (d) v *= d[k0 + k];
+                tile[r][k] = v;
+            }
+        } else {
+            // a warp reads 32 consecutive rows of one K
+            for (int it = threadIdx.x; it < kTcM * kTcK; it += 256) {
+                const int r = it % kTcM, k = it / kTcM;
+                const int row = u.rb * kTcM + r;
+                double v = 0.0;
+                if (row < np) v = src[(int64_t)(k0 + k) * np + row];
+                if (d) v *= d[k0 + k];
+                tile[r][k] = v;
+            }
         }
-        const uint32_t off = kmajor_off(r, 4 * c);
-        *reinterpret_cast<uint4*>(ahi + off) = h;
-        *reinterpret_cast<uint4*>(alo + off) = l;
-    }
-    // B^T: 64 rows (output columns) x 8 core rows = 512 pieces, 4 per thread
-#pragma unroll 2
-    for (int it = 0; it < (kTcN * kTcK / 4) / kTcThreads; it++) {
-        const int idx = it * kTcThreads + threadIdx.x;
-        const int c = (idx >> 3) & 7;
-        const int r = (idx & 7) + 8 * (idx >> 6);
-        const int col = n0 + r;
-        const int k = k0 + 4 * c;
-        double v[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            v[j] = transB ? __ldg(Bm + (int64_t)col * np + k + j) : __ldg(Bm + (int64_t)(k + j) * np + col);
-            if (dvec) v[j] *= __ldg(dvec + k + j);
+        __syncthreads();
+        uint32_t* hi = out + t.toff + ((int64_t)u.rb * nk + kc) * 2 * (kTile / 4);
+        uint32_t* lo = hi + kTile / 4;
+        for (int o = threadIdx.x; o < kTcM * kTcK; o += 256) {
+            // o = core_off(r, k)
+            const int rg = o >> 8, k4 = (o >> 5) & 7, r8 = (o >> 2) & 7, kk = o & 3;
+            const int r = rg * 8 + r8, k = k4 * 4 + kk;
+            const float f = (float)tile[r][k];
+            const uint32_t h = to_tf32(f);
+            hi[o] = h;
+            lo[o] = to_tf32(f - __uint_as_float(h));
         }
-        uint4 h, l;
-        split3(v[0], h.x, l.x);
-        split3(v[1], h.y, l.y);
-        split3(v[2], h.z, l.z);
-        split3(v[3], h.w, l.w);
-        const uint32_t off = kmajor_off(r, 4 * c);
-        *reinterpret_cast<uint4*>(bhi + off) = h;
-        *reinterpret_cast<uint4*>(blo + off) = l;
+        __syncthreads();
     }
 }
 
+// C tile (ti, tj) of 128 x 128 from the split operands: A rows 128 ti.., B
+// rows (the output columns) 128 tj..; rows and columns past np are not written.
 __global__ void __launch_bounds__(kTcThreads) tc_gemm_kernel(const BlockTask* __restrict__ tasks,
                                                              const GemmTile* __restrict__ tiles,
-                                                             const double* __restrict__ A, bool transA,
-                                                             const double* __restrict__ Bm, bool transB,
-                                                             const double* __restrict__ dvec, double* __restrict__ C,
+                                                             const uint32_t* __restrict__ wa,
+                                                             const uint32_t* __restrict__ wb, double* __restrict__ C,
                                                              const int* __restrict__ bmask) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const GemmTile tl = tiles[blockIdx.x];
     if (bmask && !bmask[tl.task]) return;
     const BlockTask t = tasks[tl.task];
-    const int np = t.np;
+    const int np = t.np, nk = np / kTcK;
     const int m0 = tl.ti * kTcM, n0 = tl.tj * kTcN;
-    const double* a = A + t.woff;
-    const double* b = Bm + t.woff;
-    const double* d = dvec ? dvec + t.doff : nullptr;
+    const unsigned char* ga = reinterpret_cast<const unsigned char*>(wa + t.toff) + (int64_t)tl.ti * nk * kOperand;
+    const unsigned char* gb = reinterpret_cast<const unsigned char*>(wb + t.toff) + (int64_t)tl.tj * nk * kOperand;
     double* c = C + t.woff;
 
-    unsigned char* stage[2] = {smem, smem + kStage};
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kStage);  // two mbarriers
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 2 * kStage + 64);
-    const uint32_t bar0 = smem_addr(&bars[0]), bar1 = smem_addr(&bars[1]);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStage);  // full[3], empty[3], done
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kStages * kStage + 128);
+    const uint32_t sbase = smem_addr(smem);
+    auto full = [&](int s) { return smem_addr(&bars[s]); };
+    auto empty = [&](int s) { return smem_addr(&bars[kStages + s]); };
+    const uint32_t done = smem_addr(&bars[2 * kStages]);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (warp == 0) {
-        // 64 TMEM columns hold the 128 x 64 FP32 accumulator
+        // 128 TMEM columns hold the 128 x 128 FP32 accumulator
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
                      "r"(kTcN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar1, 1);
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
+        }
+        mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -235,24 +242,31 @@ __global__ void __launch_bounds__(kTcThreads) tc_gemm_kernel(const BlockTask* __
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    const int nk = np / kTcK;
-    bool ok = true;
-    for (int kc = 0; kc < nk; kc++) {
-        const int s = kc & 1;
-        // the MMAs of chunk kc - 2 read this stage: wait for their commit
-        if (kc >= 2 && ok) ok = mbar_wait(s ? bar1 : bar0, (uint32_t)(((kc - 2) >> 1) & 1));
-        if (ok) stage_chunk(stage[s], a, transA, b, transB, d, np, m0, n0, kc * kTcK);
-        // generic-proxy stores become visible to the tensor cores' async proxy
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (!__syncthreads_and(ok ? 1 : 0)) {
-            ok = false;
-            break;
+    // producer (thread 0) and MMA issuer (thread 32); their outcome reaches
+    // every thread through the done barrier and the block vote below
+    int role_ok = 1;
+    if (threadIdx.x == 0) {
+        for (int kc = 0; kc < nk; kc++) {
+            const int s = kc % kStages, u = kc / kStages;
+            if (u > 0 && !mbar_wait(empty(s), (uint32_t)((u - 1) & 1))) {
+                role_ok = 0;
+                break;
+            }
+            mbar_expect_tx(full(s), (uint32_t)kStage);
+            bulk_g2s(sbase + s * kStage, ga + (int64_t)kc * kOperand, kOperand, full(s));
+            bulk_g2s(sbase + s * kStage + kOperand, gb + (int64_t)kc * kOperand, kOperand, full(s));
         }
-        if (threadIdx.x == 0) {
+    } else if (threadIdx.x == 32) {
+        int kc = 0;
+        for (; kc < nk; kc++) {
+            const int s = kc % kStages, u = kc / kStages;
+            if (!mbar_wait(full(s), (uint32_t)(u & 1))) {
+                role_ok = 0;
+                break;
+            }
             tc_fence_after();
-            const uint32_t sa = smem_addr(stage[s]);
-            const uint32_t ahi = sa, alo = sa + kTileA, bhi = sa + 2 * kTileA, blo = sa + 2 * kTileA + kTileB;
+            const uint32_t st = sbase + s * kStage;
+            const uint32_t ahi = st, alo = st + kTile, bhi = st + kOperand, blo = st + kOperand + kTile;
 #pragma unroll
             for (int ks = 0; ks < kTcK / 8; ks++) {
                 const uint32_t o = ks * 256;  // two 128-byte core matrices per K step of 8
@@ -260,34 +274,38 @@ __global__ void __launch_bounds__(kTcThreads) tc_gemm_kernel(const BlockTask* __
                 mma_tf32(tmem, smem_desc(ahi + o), smem_desc(blo + o), 1u);
                 mma_tf32(tmem, smem_desc(alo + o), smem_desc(bhi + o), 1u);
             }
-            mma_commit(s ? bar1 : bar0);
+            mma_commit(empty(s));
         }
+        // the last commit covers every MMA issued; a stopped issuer still
+        // signals done once its issued MMAs have completed
+        mma_commit(done);
     }
-    // the last commit covers every MMA of the tile
-    if (ok && nk > 0) {
-        const int kl = nk - 1;
-        ok = mbar_wait((kl & 1) ? bar1 : bar0, (uint32_t)((kl >> 1) & 1));
+    // everyone: the accumulator is complete (or the issuer stopped)
+    bool ok = mbar_wait(done, 0u);
+    ok = __syncthreads_and(ok && role_ok) != 0;
+    if (!ok) {
+        if (threadIdx.x == 0) atomicExch(&g_tc_status, 1);
+        // bulk copies still in flight complete on the full barriers: wait
+        // (bounded) for the ones the producer issued before freeing the CTA
+        if (threadIdx.x == 0)
+            for (int s = 0; s < kStages && s < nk; s++) {
+                const int last = ((nk - 1 - s) / kStages) * kStages + s;  // last chunk on stage s
+                mbar_wait(full(s), (uint32_t)((last / kStages) & 1));
+            }
     }
-    if (!ok && nk > 1) {
-        // a wait ran out: drain the other stage's commit too (bounded), so no MMA
-        // is left reading shared memory when the CTA exits
-        const int kl = nk - 2;
-        mbar_wait((kl & 1) ? bar1 : bar0, (uint32_t)((kl >> 1) & 1));
-    }
-    if (!ok && threadIdx.x == 0) atomicExch(&g_tc_status, 1);
     tc_fence_after();
     if (ok) {
         const int row = m0 + warp * 32 + lane;
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
+#pragma unroll 1
         for (int h = 0; h < kTcN / 32; h++) {
             float v[32];
             tmem_ld32(taddr + h * 32, v);
-            if (row < np) {
-                double* out = c + (int64_t)row * np + n0 + h * 32;
+            const int col0 = n0 + h * 32;
+            if (row < np && col0 < np) {
+                double* o = c + (int64_t)row * np + col0;
 #pragma unroll
-                for (int j = 0; j < 32; j += 2)
-                    *reinterpret_cast<double2*>(out + j) = make_double2((double)v[j], (double)v[j + 1]);
+                for (int j = 0; j < 32; j += 2) *reinterpret_cast<double2*>(o + j) = make_double2((double)v[j], (double)v[j + 1]);
             }
         }
     }
@@ -312,12 +330,20 @@ void set_tc_smem_attr() {
 
 }  // namespace
 
-void launch_tc_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
-                    const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s) {
-    if (ntiles == 0) return;
+int64_t tc_split_words(int np) { return (int64_t)((np + kTcM - 1) / kTcM) * kTcM * np * 2; }
+
+void launch_tc_gemm(const TcPlan& p, bool sym, const double* A, bool transA, const double* Bm, bool transB,
+                    const double* dvec, double* C, const int* bmask, cudaStream_t s) {
+    const int ntiles = sym ? p.n_sym : p.n_full;
+    if (ntiles == 0 || p.nsplit == 0) return;
     set_tc_smem_attr();
-    tc_gemm_kernel<<<ntiles, kTcThreads, kTcSmem, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    // op(A)(m, k): row-major when not transposed; op(B)^T(n, k) = op(B)(k, n):
+    // row-major storage of B^T when B is transposed
+    tc_split_kernel<<<p.nsplit, 256, 0, s>>>(p.tasks, p.split, A, !transA, nullptr, p.wa, bmask);
+    tc_split_kernel<<<p.nsplit, 256, 0, s>>>(p.tasks, p.split, Bm, transB, dvec, p.wb, bmask);
+    tc_gemm_kernel<<<ntiles, kTcThreads, kTcSmem, s>>>(p.tasks, sym ? p.tiles_sym : p.tiles_full, p.wa, p.wb, C,
+                                                       bmask);
+    g_kernel_launches.fetch_add(3, std::memory_order_relaxed);
 }
 
 int tc_gemm_status(bool reset) {

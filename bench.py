@@ -31,11 +31,14 @@ golden fixture, so the converged energies are compared with the reference's
   e2e       that whole call, copies included (seconds per step)
   L2        a 256 MiB buffer is written between steps (inputs of this size
             stay inside the 126 MB L2 otherwise)
-  roofline  the dominant kernel, the FP64 gather map (A / A^T of the CG):
-            algorithmic bytes 8 (rows + columns) per launch over its in-solve
-            CUDA-event duration, against the measured HBM copy bandwidth; the
-            same kernel timed alone on the batched workload's largest group
-            (n = 20, 19 instances) is reported beside it
+  roofline  the CG's FP64 gather map (A / A^T): algorithmic bytes 8 (rows +
+            columns) per launch over its CUDA-event duration (launches of the
+            workload's instance replayed from a CUDA graph), against the
+            measured HBM copy bandwidth; the same kernel on the batched
+            workload's largest group (n = 20, 19 instances) is reported beside
+            it (roofline_batch), and the tensor-core product of the
+            mixed-precision projection on that group's G2 blocks
+            (roofline_tensor, against half the measured BF16 peak)
 
 Other workloads: batch256 (256 seeded synthetic active spaces, n ~ U{8..20},
 singlets, DQG; instances bin-packed over ranks) with --warmup-outer capping the
@@ -245,6 +248,12 @@ def run_gpu(args):
                 for i in mine]
 
     solvers = make(kw, opt, args.max_outer)
+    if args.gemm_only:
+        if rank == 0:
+            print(json.dumps({"gemm_only": True, "detail": roofline_tensor(V, torch, dev)}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
     if args.roofline_only:
         achieved, detail = roofline_alone(V, solvers, all_spaces, mine, dev, torch)
         if rank == 0:
@@ -343,6 +352,15 @@ def run_gpu(args):
         "gpu_launches": launches,
         "roofline": roofline_workload(solvers, pk, pk_kind),
         "converged": n_conv,
+        "projection_work": {"refine_sweeps": int(sum(s["refine_sweeps"] for s in stats)),
+                            "jacobi_sweeps": int(sum(s["jacobi_sweeps"] for s in stats)),
+                            "jacobi_blocks": int(sum(s["jacobi_blocks"] for s in stats))},
+        "phase_seconds": ({"cg": float(results[0]["t_cg"]), "projection": float(results[0]["t_xz"]),
+                           "rest": value - float(results[0]["t_cg"]) - float(results[0]["t_xz"]),
+                           "note": "last step, CUDA events on the solve's stream: the CG, the projection "
+                                   "(A^T y, Update_xz), and the error norms, Anderson step and host "
+                                   "synchronisation between them"}
+                          if len(results) == 1 else None),
         "wall_s": wall,
     }
     if clocks:
@@ -394,6 +412,8 @@ def run_gpu(args):
                                  "bound": "hbm", "achieved": ach, "peak": pk, "peak_kind": pk_kind, "unit": "GB/s",
                                  "frac": ach / pk, "traffic": ROOFLINE_TRAFFIC.get((20, 19)),
                                  "bytes_per_launch": nbytes, "us_per_launch": {"A": ta * 1e6, "AT": tt * 1e6}}
+    if args.roofline_batch:
+        out["roofline_tensor"] = roofline_tensor(V, torch, dev)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
@@ -405,7 +425,45 @@ def run_gpu(args):
 # DRAM bytes (read + write) per launch of the roofline kernels, from one ncu
 # capture of the same launches (profiles/ell_kernel_*.md gives the command):
 # key = (n, instances)
-ROOFLINE_TRAFFIC = {}
+ROOFLINE_TRAFFIC = {
+    # A 556.5 MB, A^T 763.3 MB (means of 23 launches each), ell_kernel<4, 1>
+    (20, 19): 659.9e6,
+}
+
+
+def bf16_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def roofline_tensor(V, torch, dev, dims=(800,) * 19, reps=20):
+    """The projection's product on the tensor cores, timed alone: C_i = A_i B_i
+    for the G2 blocks of the batched workload's largest group (19 blocks of 800,
+    padded to 832), two TF32 split launches + the tcgen05 MMA launch per product,
+    CUDA events over `reps` back-to-back products.  Three TF32 products per FP64
+    product (hi.hi + hi.lo + lo.hi) run on the 128-row tiles (832 -> 896 rows);
+    the TF32 peak is taken as half the measured dense BF16 figure (the B200's
+    nominal TF32 : BF16 ratio)."""
+    npad = [(n + 63) // 64 * 64 for n in dims]
+    tot = sum(p * p for p in npad)
+    g = torch.Generator(device=f"cuda:{dev}").manual_seed(0)
+    a = torch.randn(tot, dtype=torch.float64, device=f"cuda:{dev}", generator=g)
+    b = torch.randn(tot, dtype=torch.float64, device=f"cuda:{dev}", generator=g)
+    c = torch.empty_like(a)
+    t_tc = V.time_block_gemm(list(dims), a.data_ptr(), b.data_ptr(), c.data_ptr(), True, reps, dev)
+    t_64 = V.time_block_gemm(list(dims), a.data_ptr(), b.data_ptr(), c.data_ptr(), False, reps, dev)
+    fp64_flops = sum(2.0 * p ** 3 for p in npad)
+    tf32_flops = sum(3 * 2.0 * (-(-p // 128) * 128) ** 2 * p for p in npad)
+    pk, kind = bf16_peak()
+    ach = tf32_flops / t_tc / 1e12
+    return {"kernel": "tc_split_kernel x 2 + tc_gemm_kernel (3xTF32 tcgen05, TMEM accumulator), "
+                      f"{len(dims)} blocks of {dims[0]}", "bound": "tensor", "achieved": ach,
+            "peak": pk / 2, "peak_kind": f"half of the {kind} dense BF16 {pk} TFLOP/s", "unit": "TFLOP/s",
+            "frac": ach / (pk / 2), "traffic": None, "us_per_product": t_tc * 1e6,
+            "fp64_equivalent_tflops": fp64_flops / t_tc / 1e12,
+            "fp64_kernel": {"us_per_product": t_64 * 1e6, "tflops": fp64_flops / t_64 / 1e12}}
 
 
 def roofline_workload(solvers, pk, pk_kind):
@@ -613,6 +671,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-sample", type=lambda s: [int(v) for v in s.split(",")], default=[8, 12, 16, 20])
     ap.add_argument("--no-clocks", dest="clocks", action="store_false")
+    ap.add_argument("--gemm-only", action="store_true",
+                    help="run only the timed block products of the mixed-precision projection (for profilers)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="run only the timed A / A^T launches of the roofline (for profilers)")
     args = ap.parse_args()

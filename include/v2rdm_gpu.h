@@ -191,8 +191,9 @@ int v2g_update_xz_noalloc(v2g_handle* h, double mu, const double* d_c, const dou
  * instance-interleaved vectors of the handle's layout: `reps` launches
  * captured in a CUDA graph and replayed between CUDA events on one stream, so
  * the figure is the kernels' own duration (plus the graph's launch gaps), not
- * the host's launch rate.  For roofline figures; no counterpart in the
- * reference. */
+ * the host's launch rate; every kernel variant is timed and the fastest
+ * reported, as the solver's autotuner picks it.  For roofline figures; no
+ * counterpart in the reference. */
 int v2g_time_maps(v2g_handle* h, int nvec, int reps, double* sec_A, double* sec_AT);
 
 /* The dense product of the projection on caller-owned device buffers, for
@@ -206,6 +207,14 @@ int v2g_time_maps(v2g_handle* h, int nvec, int reps, double* sec_A, double* sec_
  * the reference (it calls F_DGEMM, v2rdm_solver.cc:3273,3286). */
 int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int transA, const double* B, int transB,
                           const double* d, double* C, int tensor_cores, int device);
+
+/* Seconds per product C_i = A_i B_i of v2g_block_gemm_device (no transposes, no
+ * scaling) on caller-owned device buffers: 3 warm-up products, then `reps`
+ * back to back on one stream between CUDA events.  With tensor_cores = 1 a
+ * product is the two TF32 split launches and the tcgen05 MMA launch.  For
+ * roofline figures; no counterpart in the reference. */
+int v2g_time_block_gemm(int nblocks, const int* dims, const double* A, const double* B, double* C, int tensor_cores,
+                        int reps, int device, double* sec);
 
 /* Learned warm start (no counterpart in the reference, whose start is the
  * random guess of Guess, v2rdm_solver.cc:2386-2516).  A pair-wise MLP (16
@@ -237,7 +246,8 @@ int v2g_ws_gradient(v2g_warmstart* w, long rows, const float* features, const fl
  * passes; loss = the last epoch's mean */
 int v2g_ws_train(v2g_warmstart* w, long rows, const float* features, const float* targets, int epochs,
                  int batch_rows, float lr, double* loss);
-int v2g_ws_propose(v2g_warmstart* w, v2g_handle* h);
+/* use_mu = 1: the proposed mu; 0: mu = 1 with the proposed primal */
+int v2g_ws_propose(v2g_warmstart* w, v2g_handle* h, int use_mu);
 
 /* The RDMs handed to the orbital optimiser, as PackSpatialDensity
  * (v2rdm_solver.cc:3664-3773), from the handle's x: d1 = spin-summed 1-RDM,

@@ -104,3 +104,24 @@ def test_mixed_precision_alone_reaches_the_same_energy(v2g):
     e = s.compute_energy()
     assert s.result["status"] == 0
     assert abs(e - float(g["e_primal"])) <= 1e-6
+
+
+@pytest.mark.late
+def test_mixed_precision_on_tensor_cores_reaches_the_fp64_energy(v2g):
+    # n = 16: the G2aa block of 512 takes the tensor-core phase (blocks padded to
+    # 512 and more); the mixed solve must land on the FP64 solve's energy, whose
+    # path is pinned to the reference's energies at n = 8..12 above
+    from v2rdm_casscf_b200.hamiltonian import synthetic
+
+    a = synthetic(16, 45)
+    opts = dict(R_CONVERGENCE=1e-6, E_CONVERGENCE=1e-7, MU_UPDATE_FREQUENCY=250)
+    kw = dict(PRODUCT)
+    runs = []
+    for mixed in (False, True):
+        kw["mixed_precision"] = mixed
+        s = v2g.V2RDMSolver.from_active_space(a, options=opts, **kw)
+        s.guess()
+        runs.append(v2g.solve_batch([s])[0])
+    for r in runs:
+        assert r["status"] == 0
+    assert abs(runs[0]["e_total"] - runs[1]["e_total"]) <= 1e-6

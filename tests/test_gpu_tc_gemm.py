@@ -75,3 +75,27 @@ def test_tc_block_gemm_is_more_accurate_than_one_tf32_product(v2g):
     err = np.abs(dC.cpu().numpy().reshape(256, 256) - ref).max() / np.abs(ref).max()
     # one TF32 product (10-bit mantissa) is off by ~1e-3 relative on these inputs
     assert err < 2e-6, err
+
+
+def test_timed_products_leave_the_same_result(v2g):
+    """The timing entry point runs the same product: after it, C holds A B."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    dims = [300, 130]
+    A = _blocks(rng, dims, lambda r, n: r.standard_normal((n, n)))
+    B = _blocks(rng, dims, lambda r, n: r.standard_normal((n, n)))
+    dev = torch.device("cuda:0")
+    dA = torch.from_numpy(_flat(A)).to(dev)
+    dB = torch.from_numpy(_flat(B)).to(dev)
+    for tc in (True, False):
+        dC = torch.full_like(dA, float("nan"))
+        sec = v2g.time_block_gemm(dims, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), tensor_cores=tc, reps=3)
+        assert 0.0 < sec < 1.0
+        C, off = dC.cpu().numpy(), 0
+        for a, b in zip(A, B):
+            np_ = a.shape[0]
+            ref = a @ b
+            got = C[off:off + np_ * np_].reshape(np_, np_)
+            off += np_ * np_
+            assert np.abs(got - ref).max() <= (1e-5 if tc else 1e-12) * np.abs(ref).max()

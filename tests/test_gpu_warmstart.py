@@ -103,15 +103,20 @@ def test_learned_start_reaches_the_same_energy(v2g):
     loss = ws.train(X, T, epochs=400, batch_rows=128, lr=1e-3)
     print("warm-start training: loss", l0, "->", loss)
     assert loss < 0.25 * l0
-    # held-out seeds: the learned start against the feasible start
-    held = [synthetic(6, s) for s in (0, 1, 2)]
+    # held-out seeds: the learned start (with the network's mu, and with mu = 1
+    # as the feasible start has it) against the feasible start
+    held = [synthetic(6, s) for s in range(6)]
     feas = [v2g.V2RDMSolver.from_active_space(a, options=opts, start="feasible", projection="adaptive") for a in held]
     lrn = [v2g.V2RDMSolver.from_active_space(a, options=opts, start="learned", projection="adaptive") for a in held]
+    lr1 = [v2g.V2RDMSolver.from_active_space(a, options=opts, start="learned", projection="adaptive") for a in held]
     for s in lrn:
         ws.propose(s)
-    rf = v2g.solve_batch(feas)
-    rl = v2g.solve_batch(lrn)
-    for a, b in zip(rf, rl):
-        assert a["status"] == 0 and b["status"] == 0
+    for s in lr1:
+        ws.propose(s, use_mu=False)
+    rf, rl, r1 = v2g.solve_batch(feas), v2g.solve_batch(lrn), v2g.solve_batch(lr1)
+    for a, b, c in zip(rf, rl, r1):
+        assert a["status"] == 0 and b["status"] == 0 and c["status"] == 0
         assert abs(a["e_total"] - b["e_total"]) <= 1e-6
-    print("ablation (outer iterations, feasible vs learned):", [(a["oiter"], b["oiter"]) for a, b in zip(rf, rl)])
+        assert abs(a["e_total"] - c["e_total"]) <= 1e-6
+    print("ablation (outer iterations per held-out seed: feasible, learned, learned with mu = 1):",
+          [(a["oiter"], b["oiter"], c["oiter"]) for a, b, c in zip(rf, rl, r1)])

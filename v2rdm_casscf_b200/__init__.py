@@ -35,7 +35,7 @@ EXPORTS = [
     "v2g_apply_AT_device", "v2g_update_xz", "v2g_solve", "v2g_solve_batch", "v2g_A_nnz", "v2g_export_A",
     "v2g_trace", "v2g_last_batch_stats", "v2g_apply_A_batched_device", "v2g_apply_AT_batched_device",
     "v2g_update_xz_noalloc", "v2g_spatial_density_dims", "v2g_pack_spatial_density", "v2g_block_gemm_device",
-    "v2g_time_maps",
+    "v2g_time_maps", "v2g_time_block_gemm",
     "v2g_write_checkpoint", "v2g_read_checkpoint", "v2g_set_active_orbital_energies", "v2g_solve_continue",
     "v2g_ws_create", "v2g_ws_destroy", "v2g_ws_num_params", "v2g_ws_get_params", "v2g_ws_set_params", "v2g_ws_rows",
     "v2g_ws_features", "v2g_ws_targets", "v2g_ws_forward", "v2g_ws_gradient", "v2g_ws_train", "v2g_ws_propose",
@@ -166,6 +166,7 @@ def lib():
             getattr(L, f).argtypes = [P, I, P, P, P]
         L.v2g_block_gemm_device.argtypes = [I, IP, P, I, P, I, P, P, I, I]
         L.v2g_time_maps.argtypes = [P, I, I, DP, DP]
+        L.v2g_time_block_gemm.argtypes = [I, IP, P, P, P, I, I, I, DP]
         FP = ctypes.POINTER(ctypes.c_float)
         L.v2g_ws_create.argtypes = [I, I, ctypes.c_ulonglong, ctypes.POINTER(P)]
         L.v2g_ws_destroy.argtypes = [P]
@@ -180,7 +181,7 @@ def lib():
         L.v2g_ws_forward.argtypes = [P, L_, FP, FP]
         L.v2g_ws_gradient.argtypes = [P, L_, FP, FP, DP, FP]
         L.v2g_ws_train.argtypes = [P, L_, FP, FP, I, I, ctypes.c_float, DP]
-        L.v2g_ws_propose.argtypes = [P, P]
+        L.v2g_ws_propose.argtypes = [P, P, I]
         _lib = L
     return _lib
 
@@ -475,6 +476,16 @@ def block_gemm_device(dims, d_a, d_b, d_c, trans_a=False, trans_b=False, d_d=Non
                                        int(bool(tensor_cores)), int(device)))
 
 
+def time_block_gemm(dims, d_a, d_b, d_c, tensor_cores=True, reps=20, device=0):
+    """Seconds per product C_i = A_i B_i on the device (see v2g_time_block_gemm)."""
+    dims = np.ascontiguousarray(dims, dtype=np.int32)
+    sec = ctypes.c_double()
+    _check(lib().v2g_time_block_gemm(len(dims), _ip(dims), ctypes.c_void_p(d_a), ctypes.c_void_p(d_b),
+                                     ctypes.c_void_p(d_c), int(bool(tensor_cores)), int(reps), int(device),
+                                     ctypes.byref(sec)))
+    return sec.value
+
+
 def _fp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
@@ -545,8 +556,10 @@ class WarmStart:
                                   ctypes.byref(loss)))
         return loss.value
 
-    def propose(self, solver):
-        _check(lib().v2g_ws_propose(self.h, solver.h))
+    def propose(self, solver, use_mu=True):
+        """Writes the network's proposal into solver (a start="learned" solve);
+        use_mu=False keeps mu = 1 with the proposed primal."""
+        _check(lib().v2g_ws_propose(self.h, solver.h, int(bool(use_mu))))
 
 
 def last_batch_stats():

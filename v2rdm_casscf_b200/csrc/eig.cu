@@ -64,10 +64,14 @@ __device__ double block_sum(double v, double* red) {
 // Parallel cyclic Jacobi on the symmetric N x N matrix A (shared memory,
 // leading dimension kLd), round-robin ordering.  A pair (p,q) is rotated when
 // |a_pq| > rot_eps * sqrt(|a_pp a_qq|) and above an absolute floor of
-// 1e-17 ||A||_F; the method stops after a sweep without rotations (the
+// 1e-17 ||A||_F; the method stops when a sweep would rotate no pair (the
 // classical threshold criterion, which a relative off-norm test near the
-// rounding floor would never reach) or after max_sweeps.  On return V holds
-// the eigenvectors as columns and diag(A) the eigenvalues.
+// rounding floor would never reach) or after max_sweeps.  That test runs on
+// all pairs at once before each sweep, so the rotation-free last sweep of the
+// textbook loop costs one pass over A instead of N - 1 synchronised rounds
+// (the result is the same: a sweep that starts with no pair above the
+// thresholds changes nothing).  On return V holds the eigenvectors as columns
+// and diag(A) the eigenvalues.
 // With init_v = false, V already holds an orthogonal matrix (the previous
 // eigenvectors of a warm start) and the rotations accumulate onto it.
 __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double rot_eps, bool init_v = true,
@@ -75,7 +79,6 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
     __shared__ double rc[kJ / 2], rs[kJ / 2];
     __shared__ int rp[kJ / 2], rq[kJ / 2];
     __shared__ double red[33];
-    __shared__ int rotated;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int Ne = N + (N & 1);
     const int npairs = Ne / 2;
@@ -90,8 +93,14 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
     }
     const double floor_abs = fmax(1e-17 * sqrt(block_sum(tot, red)), abs_tol);
     for (int sweep = 0; sweep < max_sweeps; sweep++) {
-        if (tid == 0) rotated = 0;
-        __syncthreads();
+        int any = 0;
+        for (int i = tid; i < N * N && !any; i += nt) {
+            const int p = i / N, q = i % N;
+            if (p >= q) continue;
+            const double apq = fabs(A[p * kLd + q]);
+            any = apq > floor_abs && apq > rot_eps * sqrt(fabs(A[p * kLd + p]) * fabs(A[q * kLd + q]));
+        }
+        if (!__syncthreads_or(any)) break;
         for (int r = 0; r < Ne - 1; r++) {
             for (int k = tid; k < npairs; k += nt) {
                 int p, q;
@@ -105,7 +114,6 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
                         const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                         c = 1.0 / sqrt(1.0 + t * t);
                         s = t * c;
-                        rotated = 1;
                     }
                 }
                 rc[k] = c;
@@ -114,36 +122,43 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
                 rq[k] = q;
             }
             __syncthreads();
-            // A <- J^T A  (rows p, q)
-            for (int idx = tid; idx < npairs * N; idx += nt) {
-                const int k = idx / N, j = idx % N;
-                const double s = rs[k];
-                if (s == 0.0) continue;
-                const double c = rc[k];
-                const int p = rp[k], q = rq[k];
-                const double apj = A[p * kLd + j], aqj = A[q * kLd + j];
-                A[p * kLd + j] = c * apj - s * aqj;
-                A[q * kLd + j] = s * apj + c * aqj;
+            // A <- J^T A J in one pass: the round's pairs are disjoint, so A splits
+            // into 2 x 2 blocks (pair a rows, pair b columns) that transform
+            // independently, in place (a pair with the padding index of odd N has
+            // s = 0 and a single row / column)
+            for (int idx = tid; idx < npairs * npairs; idx += nt) {
+                const int a = idx / npairs, bb = idx % npairs;
+                const double sa = rs[a], sb = rs[bb];
+                if (sa == 0.0 && sb == 0.0) continue;
+                const double ca = rc[a], cb = rc[bb];
+                const int pa = rp[a], qa = rq[a], pb = rp[bb], qb = rq[bb];
+                const bool qa_ok = qa < N, qb_ok = qb < N;
+                const double x00 = A[pa * kLd + pb];
+                const double x01 = qb_ok ? A[pa * kLd + qb] : 0.0;
+                const double x10 = qa_ok ? A[qa * kLd + pb] : 0.0;
+                const double x11 = (qa_ok && qb_ok) ? A[qa * kLd + qb] : 0.0;
+                // rows: J^T
+                const double y00 = ca * x00 - sa * x10, y01 = ca * x01 - sa * x11;
+                const double y10 = sa * x00 + ca * x10, y11 = sa * x01 + ca * x11;
+                // columns: J
+                A[pa * kLd + pb] = cb * y00 - sb * y01;
+                if (qb_ok) A[pa * kLd + qb] = sb * y00 + cb * y01;
+                if (qa_ok) A[qa * kLd + pb] = cb * y10 - sb * y11;
+                if (qa_ok && qb_ok) A[qa * kLd + qb] = sb * y10 + cb * y11;
             }
-            __syncthreads();
-            // A <- A J, V <- V J  (columns p, q)
+            // V <- V J  (columns p, q; V is not read by the pass above)
             for (int idx = tid; idx < npairs * N; idx += nt) {
                 const int k = idx / N, i = idx % N;
                 const double s = rs[k];
                 if (s == 0.0) continue;
                 const double c = rc[k];
                 const int p = rp[k], q = rq[k];
-                const double aip = A[i * kLd + p], aiq = A[i * kLd + q];
-                A[i * kLd + p] = c * aip - s * aiq;
-                A[i * kLd + q] = s * aip + c * aiq;
                 const double vip = V[i * kLd + p], viq = V[i * kLd + q];
                 V[i * kLd + p] = c * vip - s * viq;
                 V[i * kLd + q] = s * vip + c * viq;
             }
             __syncthreads();
         }
-        if (!rotated) break;
-        __syncthreads();
     }
 }
 
@@ -273,20 +288,25 @@ __global__ void cold_start_kernel(const BlockTask* __restrict__ tasks, const dou
 }
 
 // C = op(A) diag(d) op(B) on 64 x 64 tiles of the padded workspaces.
-// 64 threads per tile, each holding an 8 x 8 block of C in registers (rows
-// ty + 8i, columns tx + 8j): 16 shared-memory loads feed 64 FMAs, which
-// matches the FP64 FMA rate to the shared-memory bandwidth.  The K loop is
-// double buffered through registers.
+// S x S threads per tile (S = 64 / R), each holding an R x R block of C in
+// registers (rows ty + S i, columns tx + S j).  R = 8 (64 threads): 16
+// shared-memory loads feed 64 FMAs, which matches the FP64 FMA rate to the
+// shared-memory bandwidth; the launch for large grids.  R = 4 (256 threads):
+// four times the warps per tile and a quarter of the serial FMA chain per
+// thread, for grids too small to fill the GPU (one instance's few blocks),
+// where the kernel is latency-bound.  The K loop is double buffered through
+// registers; every C entry is one FMA chain in k order in both forms.
 constexpr int kGemmBK = 16;
 constexpr int kGemmLd = 64 + 1;
 
+template <int NT>
 __device__ __forceinline__ void gemm_load_chunk(const double* __restrict__ a, const double* __restrict__ bb, int np,
-                                                int i0, int j0, int k0, bool transA, bool transB, double ra[16],
-                                                double rb[16]) {
-    // 1024 elements per operand chunk, 16 per thread
+                                                int i0, int j0, int k0, bool transA, bool transB,
+                                                double ra[1024 / NT], double rb[1024 / NT]) {
+    // 1024 elements per operand chunk, 1024 / NT per thread
 #pragma unroll
-    for (int u = 0; u < 16; u++) {
-        const int l = threadIdx.x + 64 * u;
+    for (int u = 0; u < 1024 / NT; u++) {
+        const int l = threadIdx.x + NT * u;
         if (transA) {
             const int kk = l >> 6, ii = l & 63;
             ra[u] = a[(int64_t)(k0 + kk) * np + i0 + ii];
@@ -304,12 +324,13 @@ __device__ __forceinline__ void gemm_load_chunk(const double* __restrict__ a, co
     }
 }
 
+template <int NT>
 __device__ __forceinline__ void gemm_store_chunk(double (*As)[kGemmLd], double (*Bs)[kGemmLd], bool transA,
-                                                 bool transB, const double ra[16], const double rb[16],
+                                                 bool transB, const double ra[1024 / NT], const double rb[1024 / NT],
                                                  const double* __restrict__ d, int k0) {
 #pragma unroll
-    for (int u = 0; u < 16; u++) {
-        const int l = threadIdx.x + 64 * u;
+    for (int u = 0; u < 1024 / NT; u++) {
+        const int l = threadIdx.x + NT * u;
         int kk, ii, jj;
         if (transA) {
             kk = l >> 6;
@@ -330,11 +351,15 @@ __device__ __forceinline__ void gemm_store_chunk(double (*As)[kGemmLd], double (
     }
 }
 
-__global__ void __launch_bounds__(64) gemm_kernel(const BlockTask* __restrict__ tasks,
-                                                  const GemmTile* __restrict__ tiles, const double* __restrict__ A,
-                                                  int transA, const double* __restrict__ Bm, int transB,
-                                                  const double* __restrict__ dvec, double* __restrict__ C,
-                                                  const int* __restrict__ bmask) {
+template <int R>
+__global__ void __launch_bounds__((64 / R) * (64 / R)) gemm_kernel(const BlockTask* __restrict__ tasks,
+                                                                   const GemmTile* __restrict__ tiles,
+                                                                   const double* __restrict__ A, int transA,
+                                                                   const double* __restrict__ Bm, int transB,
+                                                                   const double* __restrict__ dvec,
+                                                                   double* __restrict__ C,
+                                                                   const int* __restrict__ bmask) {
+    constexpr int S = 64 / R, NT = S * S, U = 1024 / NT;
     __shared__ double As[2][kGemmBK][kGemmLd];
     __shared__ double Bs[2][kGemmBK][kGemmLd];
     const GemmTile tl = tiles[blockIdx.x];
@@ -344,44 +369,44 @@ __global__ void __launch_bounds__(64) gemm_kernel(const BlockTask* __restrict__ 
     const double* a = A + t.woff;
     const double* bb = Bm + t.woff;
     const double* d = dvec ? dvec + t.doff : nullptr;
-    const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
+    const int tx = threadIdx.x % S, ty = threadIdx.x / S;
     const int i0 = tl.ti * 64, j0 = tl.tj * 64;
-    double acc[8][8];
+    double acc[R][R];
 #pragma unroll
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < R; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
-    double ra[16], rb[16];
-    gemm_load_chunk(a, bb, np, i0, j0, 0, transA, transB, ra, rb);
-    gemm_store_chunk(As[0], Bs[0], transA, transB, ra, rb, d, 0);
+        for (int j = 0; j < R; j++) acc[i][j] = 0.0;
+    double ra[U], rb[U];
+    gemm_load_chunk<NT>(a, bb, np, i0, j0, 0, transA, transB, ra, rb);
+    gemm_store_chunk<NT>(As[0], Bs[0], transA, transB, ra, rb, d, 0);
     __syncthreads();
     int buf = 0;
     for (int k0 = 0; k0 < np; k0 += kGemmBK) {
         const bool more = k0 + kGemmBK < np;
-        if (more) gemm_load_chunk(a, bb, np, i0, j0, k0 + kGemmBK, transA, transB, ra, rb);
+        if (more) gemm_load_chunk<NT>(a, bb, np, i0, j0, k0 + kGemmBK, transA, transB, ra, rb);
 #pragma unroll
         for (int kk = 0; kk < kGemmBK; kk++) {
-            double av[8], bv[8];
+            double av[R], bv[R];
 #pragma unroll
-            for (int i = 0; i < 8; i++) av[i] = As[buf][kk][ty + 8 * i];
+            for (int i = 0; i < R; i++) av[i] = As[buf][kk][ty + S * i];
 #pragma unroll
-            for (int j = 0; j < 8; j++) bv[j] = Bs[buf][kk][tx + 8 * j];
+            for (int j = 0; j < R; j++) bv[j] = Bs[buf][kk][tx + S * j];
 #pragma unroll
-            for (int i = 0; i < 8; i++)
+            for (int i = 0; i < R; i++)
 #pragma unroll
-                for (int j = 0; j < 8; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+                for (int j = 0; j < R; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
         }
         if (more) {
-            gemm_store_chunk(As[buf ^ 1], Bs[buf ^ 1], transA, transB, ra, rb, d, k0 + kGemmBK);
+            gemm_store_chunk<NT>(As[buf ^ 1], Bs[buf ^ 1], transA, transB, ra, rb, d, k0 + kGemmBK);
             __syncthreads();
             buf ^= 1;
         }
     }
     double* cc = C + t.woff;
 #pragma unroll
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < R; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) cc[(int64_t)(i0 + ty + 8 * i) * np + j0 + tx + 8 * j] = acc[i][j];
+        for (int j = 0; j < R; j++) cc[(int64_t)(i0 + ty + S * i) * np + j0 + tx + S * j] = acc[i][j];
 }
 
 // Global index of local row a (0..63) of pair (I, J): first 32 rows are column
@@ -1013,7 +1038,12 @@ void launch_cold_start(const BlockTask* tasks, int ntasks, int max_np, const dou
 void launch_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, const double* A, bool transA,
                  const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s) {
     if (ntiles == 0) return;
-    gemm_kernel<<<ntiles, 64, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
+    // below two tiles per SM (148 SMs) the 256-thread form hides the latency
+    // the 64-thread form cannot
+    if (ntiles < 2 * 148)
+        gemm_kernel<4><<<ntiles, 256, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
+    else
+        gemm_kernel<8><<<ntiles, 64, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -31,8 +31,14 @@ struct DevMap {
     int64_t row_off[kMaxBuckets] = {};  // into rows
     int64_t ent_off[kMaxBuckets] = {};  // into cols / vals
     const int32_t* rows = nullptr;
+    // Entry words.  Unpacked: the column, with vals[] the coefficient.  Packed
+    // (book != nullptr, vals == nullptr): column | code << kCodeShift, the
+    // coefficient book[code] (the maps have a handful of distinct
+    // coefficients: +-1, +-1/2, -1/sqrt 2, a few small integers), 4 bytes per
+    // entry instead of 12.  Padding slots are -1 in both forms.
     const int32_t* cols = nullptr;
     const double* vals = nullptr;
+    const double* book = nullptr;
     int nlong = 0;
     const int32_t* long_rows = nullptr;
     const int32_t* long_ptr = nullptr;
@@ -42,6 +48,8 @@ struct DevMap {
     // built-in rule); see kMapVariants
     int variant = -1;
 };
+constexpr int kCodeShift = 27;                 // packed entry: 27 column bits, 4 code bits
+constexpr int kBookSize = 1 << (31 - kCodeShift);  // 16 coefficients at most
 // Map kernel variants: instances per thread (2, 4, 8) and whether the table
 // loads and output stores bypass the caches (streaming hints).
 constexpr int kMapVariants = 4;  // 0: 2 plain, 1: 4 plain, 2: 4 streamed, 3: 8 streamed

@@ -101,15 +101,15 @@ struct Blocks {
     int nchunk;                  // instance chunks per row tile
 };
 
-template <int W, bool VEC, int CH, bool STREAM>
+template <int W, bool VEC, int CH, bool STREAM, bool PK>
 __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0, int64_t ntile, int B, int b0,
                                          int cnt, unsigned act, const double* __restrict__ in, const Epi& e,
-                                         double (&dot)[CH]) {
+                                         const double* sbook, double (&dot)[CH]) {
     constexpr int KB = W < kSlotBatch ? W : kSlotBatch;
     const int64_t ns = M.nslots[bi];
     const int32_t* rows = M.rows + M.row_off[bi];
     const int32_t* cols = M.cols + M.ent_off[bi];
-    const double* vals = M.vals + M.ent_off[bi];
+    const double* vals = PK ? nullptr : M.vals + M.ent_off[bi];
     for (int64_t i = tile0 * kThreads + threadIdx.x; i < ns; i += ntile * kThreads) {
         double acc[CH];
 #pragma unroll
@@ -120,12 +120,15 @@ __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0,
             double v[KB];
 #pragma unroll
             for (int k = 0; k < KB; k++) {
-                if (STREAM) {
-                    c[k] = __ldcs(cols + (int64_t)(k0 + k) * ns + i);
-                    v[k] = __ldcs(vals + (int64_t)(k0 + k) * ns + i);
+                const int32_t wd = STREAM ? __ldcs(cols + (int64_t)(k0 + k) * ns + i)
+                                          : __ldg(cols + (int64_t)(k0 + k) * ns + i);
+                if (PK) {
+                    c[k] = wd < 0 ? -1 : (wd & ((1 << kCodeShift) - 1));
+                    v[k] = sbook[wd < 0 ? 0 : (wd >> kCodeShift)];
                 } else {
-                    c[k] = __ldg(cols + (int64_t)(k0 + k) * ns + i);
-                    v[k] = __ldg(vals + (int64_t)(k0 + k) * ns + i);
+                    c[k] = wd;
+                    v[k] = STREAM ? __ldcs(vals + (int64_t)(k0 + k) * ns + i)
+                                  : __ldg(vals + (int64_t)(k0 + k) * ns + i);
                 }
             }
 #pragma unroll
@@ -194,10 +197,37 @@ __device__ __forceinline__ void long_row(const DevMap& M, int B, const double* _
     if (partial) block_partial(threadIdx.x < B ? acc : 0.0, B, partial, (int64_t)partial_base + lr);
 }
 
+// One row tile of an ELL bucket of width code wv (= 2 width + (B even)).
+template <int CH, bool STREAM, bool PK>
+__device__ __forceinline__ void ell_tile(int wv, const DevMap& M, int bi, int64_t t0, int64_t nt, int B, int b0,
+                                         int cnt, unsigned act, const double* __restrict__ in, const Epi& e,
+                                         const double* sbook, double (&dot)[CH]) {
+    switch (wv) {
+        case 2: ell_rows<1, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 3: ell_rows<1, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 4: ell_rows<2, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 5: ell_rows<2, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 8: ell_rows<4, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 9: ell_rows<4, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 16: ell_rows<8, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 17: ell_rows<8, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 32: ell_rows<16, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 33: ell_rows<16, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 64: ell_rows<32, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        default: ell_rows<32, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+    }
+}
+
 template <int CH, bool STREAM>
 __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in,
                                                        Epi e, const int* __restrict__ mask,
                                                        double* __restrict__ partial) {
+    // the coefficient book of a packed table, in shared memory
+    __shared__ double sbook[kBookSize];
+    if (M.book) {
+        if (threadIdx.x < kBookSize) sbook[threadIdx.x] = M.book[threadIdx.x];
+        __syncthreads();
+    }
     const int ntiles = bl.start[M.nb];
     if ((int)blockIdx.x >= ntiles * bl.nchunk) {
         long_row(M, B, in, e, mask, partial, ntiles, blockIdx.x - ntiles * bl.nchunk);
@@ -217,21 +247,11 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int 
     for (int j = 0; j < CH; j++) dot[j] = 0.0;
     if (act) {
         const int64_t t0 = tile - bl.start[bi], nt = bl.start[bi + 1] - bl.start[bi];
-        const bool vec = (B & 1) == 0;
-        switch (M.width[bi] * 2 + (vec ? 1 : 0)) {
-            case 2: ell_rows<1, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 3: ell_rows<1, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 4: ell_rows<2, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 5: ell_rows<2, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 8: ell_rows<4, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 9: ell_rows<4, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 16: ell_rows<8, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 17: ell_rows<8, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 32: ell_rows<16, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 33: ell_rows<16, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            case 64: ell_rows<32, false, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-            default: ell_rows<32, true, CH, STREAM>(M, bi, t0, nt, B, b0, cnt, act, in, e, dot); break;
-        }
+        const int wv = M.width[bi] * 2 + ((B & 1) == 0 ? 1 : 0);
+        if (M.book)
+            ell_tile<CH, STREAM, true>(wv, M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot);
+        else
+            ell_tile<CH, STREAM, false>(wv, M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot);
     }
     if (!partial) return;
     // per-instance block sums in a fixed order: warp shuffles, then warps

@@ -97,8 +97,36 @@ struct DevBuf {
 // One map (A or A^T) on the device in the bucketed-ELL form of kernels.cuh.
 struct MapTable {
     DevBuf<int32_t> rows, cols, long_rows, long_ptr, long_col;
-    DevBuf<double> vals, long_val;
+    DevBuf<double> vals, long_val, book;
     DevMap dm;
+
+    // Packs the coefficient of every ELL entry into its column word when the
+    // columns fit in kCodeShift bits and the table has at most kBookSize
+    // distinct coefficients (compared bit for bit, so the sums are unchanged);
+    // returns the book, or an empty vector when the table stays unpacked.
+    static std::vector<double> pack(std::vector<int32_t>& hcols, const std::vector<double>& hvals) {
+        std::map<uint64_t, int> code;
+        std::vector<double> bk;
+        for (size_t k = 0; k < hcols.size(); k++) {
+            if (hcols[k] < 0) continue;
+            if (hcols[k] >= (1 << kCodeShift)) return {};
+            uint64_t bits;
+            std::memcpy(&bits, &hvals[k], sizeof bits);
+            if (code.count(bits)) continue;
+            if ((int)bk.size() == kBookSize) return {};
+            code[bits] = (int)bk.size();
+            bk.push_back(hvals[k]);
+        }
+        if (bk.empty()) return {};
+        for (size_t k = 0; k < hcols.size(); k++) {
+            if (hcols[k] < 0) continue;
+            uint64_t bits;
+            std::memcpy(&bits, &hvals[k], sizeof bits);
+            hcols[k] |= code[bits] << kCodeShift;
+        }
+        bk.resize(kBookSize, 0.0);
+        return bk;
+    }
 
     void build(const Csr& M) {
         static const int widths[kMaxBuckets] = {1, 2, 4, 8, 16, 32};
@@ -155,16 +183,21 @@ struct MapTable {
                 }
             }
         }
+        const std::vector<double> bk = pack(hcols, hvals);
         rows.upload(hrows.data(), hrows.size());
         cols.upload(hcols.data(), hcols.size());
-        vals.upload(hvals.data(), hvals.size());
+        if (bk.empty())
+            vals.upload(hvals.data(), hvals.size());
+        else
+            book.upload(bk.data(), bk.size());
         long_rows.upload(lrows.data(), lrows.size());
         long_ptr.upload(lptr.data(), lptr.size());
         long_col.upload(lcol.data(), lcol.size());
         long_val.upload(lval.data(), lval.size());
         dm.rows = rows.p;
         dm.cols = cols.p;
-        dm.vals = vals.p;
+        dm.vals = bk.empty() ? vals.p : nullptr;
+        dm.book = bk.empty() ? nullptr : book.p;
         dm.nlong = (int)lrows.size();
         dm.long_rows = long_rows.p;
         dm.long_ptr = long_ptr.p;
@@ -277,6 +310,9 @@ class GroupRun {
         if (B_ < 1 || B_ > 256) throw std::invalid_argument("a group holds 1..256 instances");
         CK(cudaSetDevice(T.device));
         CK(cudaStreamCreate(&s_));
+        CK(cudaStreamCreate(&s_small_));
+        CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
         nx_ = T.L.dimx;
         nc_ = T.L.ncon;
         const size_t X = (size_t)nx_ * B_, C = (size_t)nc_ * B_;
@@ -334,6 +370,9 @@ class GroupRun {
         if (hcs_) cudaFreeHost(hcs_);
         if (hdots_ptr_) cudaFreeHost(hdots_ptr_);
         if (stage_) cudaFreeHost(stage_);
+        if (ev_fork_) cudaEventDestroy(ev_fork_);
+        if (ev_join_) cudaEventDestroy(ev_join_);
+        if (s_small_) cudaStreamDestroy(s_small_);
         if (s_) cudaStreamDestroy(s_);
     }
 
@@ -383,14 +422,28 @@ class GroupRun {
         tc_ = mixed && ntc_gtiles_ > 0;
         if (tc_) tc_projections_++;
         launch_spmv(mAT_, B_, y_.p, aty_.p, nullptr, nullptr, nullptr, mask_.p, s_);
-        // the small blocks start from their previous eigenvectors, except in
-        // the first projection, after a cold restart and every kSmallCold-th
-        // projection (so that rounding in the kept eigenvectors cannot build up)
+        // The small blocks (one CTA each: a few SMs for a few hundred
+        // microseconds) run on a second stream beside the large blocks' path;
+        // both read A^T y, c and mu and write disjoint entries of x and z.
+        // They start from their previous eigenvectors, except in the first
+        // projection, after a cold restart and every kSmallCold-th projection
+        // (so that rounding in the kept eigenvectors cannot build up).
         const bool small_warm = small_warm_ && (nproj_ % kSmallCold) != 0;
-        launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_, vsmall_.p,
-                             small_warm);
+        const bool fork = nsmall_ > 0;
+        if (fork) {
+            CK(cudaEventRecord(ev_fork_, s_));
+            CK(cudaStreamWaitEvent(s_small_, ev_fork_, 0));
+            launch_small_project(small_d_.p, nsmall_, B_, aty_.p, c_.p, x_.p, z_.p, mu_.p, mask_.p, s_small_,
+                                 vsmall_.p, small_warm);
+            CK(cudaEventRecord(ev_join_, s_small_));
+        }
         small_warm_ = true;
         nproj_++;
+        project_large(rho);
+        if (fork) CK(cudaStreamWaitEvent(s_, ev_join_, 0));
+    }
+
+    void project_large(const std::vector<double>& rho) {
         if (nlarge_ == 0) return;
         launch_form_u(large_d_.p, nlarge_, max_np_, B_, aty_.p, c_.p, x_.p, mu_.p, mask_.p, U_.p, s_);
         set_block_masks();  // bact_ = blocks of active instances
@@ -457,6 +510,10 @@ class GroupRun {
             // the refinement skipped these blocks' update, so their V carries the
             // orthogonality error of the previous iteration: two Newton-Schulz
             // steps first (Jacobi's rotations preserve V^T V, whatever it is)
+            // (FP64 products even in the mixed phase: the Jacobi below converges
+            // W = V^T U V to its tolerance, which FP32 rounding in W would not allow)
+            const bool tc = tc_;
+            tc_ = false;
             for (int k = 0; k < 2; k++) {
                 gemm_sym(V_.p, true, V_.p, false, nullptr, G_.p, bjac_.p);
                 launch_mirror(large_d_.p, nlarge_, max_np_, G_.p, bjac_.p, s_);
@@ -467,6 +524,7 @@ class GroupRun {
             // warm block Jacobi on W = V^T U V with the current V
             gemm_full(U_.p, false, V_.p, false, nullptr, Tm_.p, bjac_.p);
             gemm_sym(V_.p, true, Tm_.p, false, nullptr, W_.p, bjac_.p);
+            tc_ = tc;
             launch_mirror(large_d_.p, nlarge_, max_np_, W_.p, bjac_.p, s_);
         }
         if (hnact_[4] > 0) {
@@ -1322,6 +1380,8 @@ class GroupRun {
     int B_;
     int64_t nx_ = 0, nc_ = 0;
     cudaStream_t s_ = nullptr;
+    cudaStream_t s_small_ = nullptr;  // the small blocks' projection, beside the large blocks'
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     DevBuf<double> c_, x_, z_, aty_, atp_, y_, ax_, bv_, r_, p_, ap_, partial_, red_, mu_, coef_;
     DevBuf<int> mask_, nact_, smask1_, smask2_;
     DevBuf<CgScalars> cs_;
@@ -2102,34 +2162,38 @@ int v2g_time_maps(v2g_handle* h, int nvec, int reps, double* sec_A, double* sec_
         try {
             CK(cudaEventCreate(&e0));
             CK(cudaEventCreate(&e1));
-            for (int which = 0; which < 2; which++) {
-                const v2g::DevMap& M = which == 0 ? T.A() : T.AT();
-                const double* in = which == 0 ? x.p : y.p;
-                double* out = which == 0 ? oy.p : ox.p;
-                for (int k = 0; k < 3; k++) v2g::launch_spmv(M, nvec, in, out, nullptr, nullptr, nullptr, nullptr, s);
-                CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-                for (int k = 0; k < reps; k++)
-                    v2g::launch_spmv(M, nvec, in, out, nullptr, nullptr, nullptr, nullptr, s);
-                cudaGraph_t g = nullptr;
-                CK(cudaStreamEndCapture(s, &g));
-                size_t nodes = 0;
-                cudaGraphGetNodes(g, nullptr, &nodes);
-                v2g::g_kernel_launches.fetch_sub((long)nodes, std::memory_order_relaxed);
-                const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
-                cudaGraphDestroy(g);
-                CK(ie);
-                CK(cudaGraphLaunch(ex, s));  // warm
-                CK(cudaEventRecord(e0, s));
-                CK(cudaGraphLaunch(ex, s));
-                CK(cudaEventRecord(e1, s));
-                CK(cudaEventSynchronize(e1));
-                v2g::g_kernel_launches.fetch_add(2 * (long)nodes, std::memory_order_relaxed);
-                float ms = 0.f;
-                CK(cudaEventElapsedTime(&ms, e0, e1));
-                (which == 0 ? *sec_A : *sec_AT) = ms * 1e-3 / reps;
-                cudaGraphExecDestroy(ex);
-                ex = nullptr;
-            }
+            // every kernel variant is timed and the fastest kept (the autotuner's choice)
+            for (int which = 0; which < 2; which++)
+                for (int v = 0; v < v2g::kMapVariants; v++) {
+                    v2g::DevMap M = which == 0 ? T.A() : T.AT();
+                    M.variant = v;
+                    const double* in = which == 0 ? x.p : y.p;
+                    double* out = which == 0 ? oy.p : ox.p;
+                    for (int k = 0; k < 3; k++) v2g::launch_spmv(M, nvec, in, out, nullptr, nullptr, nullptr, nullptr, s);
+                    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                    for (int k = 0; k < reps; k++)
+                        v2g::launch_spmv(M, nvec, in, out, nullptr, nullptr, nullptr, nullptr, s);
+                    cudaGraph_t g = nullptr;
+                    CK(cudaStreamEndCapture(s, &g));
+                    size_t nodes = 0;
+                    cudaGraphGetNodes(g, nullptr, &nodes);
+                    v2g::g_kernel_launches.fetch_sub((long)nodes, std::memory_order_relaxed);
+                    const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+                    cudaGraphDestroy(g);
+                    CK(ie);
+                    CK(cudaGraphLaunch(ex, s));  // warm
+                    CK(cudaEventRecord(e0, s));
+                    CK(cudaGraphLaunch(ex, s));
+                    CK(cudaEventRecord(e1, s));
+                    CK(cudaEventSynchronize(e1));
+                    v2g::g_kernel_launches.fetch_add(2 * (long)nodes, std::memory_order_relaxed);
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    double& best = which == 0 ? *sec_A : *sec_AT;
+                    if (v == 0 || ms * 1e-3 / reps < best) best = ms * 1e-3 / reps;
+                    cudaGraphExecDestroy(ex);
+                    ex = nullptr;
+                }
         } catch (...) {
             cleanup();
             throw;
@@ -2139,18 +2203,27 @@ int v2g_time_maps(v2g_handle* h, int nvec, int reps, double* sec_A, double* sec_
     });
 }
 
-int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int transA, const double* B, int transB,
-                          const double* d, double* C, int tensor_cores, int device) {
-    return v2g::guarded([&]() -> int {
-        if (nblocks < 1 || !dims || !A || !B || !C) return v2g::fail(V2G_ERR_ARG, "bad block GEMM arguments");
-        v2g::require_device();
-        v2g::DeviceScope scope(device);
-        std::vector<v2g::BlockTask> tasks(nblocks);
-        std::vector<v2g::GemmTile> tiles;
-        std::vector<v2g::TcSplit> split;
-        int64_t woff = 0, doff = 0, toff = 0;
+namespace {
+// Tasks, tiles and split units of a batched block product on the device.
+struct BlockGemmPlan {
+    std::vector<v2g::BlockTask> tasks;
+    std::vector<v2g::GemmTile> tiles;
+    std::vector<v2g::TcSplit> split;
+    int64_t toff = 0;
+    v2g::DevBuf<v2g::BlockTask> dt;
+    v2g::DevBuf<v2g::GemmTile> dg;
+    v2g::DevBuf<v2g::TcSplit> ds;
+    v2g::DevBuf<uint32_t> wa, wb;
+    v2g::TcPlan tc;
+    bool tensor_cores = false;
+
+    // false: a dimension out of range
+    bool build(int nblocks, const int* dims, bool use_tc) {
+        tensor_cores = use_tc;
+        tasks.resize(nblocks);
+        int64_t woff = 0, doff = 0;
         for (int i = 0; i < nblocks; i++) {
-            if (dims[i] < 1 || dims[i] > 16384) return v2g::fail(V2G_ERR_ARG, "block dimension out of range");
+            if (dims[i] < 1 || dims[i] > 16384) return false;
             v2g::BlockTask t{};
             t.n = dims[i];
             t.np = (dims[i] + 63) / 64 * 64;
@@ -2162,7 +2235,7 @@ int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int tra
             doff += t.np;
             toff += v2g::tc_split_words(t.np);
             tasks[i] = t;
-            if (tensor_cores) {
+            if (use_tc) {
                 const int nr = (t.np + 127) / 128;
                 for (int a = 0; a < nr; a++) {
                     split.push_back({i, a});
@@ -2174,31 +2247,86 @@ int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int tra
                     for (int b = 0; b < nt; b++) tiles.push_back({i, a, b});
             }
         }
-        v2g::DevBuf<v2g::BlockTask> dt;
-        v2g::DevBuf<v2g::GemmTile> dg;
-        v2g::DevBuf<v2g::TcSplit> ds;
-        v2g::DevBuf<uint32_t> wa, wb;
         dt.upload(tasks.data(), tasks.size());
         dg.upload(tiles.data(), tiles.size());
-        if (tensor_cores) {
+        if (use_tc) {
             ds.upload(split.data(), split.size());
             wa.alloc(toff);
             wb.alloc(toff);
-            v2g::TcPlan plan;
-            plan.tasks = dt.p;
-            plan.tiles_full = dg.p;
-            plan.n_full = (int)tiles.size();
-            plan.split = ds.p;
-            plan.nsplit = (int)split.size();
-            plan.wa = wa.p;
-            plan.wb = wb.p;
-            v2g::tc_gemm_status(true);
-            v2g::launch_tc_gemm(plan, false, A, transA != 0, B, transB != 0, d, C, nullptr, 0);
-        } else {
-            v2g::launch_gemm(dt.p, dg.p, (int)tiles.size(), A, transA != 0, B, transB != 0, d, C, nullptr, 0);
+            tc.tasks = dt.p;
+            tc.tiles_full = dg.p;
+            tc.n_full = (int)tiles.size();
+            tc.split = ds.p;
+            tc.nsplit = (int)split.size();
+            tc.wa = wa.p;
+            tc.wb = wb.p;
         }
+        return true;
+    }
+    void launch(const double* A, bool transA, const double* B, bool transB, const double* d, double* C,
+                cudaStream_t s) const {
+        if (tensor_cores)
+            v2g::launch_tc_gemm(tc, false, A, transA, B, transB, d, C, nullptr, s);
+        else
+            v2g::launch_gemm(dt.p, dg.p, (int)tiles.size(), A, transA, B, transB, d, C, nullptr, s);
+    }
+};
+}  // namespace
+
+int v2g_block_gemm_device(int nblocks, const int* dims, const double* A, int transA, const double* B, int transB,
+                          const double* d, double* C, int tensor_cores, int device) {
+    return v2g::guarded([&]() -> int {
+        if (nblocks < 1 || !dims || !A || !B || !C) return v2g::fail(V2G_ERR_ARG, "bad block GEMM arguments");
+        v2g::require_device();
+        v2g::DeviceScope scope(device);
+        BlockGemmPlan plan;
+        if (!plan.build(nblocks, dims, tensor_cores != 0))
+            return v2g::fail(V2G_ERR_ARG, "block dimension out of range");
+        if (tensor_cores) v2g::tc_gemm_status(true);
+        plan.launch(A, transA != 0, B, transB != 0, d, C, 0);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(0));
+        if (tensor_cores && v2g::tc_gemm_status(true) != 0)
+            return v2g::fail(V2G_ERR_CUDA, "a tensor-core GEMM pipeline wait ran out");
+        return V2G_OK;
+    });
+}
+
+int v2g_time_block_gemm(int nblocks, const int* dims, const double* A, const double* B, double* C, int tensor_cores,
+                        int reps, int device, double* sec) {
+    return v2g::guarded([&]() -> int {
+        if (nblocks < 1 || !dims || !A || !B || !C || !sec || reps < 1 || reps > 10000)
+            return v2g::fail(V2G_ERR_ARG, "bad block GEMM timing arguments");
+        v2g::require_device();
+        v2g::DeviceScope scope(device);
+        BlockGemmPlan plan;
+        if (!plan.build(nblocks, dims, tensor_cores != 0))
+            return v2g::fail(V2G_ERR_ARG, "block dimension out of range");
+        cudaStream_t s = nullptr;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        auto cleanup = [&]() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (s) cudaStreamDestroy(s);
+        };
+        try {
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            if (tensor_cores) v2g::tc_gemm_status(true);
+            for (int k = 0; k < 3; k++) plan.launch(A, false, B, false, nullptr, C, s);
+            CK(cudaEventRecord(e0, s));
+            for (int k = 0; k < reps; k++) plan.launch(A, false, B, false, nullptr, C, s);
+            CK(cudaEventRecord(e1, s));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            *sec = ms * 1e-3 / reps;
+        } catch (...) {
+            cleanup();
+            throw;
+        }
+        cleanup();
         if (tensor_cores && v2g::tc_gemm_status(true) != 0)
             return v2g::fail(V2G_ERR_CUDA, "a tensor-core GEMM pipeline wait ran out");
         return V2G_OK;
@@ -2312,7 +2440,7 @@ int v2g_ws_train(v2g_warmstart* w, long rows, const float* features, const float
     });
 }
 
-int v2g_ws_propose(v2g_warmstart* w, v2g_handle* h) {
+int v2g_ws_propose(v2g_warmstart* w, v2g_handle* h, int use_mu) {
     return v2g::guarded([&]() -> int {
         if (!w || !h) return v2g::fail(V2G_ERR_ARG, "null argument");
         Problem& P = h->P;
@@ -2345,7 +2473,7 @@ int v2g_ws_propose(v2g_warmstart* w, v2g_handle* h) {
                 P.x[L.off[v2g::F_D2AB][0] + (int64_t)g1 * gab + g1] = d2;
                 P.x[L.off[v2g::F_D2AB][0] + (int64_t)g2 * gab + g2] = d2;
             }
-        P.mu = std::min(10.0, std::max(0.1, std::exp(lmu / rows)));
+        P.mu = use_mu ? std::min(10.0, std::max(0.1, std::exp(lmu / rows))) : 1.0;
         P.proposal = true;
         return V2G_OK;
     });

@@ -117,6 +117,9 @@ void launch_cg_step(int64_t n, int B, double* y, double* r, const double* p, con
                     const double* pap, double* partial, int* n_active, cudaStream_t s);
 // p = beta p + r
 void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s);
+// Sets the WHILE condition h of a device-side CG loop: ++*count, then
+// continue while *n_active > 0 and *count < cap.
+void launch_cg_while(cudaGraphConditionalHandle h, const int* n_active, int* count, int cap, cudaStream_t s);
 // CG start extrapolation over [e * B + b]: where mode[b] == 2,
 // y <- y + (y - yprev); where mode[b] >= 1, yprev <- y (its value on entry)
 void launch_cg_extrapolate(int64_t n, int B, double* y, double* yprev, const int* mode, cudaStream_t s);

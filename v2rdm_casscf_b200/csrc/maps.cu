@@ -850,6 +850,19 @@ void launch_cg_beta(int B, CgScalars* cs, const double* rrnew, int* n_active, cu
     cg_beta_kernel<<<1, 32, 0, s>>>(B, cs, rrnew, n_active);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
+// Condition of the device-side CG loop (the body of a WHILE node in the
+// group's CUDA graph): another iteration while an instance still iterates,
+// and never more than `cap` iterations in all.
+__global__ void cg_while_kernel(cudaGraphConditionalHandle h, const int* __restrict__ n_active, int* count,
+                                int cap) {
+    const int c = *count + 1;
+    *count = c;
+    cudaGraphSetConditional(h, (*n_active > 0 && c < cap) ? 1u : 0u);
+}
+void launch_cg_while(cudaGraphConditionalHandle h, const int* n_active, int* count, int cap, cudaStream_t s) {
+    cg_while_kernel<<<1, 1, 0, s>>>(h, n_active, count, cap);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
 void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s) {
     cg_update_p_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, p, r, cs);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);

@@ -363,6 +363,7 @@ class GroupRun {
     }
     ~GroupRun() {
         if (cg_exec_) cudaGraphExecDestroy(cg_exec_);
+        if (cg_loop_exec_) cudaGraphExecDestroy(cg_loop_exec_);
         if (diag_file_) std::fclose(diag_file_);
         for (auto e : prof_ev_) cudaEventDestroy(e);
         if (hscal_) cudaFreeHost(hscal_);
@@ -1146,10 +1147,28 @@ class GroupRun {
         launch_cg_init(nc_, B_, bv_.p, ap_.p, r_.p, p_.p, cs_.p, s_);
         launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
         launch_cg_set_rr(B_, cs_.p, red_.p, nact_.p, s_);
-        // CG iterations run in chunks of kCgChunk (a CUDA graph, captured once
-        // per group, outside profile mode); instances that converge inside a
-        // chunk are masked by their scalars, and the host looks at the count of
-        // instances still iterating after each chunk
+        // Outside profile mode the iterations run as a device-side loop: a
+        // CUDA graph (captured once per group) whose WHILE node repeats one
+        // CG iteration until no instance iterates, bounded by the largest
+        // CG_MAXITER of the group, with one host synchronisation per solve.
+        // Instances that converge earlier are masked by their scalars, so the
+        // result is the same as iteration by iteration.
+        if (!profile_ && cg_loop_ok_) {
+            if (!cg_loop_exec_) capture_cg_loop();
+            if (cg_loop_exec_) {
+                CK(cudaMemsetAsync(nact_.p + 6, 0, sizeof(int), s_));
+                CK(cudaGraphLaunch(cg_loop_exec_, s_));
+                CK(cudaMemcpyAsync(hnact_, nact_.p, sizeof(int), cudaMemcpyDeviceToHost, s_));
+                CK(cudaMemcpyAsync(hnact_ + 6, nact_.p + 6, sizeof(int), cudaMemcpyDeviceToHost, s_));
+                CK(cudaStreamSynchronize(s_));
+                g_kernel_launches.fetch_add(cg_loop_nodes_ * (long)hnact_[6], std::memory_order_relaxed);
+                if (hnact_[0] == 0) return;
+            }
+        }
+        // Otherwise (and should the loop stop at its cap with an instance still
+        // iterating) chunks of kCgChunk iterations, a CUDA graph outside
+        // profile mode, with the host looking at the count of instances still
+        // iterating after each chunk
         while (true) {
             if (!profile_) {
                 if (!cg_exec_) capture_cg_chunk();
@@ -1190,6 +1209,54 @@ class GroupRun {
         const cudaError_t e = cudaGraphInstantiate(&cg_exec_, g, 0);
         cudaGraphDestroy(g);
         CK(e);
+    }
+
+    // One CG iteration and its loop condition captured as the body of a WHILE
+    // node (conditional graph nodes); if the runtime refuses the conditional
+    // node, the chunked graph serves instead.
+    void capture_cg_loop() {
+        int cap = 1;
+        for (auto* p : P_) cap = std::max(cap, p->opt.cg_maxiter);
+        cap += 2;  // the scalars stop every instance at its CG_MAXITER before this
+        cudaGraph_t g = nullptr;
+        CK(cudaGraphCreate(&g, 0));
+        cudaGraphConditionalHandle h{};
+        cudaGraphNodeParams cp{};
+        cudaGraphNode_t node = nullptr;
+        if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphDestroy(g);
+            cg_loop_ok_ = false;
+            return;
+        }
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        if (cudaGraphAddNode(&node, g, nullptr, 0, &cp) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphDestroy(g);
+            cg_loop_ok_ = false;
+            return;
+        }
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(s_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        cg_iteration();
+        launch_cg_while(h, nact_.p, nact_.p + 6, cap, s_);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s_, &captured);
+        size_t nodes = 0;
+        if (ce == cudaSuccess) cudaGraphGetNodes(body, nullptr, &nodes);
+        // the launchers counted the captured kernels; replays are counted per iteration
+        g_kernel_launches.fetch_sub((long)nodes, std::memory_order_relaxed);
+        cg_loop_nodes_ = (long)nodes;
+        const cudaError_t ie = ce == cudaSuccess ? cudaGraphInstantiate(&cg_loop_exec_, g, 0) : ce;
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            cudaGetLastError();
+            cg_loop_exec_ = nullptr;
+            cg_loop_ok_ = false;
+        }
     }
 
     // Jacobi: relative off-diagonal norm 1e-13 or the absolute rho share of
@@ -1436,6 +1503,9 @@ class GroupRun {
     // the captured CG chunk
     cudaGraphExec_t cg_exec_ = nullptr;
     long cg_chunk_nodes_ = 0;
+    cudaGraphExec_t cg_loop_exec_ = nullptr;  // the device-side CG loop (WHILE node)
+    long cg_loop_nodes_ = 0;
+    bool cg_loop_ok_ = true;
     // diagnostics (V2G_DIAG)
     int diag_every_ = 0;
     std::FILE* diag_file_ = nullptr;

@@ -354,7 +354,9 @@ def run_gpu(args):
         "converged": n_conv,
         "projection_work": {"refine_sweeps": int(sum(s["refine_sweeps"] for s in stats)),
                             "jacobi_sweeps": int(sum(s["jacobi_sweeps"] for s in stats)),
-                            "jacobi_blocks": int(sum(s["jacobi_blocks"] for s in stats))},
+                            "jacobi_blocks": int(sum(s["jacobi_blocks"] for s in stats)),
+                            "jacobi_unconverged": int(sum(s["jacobi_unconverged"] for s in stats)),
+                            "steps": len(stats)},
         "phase_seconds": ({"cg": float(results[0]["t_cg"]), "projection": float(results[0]["t_xz"]),
                            "rest": value - float(results[0]["t_cg"]) - float(results[0]["t_xz"]),
                            "note": "last step, CUDA events on the solve's stream: the CG, the projection "

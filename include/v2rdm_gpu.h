@@ -312,6 +312,9 @@ typedef struct v2g_batch_stats {
     long refine_sweeps;       /* Ogita-Aishima sweeps over the large PSD blocks */
     long jacobi_sweeps;       /* block-Jacobi sweeps (cold starts and fallbacks) */
     long jacobi_blocks;       /* large blocks that fell back to block Jacobi */
+    long jacobi_unconverged;  /* of those, blocks whose refinement was still short of its
+                                 tolerance after its sweep cap (the others had a first-order
+                                 step too large to trust) */
 } v2g_batch_stats;
 int v2g_last_batch_stats(v2g_batch_stats* out);
 

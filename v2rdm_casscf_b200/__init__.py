@@ -84,6 +84,7 @@ class BatchStats(ctypes.Structure):
         ("refine_sweeps", ctypes.c_long),
         ("jacobi_sweeps", ctypes.c_long),
         ("jacobi_blocks", ctypes.c_long),
+        ("jacobi_unconverged", ctypes.c_long),
     ]
 
     def as_dict(self):

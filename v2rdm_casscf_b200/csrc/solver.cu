@@ -499,7 +499,10 @@ class GroupRun {
             oa_sweeps_++;
         }
         // blocks still unconverged join the Jacobi set (their OA update was applied)
-        if (nref > 0 && !tc_) launch_merge_mask(nlarge_, bref_.p, bjac_.p, s_);
+        if (nref > 0 && !tc_) {
+            launch_merge_mask(nlarge_, bref_.p, bjac_.p, s_);
+            jacobi_unconverged_ += nref;
+        }
         launch_count(nlarge_, bjac_.p, nact_.p + 3, s_);
         // blocks whose eigenvectors degraded restart cold (V = I, W = U) and
         // converge fully; they leave the refinement and warm Jacobi sets
@@ -1001,6 +1004,7 @@ class GroupRun {
     long jacobi_sweeps() const { return sweeps_total_; }
     long oa_sweeps() const { return oa_sweeps_; }
     long jacobi_blocks() const { return jacobi_blocks_; }
+    long jacobi_unconverged() const { return jacobi_unconverged_; }
     long tc_projections() const { return tc_projections_; }
     double map_seconds() const { return map_sec_; }
     long map_launches() const { return map_n_; }
@@ -1481,7 +1485,7 @@ class GroupRun {
     DevBuf<double> pthr_;
     long restarts_ = 0;
     bool cap_ = false;
-    long oa_sweeps_ = 0, jacobi_blocks_ = 0;
+    long oa_sweeps_ = 0, jacobi_blocks_ = 0, jacobi_unconverged_ = 0;
     DevBuf<GemmTile> gtiles_, stiles_, tc_gtiles_, tc_stiles_, lo_gtiles_, lo_stiles_;
     int ntc_gtiles_ = 0, nlo_gtiles_ = 0, nlo_stiles_ = 0;
     DevBuf<TcSplit> tc_split_;
@@ -2039,6 +2043,7 @@ int v2g_solve_batch(v2g_handle** hs, int count, v2g_result* res) {
             st.refine_sweeps += r->oa_sweeps();
             st.jacobi_sweeps += r->jacobi_sweeps();
             st.jacobi_blocks += r->jacobi_blocks();
+            st.jacobi_unconverged += r->jacobi_unconverged();
         }
         v2g::g_stats = st;
         cudaEventDestroy(t0);

@@ -120,6 +120,25 @@ void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgSc
 // Sets the WHILE condition h of a device-side CG loop: ++*count, then
 // continue while *n_active > 0 and *count < cap.
 void launch_cg_while(cudaGraphConditionalHandle h, const int* n_active, int* count, int cap, cudaStream_t s);
+
+// Persistent CG (maps.cu): a whole CG solve of a small group in one
+// cooperative launch.  Groups of at most kLoopMaxB instances and
+// kLoopMaxElems constraint elements (nc * B), where launch latency, not
+// bandwidth, bounds an iteration.
+constexpr int kLoopMaxB = 8;
+constexpr int64_t kLoopMaxElems = 1 << 21;
+bool cg_loop_fits(int64_t nc, int B);
+// CTAs of the cooperative grid on this device (0: no cooperative launch)
+int cg_loop_grid(int device);
+// Iterates until no instance of cs is active or cap iterations: y, r, p and
+// cs as the chunked path leaves them; *n_active the instances still active,
+// *iters the iterations run, *err = 1 if a grid barrier wait ran out (then the
+// results are invalid).  *bar must be 0 at the launch.  part_dot holds
+// (row tiles + long rows of A) x B, part_rr grid x B doubles.
+cudaError_t launch_cg_loop(const DevMap& A, const DevMap& AT, int B, int64_t nc, double* y, double* r, double* p,
+                           double* atp, double* ap, CgScalars* cs, double* part_dot, double* part_rr,
+                           unsigned int* bar, int* err, int* n_active, int* iters, int cap, int grid,
+                           cudaStream_t s);
 // CG start extrapolation over [e * B + b]: where mode[b] == 2,
 // y <- y + (y - yprev); where mode[b] >= 1, yprev <- y (its value on entry)
 void launch_cg_extrapolate(int64_t n, int B, double* y, double* yprev, const int* mode, cudaStream_t s);

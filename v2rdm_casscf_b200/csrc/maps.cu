@@ -6,6 +6,9 @@
 // constraints itself: no atomics, deterministic order, and the two maps are
 // exact adjoints.  These kernels are HBM-bound; their algorithmic traffic per
 // application is 8 * (dimx + nconstraints) bytes per instance.
+#include <map>
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace v2g {
@@ -72,7 +75,9 @@ struct Epi {
     const double* dotv;
     double* out;
 };
-template <bool STREAM = false>
+// COH: the vectors are written by other CTAs of the same (persistent) launch,
+// so they are loaded through L2 (ld.global.cg), never from a stale L1 line.
+template <bool STREAM = false, bool COH = false>
 __device__ __forceinline__ double epilogue(const Epi& e, int64_t r, int B, int b, double s) {
     const int64_t t = r * B + b;
     if (e.sub) s -= e.sub[r];
@@ -82,7 +87,8 @@ __device__ __forceinline__ double epilogue(const Epi& e, int64_t r, int B, int b
         __stcs(e.out + t, s);  // written once, not read again by this launch
     else
         e.out[t] = s;
-    return e.dotv ? e.dotv[t] * s : 0.0;
+    if (!e.dotv) return 0.0;
+    return (COH ? __ldcg(e.dotv + t) : e.dotv[t]) * s;
 }
 
 // Bucketed-ELL part.  One lane per row (slot index i of its bucket) and a
@@ -101,7 +107,7 @@ struct Blocks {
     int nchunk;                  // instance chunks per row tile
 };
 
-template <int W, bool VEC, int CH, bool STREAM, bool PK>
+template <int W, bool VEC, int CH, bool STREAM, bool PK, bool COH>
 __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0, int64_t ntile, int B, int b0,
                                          int cnt, unsigned act, const double* __restrict__ in, const Epi& e,
                                          const double* sbook, double (&dot)[CH]) {
@@ -139,21 +145,22 @@ __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0,
 #pragma unroll
                     for (int j = 0; j < CH; j += 2)
                         if (j < cnt) {
-                            const double2 q = __ldg(reinterpret_cast<const double2*>(g + j));
+                            const double2 q = COH ? __ldcg(reinterpret_cast<const double2*>(g + j))
+                                                  : __ldg(reinterpret_cast<const double2*>(g + j));
                             acc[j] += v[k] * q.x;
                             acc[j + 1] += v[k] * q.y;
                         }
                 } else {
 #pragma unroll
                     for (int j = 0; j < CH; j++)
-                        if (j < cnt) acc[j] += v[k] * __ldg(g + j);
+                        if (j < cnt) acc[j] += v[k] * (COH ? __ldcg(g + j) : __ldg(g + j));
                 }
             }
         }
         const int64_t r = STREAM ? __ldcs(rows + i) : rows[i];
 #pragma unroll
         for (int j = 0; j < CH; j++)
-            if (j < cnt && ((act >> j) & 1u)) dot[j] += epilogue<STREAM>(e, r, B, b0 + j, acc[j]);
+            if (j < cnt && ((act >> j) & 1u)) dot[j] += epilogue<STREAM, COH>(e, r, B, b0 + j, acc[j]);
     }
 }
 
@@ -173,6 +180,7 @@ __device__ __forceinline__ void chunk_range(int B, int nchunk, int ch, int& b0, 
 // Long rows: one CTA per row; thread t sums entries k = t / B, t / B + T / B,
 // ... for instance t % B, then a fixed-order reduction per instance.  Run by
 // the CTAs of ell_kernel past its row tiles (one launch per map).
+template <bool COH>
 __device__ __forceinline__ void long_row(const DevMap& M, int B, const double* __restrict__ in, const Epi& e,
                                          const int* __restrict__ mask, double* __restrict__ partial,
                                          int partial_base, int lr) {
@@ -184,57 +192,62 @@ __device__ __forceinline__ void long_row(const DevMap& M, int B, const double* _
     const int k0 = M.long_ptr[lr], k1 = M.long_ptr[lr + 1];
     double s = 0.0;
     if (threadIdx.x < lanes * B)
-        for (int k = k0 + l; k < k1; k += lanes) s += M.long_val[k] * in[(int64_t)M.long_col[k] * B + b];
+        for (int k = k0 + l; k < k1; k += lanes) {
+            const double* g = in + (int64_t)M.long_col[k] * B + b;
+            s += M.long_val[k] * (COH ? __ldcg(g) : *g);
+        }
     shl[threadIdx.x] = s;
     __syncthreads();
     double acc = 0.0;
     if (threadIdx.x < B) {
         double t = 0.0;
         for (int q = 0; q < lanes; q++) t += shl[threadIdx.x + q * B];
-        if (!(mask && !mask[threadIdx.x])) acc = epilogue(e, r, B, threadIdx.x, t);
+        if (!(mask && !mask[threadIdx.x])) acc = epilogue<false, COH>(e, r, B, threadIdx.x, t);
     }
     __syncthreads();
     if (partial) block_partial(threadIdx.x < B ? acc : 0.0, B, partial, (int64_t)partial_base + lr);
+    if (COH) __syncthreads();  // the shared partials are reused by the CTA's next unit
 }
 
 // One row tile of an ELL bucket of width code wv (= 2 width + (B even)).
-template <int CH, bool STREAM, bool PK>
+template <int CH, bool STREAM, bool PK, bool COH>
 __device__ __forceinline__ void ell_tile(int wv, const DevMap& M, int bi, int64_t t0, int64_t nt, int B, int b0,
                                          int cnt, unsigned act, const double* __restrict__ in, const Epi& e,
                                          const double* sbook, double (&dot)[CH]) {
+#define V2G_ELL(W, V) ell_rows<W, V, CH, STREAM, PK, COH>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot)
     switch (wv) {
-        case 2: ell_rows<1, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 3: ell_rows<1, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 4: ell_rows<2, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 5: ell_rows<2, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 8: ell_rows<4, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 9: ell_rows<4, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 16: ell_rows<8, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 17: ell_rows<8, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 32: ell_rows<16, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 33: ell_rows<16, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        case 64: ell_rows<32, false, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
-        default: ell_rows<32, true, CH, STREAM, PK>(M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot); break;
+        case 2: V2G_ELL(1, false); break;
+        case 3: V2G_ELL(1, true); break;
+        case 4: V2G_ELL(2, false); break;
+        case 5: V2G_ELL(2, true); break;
+        case 8: V2G_ELL(4, false); break;
+        case 9: V2G_ELL(4, true); break;
+        case 16: V2G_ELL(8, false); break;
+        case 17: V2G_ELL(8, true); break;
+        case 32: V2G_ELL(16, false); break;
+        case 33: V2G_ELL(16, true); break;
+        case 64: V2G_ELL(32, false); break;
+        default: V2G_ELL(32, true); break;
     }
+#undef V2G_ELL
 }
 
-template <int CH, bool STREAM>
-__global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in,
-                                                       Epi e, const int* __restrict__ mask,
-                                                       double* __restrict__ partial) {
-    // the coefficient book of a packed table, in shared memory
-    __shared__ double sbook[kBookSize];
-    if (M.book) {
-        if (threadIdx.x < kBookSize) sbook[threadIdx.x] = M.book[threadIdx.x];
-        __syncthreads();
-    }
+// Work unit `blk` of one map application: a row tile of an ELL bucket times
+// an instance chunk (per-instance partial sums of the optional dot into
+// partial[tile * B + b]), or, past the tiles, one long row (its partial at
+// slot ntiles + row).  ell_kernel runs one unit per CTA; the persistent CG
+// kernel walks the units of a map with its whole grid (COH loads).
+template <int CH, bool STREAM, bool COH>
+__device__ __forceinline__ void ell_unit(const DevMap& M, const Blocks& bl, int B, const double* __restrict__ in,
+                                         const Epi& e, const int* mask, double* __restrict__ partial,
+                                         const double* sbook, int blk) {
     const int ntiles = bl.start[M.nb];
-    if ((int)blockIdx.x >= ntiles * bl.nchunk) {
-        long_row(M, B, in, e, mask, partial, ntiles, blockIdx.x - ntiles * bl.nchunk);
+    if (blk >= ntiles * bl.nchunk) {
+        long_row<COH>(M, B, in, e, mask, partial, ntiles, blk - ntiles * bl.nchunk);
         return;
     }
-    const int tile = blockIdx.x / bl.nchunk;
-    const int ch = blockIdx.x % bl.nchunk;
+    const int tile = blk / bl.nchunk;
+    const int ch = blk % bl.nchunk;
     int bi = 0;
     while (bi + 1 < M.nb && tile >= bl.start[bi + 1]) bi++;
     int b0, cnt;
@@ -249,9 +262,9 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int 
         const int64_t t0 = tile - bl.start[bi], nt = bl.start[bi + 1] - bl.start[bi];
         const int wv = M.width[bi] * 2 + ((B & 1) == 0 ? 1 : 0);
         if (M.book)
-            ell_tile<CH, STREAM, true>(wv, M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot);
+            ell_tile<CH, STREAM, true, COH>(wv, M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot);
         else
-            ell_tile<CH, STREAM, false>(wv, M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot);
+            ell_tile<CH, STREAM, false, COH>(wv, M, bi, t0, nt, B, b0, cnt, act, in, e, sbook, dot);
     }
     if (!partial) return;
     // per-instance block sums in a fixed order: warp shuffles, then warps
@@ -269,6 +282,20 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int 
         for (int w = 0; w < kThreads / 32; w++) t += sh[w][threadIdx.x];
         partial[(int64_t)tile * B + b0 + threadIdx.x] = t;
     }
+    if (COH) __syncthreads();  // sh is reused by the CTA's next unit
+}
+
+template <int CH, bool STREAM>
+__global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int B, const double* __restrict__ in,
+                                                       Epi e, const int* __restrict__ mask,
+                                                       double* __restrict__ partial) {
+    // the coefficient book of a packed table, in shared memory
+    __shared__ double sbook[kBookSize];
+    if (M.book) {
+        if (threadIdx.x < kBookSize) sbook[threadIdx.x] = M.book[threadIdx.x];
+        __syncthreads();
+    }
+    ell_unit<CH, STREAM, false>(M, bl, B, in, e, mask, partial, sbook, blockIdx.x);
 }
 
 // Stage 1: block g reduces a contiguous chunk of elements for every instance;
@@ -580,6 +607,41 @@ __global__ void cg_step_yr_kernel(int64_t n, int B, double* __restrict__ y, doub
     block_partial(acc, B, partial, blockIdx.x);
 }
 
+// The scalars of cg_solver.cc:159-177 after a step with p.Ap = pap and the new
+// r.r = rn: alpha, the ||r|| < tol test, beta and the iteration count, the
+// stops on p.Ap <= 0 and on residual growth (kCgGrowth).
+__device__ __forceinline__ void cg_scalar_step(CgScalars& c, double pap, double rn) {
+    c.do_p = 0;
+    if (!c.active) return;
+    c.pap = pap;
+    if (!(c.pap > 0.0)) {
+        // p has no component outside the null space of A^T (or r = 0): no step
+        c.alpha = 0.0;
+        c.active = 0;
+        c.stalled = 1;
+        return;
+    }
+    c.alpha = c.rr / c.pap;
+    c.rrnew = rn;
+    if (!(sqrt(rn) < c.tol)) {
+        if (rn > kCgGrowth * c.rrmin) {
+            // diverging on the null space of A^T: keep the current y (kernels.cuh)
+            c.active = 0;
+            c.stalled = 1;
+        } else {
+            c.beta = rn / c.rr;
+            c.rr = rn;
+            c.rrmin = fmin(c.rrmin, rn);
+            c.do_p = 1;
+            c.iter += 1;
+            if (c.iter >= c.maxiter) c.active = 0;
+        }
+    } else {
+        c.active = 0;
+    }
+    if (!isfinite(rn)) c.active = 0;
+}
+
 // One block per instance: r.r from the step kernel's partials (fixed tree),
 // then the scalars of cg_solver.cc:159-177: alpha, the ||r|| < tol test,
 // beta and the iteration count, the stops on p.Ap <= 0 and on residual
@@ -598,37 +660,7 @@ __global__ void cg_beta_reduce_kernel(int nblk, int B, const double* __restrict_
     }
     if (threadIdx.x != 0) return;
     CgScalars c = cs[b];
-    c.do_p = 0;
-    if (c.active) {
-        c.pap = pap[b];
-        if (!(c.pap > 0.0)) {
-            // p has no component outside the null space of A^T (or r = 0): no step
-            c.alpha = 0.0;
-            c.active = 0;
-            c.stalled = 1;
-        } else {
-            c.alpha = c.rr / c.pap;
-            const double rn = sh[0];
-            c.rrnew = rn;
-            if (!(sqrt(rn) < c.tol)) {
-                if (rn > kCgGrowth * c.rrmin) {
-                    // diverging on the null space of A^T: keep the current y (kernels.cuh)
-                    c.active = 0;
-                    c.stalled = 1;
-                } else {
-                    c.beta = rn / c.rr;
-                    c.rr = rn;
-                    c.rrmin = fmin(c.rrmin, rn);
-                    c.do_p = 1;
-                    c.iter += 1;
-                    if (c.iter >= c.maxiter) c.active = 0;
-                }
-            } else {
-                c.active = 0;
-            }
-            if (!isfinite(rn)) c.active = 0;
-        }
-    }
+    cg_scalar_step(c, pap[b], sh[0]);
     cs[b] = c;
     if (c.active) atomicAdd(n_active, 1);
 }
@@ -677,6 +709,185 @@ __global__ void cg_update_p_kernel(int64_t n, int B, double* __restrict__ p, con
         const int b = (int)(t % B);
         if (!cs[b].do_p) continue;
         p[t] = cs[b].beta * p[t] + r[t];
+    }
+}
+
+// ---- persistent CG for small groups ------------------------------------------
+//
+// One cooperative launch runs a whole CG solve (cg_solver.cc:141-177) for a
+// group of at most kLoopMaxB instances: per iteration four phases over the
+// whole grid (A^T p; A (A^T p) with the per-unit partials of p.Ap; y += alpha
+// p and r -= alpha Ap with per-CTA partials of r.r; p = beta p + r),
+// separated by grid barriers.  Every CTA sums the partials itself in the same
+// fixed order, so every CTA holds the same scalars and takes the same
+// decision to continue; no CTA waits for a value only another CTA computes.
+// Vectors written inside the launch are read through L2 (ld.global.cg).
+// Each barrier wait is bounded: a wait that runs out sets *err and the CTA
+// leaves the kernel; the others then run out at their next wait.
+
+constexpr long kGridWaitPolls = 1L << 24;  // ~1 s of polling with a short sleep
+
+struct CgLoopArgs {
+    DevMap A, AT;
+    Blocks blA, blAT;  // unit layouts of the two maps for ell_unit<CH, false>
+    int B;
+    int64_t nc;
+    double *y, *r, *p, *atp, *ap;
+    CgScalars* cs;
+    double* part_dot;  // (A's row tiles + long rows) x B
+    double* part_rr;   // grid x B
+    unsigned int* bar;
+    int* err;
+    int* n_active;
+    int* iters;
+    int cap;
+};
+
+// Arrive at barrier number target / gridDim.x of the launch and wait for all
+// CTAs; false when the wait ran out.
+__device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target, int* err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        __threadfence();
+        atomicAdd(bar, 1u);
+        unsigned int v = 0;
+        for (long n = 0;; n++) {
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if (v >= target) break;
+            if (n >= kGridWaitPolls) {
+                atomicExch(err, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// out[b] = sum over k < n of part[k * B + b] for every instance b < B, the
+// same fixed order in every CTA (strided per thread, warp shuffles, warps).
+__device__ __forceinline__ void loop_reduce(const double* part, int n, int B, double* out) {
+    __shared__ double wsum[kThreads / 32][kLoopMaxB];
+    double acc[kLoopMaxB];
+#pragma unroll
+    for (int b = 0; b < kLoopMaxB; b++) acc[b] = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+#pragma unroll
+        for (int b = 0; b < kLoopMaxB; b++)
+            if (b < B) acc[b] += __ldcg(part + (int64_t)k * B + b);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int b = 0; b < kLoopMaxB; b++) {
+        double v = acc[b];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) wsum[warp][b] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < B) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; w++) t += wsum[w][threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+template <int CH>
+__global__ void __launch_bounds__(kThreads) cg_loop_kernel(const CgLoopArgs L) {
+    __shared__ double bookA[kBookSize], bookAT[kBookSize];
+    __shared__ CgScalars sc[kLoopMaxB];
+    __shared__ int sact[kLoopMaxB];
+    __shared__ double spap[kLoopMaxB], srn[kLoopMaxB];
+    __shared__ int s_any;
+    const int B = L.B;
+    if (threadIdx.x < kBookSize) {
+        if (L.A.book) bookA[threadIdx.x] = L.A.book[threadIdx.x];
+        if (L.AT.book) bookAT[threadIdx.x] = L.AT.book[threadIdx.x];
+    }
+    if ((int)threadIdx.x < B) {
+        sc[threadIdx.x] = L.cs[threadIdx.x];
+        sact[threadIdx.x] = sc[threadIdx.x].active;
+    }
+    __syncthreads();
+    const unsigned int G = gridDim.x;
+    unsigned int target = 0;
+    const int unitsAT = L.blAT.start[L.AT.nb] * L.blAT.nchunk + L.AT.nlong;
+    const int unitsA = L.blA.start[L.A.nb] * L.blA.nchunk + L.A.nlong;
+    const int slotsA = L.blA.start[L.A.nb] + L.A.nlong;  // partial slots of the A map
+    const Epi eAT{nullptr, nullptr, nullptr, nullptr, L.atp};
+    const Epi eA{nullptr, nullptr, nullptr, L.p, L.ap};
+    int it = 0;
+    while (true) {
+        if (threadIdx.x == 0) {
+            int a = 0;
+            for (int b = 0; b < B; b++) a |= sact[b];
+            s_any = a;
+        }
+        __syncthreads();
+        if (!s_any || it >= L.cap) break;
+        // A^T p
+        for (int u = blockIdx.x; u < unitsAT; u += G)
+            ell_unit<CH, false, true>(L.AT, L.blAT, B, L.p, eAT, sact, nullptr, bookAT, u);
+        target += G;
+        if (!grid_wait(L.bar, target, L.err)) return;
+        // Ap = A (A^T p) and the partials of p.Ap
+        for (int u = blockIdx.x; u < unitsA; u += G)
+            ell_unit<CH, false, true>(L.A, L.blA, B, L.atp, eA, sact, L.part_dot, bookA, u);
+        target += G;
+        if (!grid_wait(L.bar, target, L.err)) return;
+        loop_reduce(L.part_dot, slotsA, B, spap);
+        // y += alpha p, r -= alpha Ap (cg_solver.cc:159-165), partials of r.r
+        {
+            const int rpp = kThreads / B, lanes = rpp * B;
+            const int b = threadIdx.x % B, rsub = threadIdx.x / B;
+            double acc = 0.0;
+            if ((int)threadIdx.x < lanes) {
+                const double pp = spap[b];
+                const bool act = sc[b].active && pp > 0.0;
+                const double a = act ? sc[b].rr / pp : 0.0;
+                for (int64_t e = (int64_t)blockIdx.x * rpp + rsub; e < L.nc; e += (int64_t)G * rpp) {
+                    const int64_t t = e * B + b;
+                    double rv = __ldcg(L.r + t);
+                    if (act) {
+                        L.y[t] = __ldcg(L.y + t) + a * __ldcg(L.p + t);
+                        rv += -a * __ldcg(L.ap + t);
+                        L.r[t] = rv;
+                    }
+                    acc += rv * rv;
+                }
+            }
+            block_partial(acc, B, L.part_rr, blockIdx.x);
+        }
+        target += G;
+        if (!grid_wait(L.bar, target, L.err)) return;
+        loop_reduce(L.part_rr, (int)G, B, srn);
+        if ((int)threadIdx.x < B) {
+            cg_scalar_step(sc[threadIdx.x], spap[threadIdx.x], srn[threadIdx.x]);
+            sact[threadIdx.x] = sc[threadIdx.x].active;
+        }
+        __syncthreads();
+        // p = beta p + r where the instance continues (cg_solver.cc:173-176)
+        for (int64_t t = (int64_t)blockIdx.x * kThreads + threadIdx.x; t < L.nc * B; t += (int64_t)G * kThreads) {
+            const int b = (int)(t % B);
+            if (!sc[b].do_p) continue;
+            L.p[t] = sc[b].beta * __ldcg(L.p + t) + __ldcg(L.r + t);
+        }
+        it++;
+        target += G;
+        if (!grid_wait(L.bar, target, L.err)) return;
+    }
+    if (blockIdx.x == 0) {
+        if ((int)threadIdx.x < B) L.cs[threadIdx.x] = sc[threadIdx.x];
+        if (threadIdx.x == 0) {
+            int cnt = 0;
+            for (int b = 0; b < B; b++) cnt += sact[b];
+            *L.n_active = cnt;
+            *L.iters = it;
+        }
     }
 }
 
@@ -866,6 +1077,63 @@ void launch_cg_while(cudaGraphConditionalHandle h, const int* n_active, int* cou
 void launch_cg_update_p(int64_t n, int B, double* p, const double* r, const CgScalars* cs, cudaStream_t s) {
     cg_update_p_kernel<<<grid_for(n * B), kThreads, 0, s>>>(n, B, p, r, cs);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+int cg_loop_grid(int device) {
+    static std::mutex mu;
+    static std::map<int, int> grid;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = grid.find(device);
+    if (it != grid.end()) return it->second;
+    int sms = 0, coop = 0, occ2 = 0, occ4 = 0;
+    int g = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, cg_loop_kernel<2>, kThreads, 0) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ4, cg_loop_kernel<4>, kThreads, 0) == cudaSuccess) {
+        // two CTAs per SM at most: more barrier arrivals cost more than the
+        // extra CTAs gain on these sizes
+        const int per_sm = std::min(2, std::min(occ2, occ4));
+        if (per_sm >= 1) g = sms * per_sm;
+    }
+    cudaGetLastError();
+    grid[device] = g;
+    return g;
+}
+
+bool cg_loop_fits(int64_t nc, int B) { return B >= 1 && B <= kLoopMaxB && nc * B <= kLoopMaxElems; }
+
+cudaError_t launch_cg_loop(const DevMap& A, const DevMap& AT, int B, int64_t nc, double* y, double* r, double* p,
+                           double* atp, double* ap, CgScalars* cs, double* part_dot, double* part_rr,
+                           unsigned int* bar, int* err, int* n_active, int* iters, int cap, int grid,
+                           cudaStream_t s) {
+    CgLoopArgs L;
+    const int ch = B <= 2 ? 2 : 4;
+    L.A = A;
+    L.AT = AT;
+    L.A.variant = L.AT.variant = (ch == 2 ? 0 : 1);  // the unit layout of ell_unit<ch, false>
+    L.blA = map_blocks(L.A, B);
+    L.blAT = map_blocks(L.AT, B);
+    L.B = B;
+    L.nc = nc;
+    L.y = y;
+    L.r = r;
+    L.p = p;
+    L.atp = atp;
+    L.ap = ap;
+    L.cs = cs;
+    L.part_dot = part_dot;
+    L.part_rr = part_rr;
+    L.bar = bar;
+    L.err = err;
+    L.n_active = n_active;
+    L.iters = iters;
+    L.cap = cap;
+    void* args[] = {&L};
+    const void* fn = ch == 2 ? (const void*)cg_loop_kernel<2> : (const void*)cg_loop_kernel<4>;
+    const cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, s);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    return e;
 }
 
 }  // namespace v2g

@@ -351,6 +351,11 @@ class GroupRun {
         build_projection_plan();
         upload_state();
         tune_maps();
+        if (cg_loop_fits(nc_, B_)) loop_grid_ = cg_loop_grid(T.device);
+        if (loop_grid_ > 0) {
+            loopbar_.alloc(2);
+            looppart_.alloc((size_t)loop_grid_ * B_);
+        }
         alloc_anderson(X);
         if (const char* d = std::getenv("V2G_DIAG")) diag_every_ = std::atoi(d);
         if (diag_every_ > 0)
@@ -1151,6 +1156,25 @@ class GroupRun {
         launch_cg_init(nc_, B_, bv_.p, ap_.p, r_.p, p_.p, cs_.p, s_);
         launch_reduce(RED_DOT, nc_, B_, r_.p, r_.p, nullptr, nullptr, partial_.p, red_.p, s_);
         launch_cg_set_rr(B_, cs_.p, red_.p, nact_.p, s_);
+        // Small groups (outside profile mode): the whole solve in one
+        // cooperative launch, the phases of each iteration separated by grid
+        // barriers (maps.cu), one host synchronisation per solve
+        if (!profile_ && loop_grid_ > 0) {
+            int cap = 1;
+            for (auto* p : P_) cap = std::max(cap, p->opt.cg_maxiter);
+            cap += 2;
+            CK(cudaMemsetAsync(loopbar_.p, 0, 2 * sizeof(unsigned int), s_));
+            CK(launch_cg_loop(mA_, mAT_, B_, nc_, y_.p, r_.p, p_.p, atp_.p, ap_.p, cs_.p, partial_.p, looppart_.p,
+                              loopbar_.p, reinterpret_cast<int*>(loopbar_.p + 1), nact_.p, nact_.p + 6, cap,
+                              loop_grid_, s_));
+            CK(cudaMemcpyAsync(hnact_, nact_.p, sizeof(int), cudaMemcpyDeviceToHost, s_));
+            CK(cudaMemcpyAsync(hnact_ + 6, nact_.p + 6, sizeof(int), cudaMemcpyDeviceToHost, s_));
+            CK(cudaMemcpyAsync(hnact_ + 7, loopbar_.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s_));
+            CK(cudaStreamSynchronize(s_));
+            if (hnact_[7] != 0) throw CudaError("a grid barrier of the persistent CG did not complete (wait ran out)");
+            cg_loop_iters_ += hnact_[6];
+            if (hnact_[0] == 0) return;
+        }
         // Outside profile mode the iterations run as a device-side loop: a
         // CUDA graph (captured once per group) whose WHILE node repeats one
         // CG iteration until no instance iterates, bounded by the largest
@@ -1507,6 +1531,12 @@ class GroupRun {
     // the captured CG chunk
     cudaGraphExec_t cg_exec_ = nullptr;
     long cg_chunk_nodes_ = 0;
+    // the persistent CG (small groups): cooperative grid size (0: not used),
+    // barrier counter and error flag, per-CTA partials of r.r
+    int loop_grid_ = 0;
+    DevBuf<unsigned int> loopbar_;
+    DevBuf<double> looppart_;
+    long cg_loop_iters_ = 0;
     cudaGraphExec_t cg_loop_exec_ = nullptr;  // the device-side CG loop (WHILE node)
     long cg_loop_nodes_ = 0;
     bool cg_loop_ok_ = true;

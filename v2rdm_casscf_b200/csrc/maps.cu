@@ -53,18 +53,40 @@ __device__ __forceinline__ Chunk chunk_of(int64_t nrows, int B) {
     return c;
 }
 
+// Per-instance sum over the CTA of v, where thread t holds instance t % B;
+// the sum for instance b is returned to thread b < B (0 elsewhere), in a fixed
+// order.  When B divides 32 the lanes of one instance sit at stride B in every
+// warp: shuffles fold them, then thread b adds the warps' sums; otherwise
+// thread b walks its rows.  The CTA synchronises on entry and on exit, so
+// the shared scratch can be reused right away.
+__device__ __forceinline__ double cta_instance_sum(double v, int B) {
+    __shared__ double sh[kThreads];
+    double s = 0.0;
+    __syncthreads();
+    if ((32 % B) == 0) {
+        for (int o = 16; o >= B; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane < B) sh[warp * B + lane] = v;
+        __syncthreads();
+        if ((int)threadIdx.x < B)
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sh[w * B + threadIdx.x];
+    } else {
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        if ((int)threadIdx.x < B) {
+            const int rows_per_pass = blockDim.x / B;
+            for (int k = 0; k < rows_per_pass; k++) s += sh[threadIdx.x + k * B];
+        }
+    }
+    __syncthreads();
+    return s;
+}
+
 // Per-instance block partial of v, written to partial[slot * B + b] (slot is
 // the block's index among the partial sums, not always blockIdx.x).
 __device__ __forceinline__ void block_partial(double v, int B, double* __restrict__ partial, int64_t slot) {
-    __shared__ double sh[kThreads];
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    if (threadIdx.x < B) {
-        const int rows_per_pass = blockDim.x / B;
-        double s = 0.0;
-        for (int k = 0; k < rows_per_pass; k++) s += sh[threadIdx.x + k * B];
-        partial[slot * B + threadIdx.x] = s;
-    }
+    const double s = cta_instance_sum(v, B);
+    if ((int)threadIdx.x < B) partial[slot * B + threadIdx.x] = s;
 }
 
 // Per-row epilogue shared by the map kernels.
@@ -303,7 +325,6 @@ __global__ void __launch_bounds__(kThreads) ell_kernel(DevMap M, Blocks bl, int 
 __global__ void reduce_stage1(int mode, int64_t n, int B, const double* __restrict__ u, const double* __restrict__ v,
                               const double* __restrict__ w, const double* __restrict__ row,
                               double* __restrict__ partial) {
-    __shared__ double sh[kThreads];
     const int rows_per_pass = blockDim.x / B;
     const int lanes = rows_per_pass * B;
     const int b = threadIdx.x % B;
@@ -333,13 +354,8 @@ __global__ void reduce_stage1(int mode, int64_t n, int B, const double* __restri
             acc += term;
         }
     }
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    if (threadIdx.x < B) {
-        double s = 0.0;
-        for (int k = 0; k < rows_per_pass; k++) s += sh[b + k * B];
-        partial[(int64_t)blockIdx.x * B + b] = s;
-    }
+    const double s = cta_instance_sum(acc, B);
+    if ((int)threadIdx.x < B) partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
 }
 
 // Stage 2: one block per instance sums its nblk partials with a fixed tree
@@ -453,19 +469,11 @@ __global__ void __launch_bounds__(kThreads) aa_update_kernel(
         }
     }
     // partial[(k * gridDim.x + block) * B + b] for k <= 2 m
-    __shared__ double sh[kThreads];
-    const int rows_per_pass = blockDim.x / B;
 #pragma unroll
     for (int k = 0; k < 2 * MAXM + 1; k++) {
         if (k <= 2 * m) {
-            sh[threadIdx.x] = (k == 2 * m) ? ff : acc[k];
-            __syncthreads();
-            if ((int)threadIdx.x < B) {
-                double sum = 0.0;
-                for (int r = 0; r < rows_per_pass; r++) sum += sh[threadIdx.x + r * B];
-                partial[((int64_t)k * gridDim.x + blockIdx.x) * B + threadIdx.x] = sum;
-            }
-            __syncthreads();
+            const double sum = cta_instance_sum((k == 2 * m) ? ff : acc[k], B);
+            if ((int)threadIdx.x < B) partial[((int64_t)k * gridDim.x + blockIdx.x) * B + threadIdx.x] = sum;
         }
     }
 }
@@ -725,7 +733,8 @@ __global__ void cg_update_p_kernel(int64_t n, int B, double* __restrict__ p, con
 // Each barrier wait is bounded: a wait that runs out sets *err and the CTA
 // leaves the kernel; the others then run out at their next wait.
 
-constexpr long kGridWaitPolls = 1L << 24;  // ~1 s of polling with a short sleep
+constexpr long kGridWaitPolls = 1L << 25;  // about a second of polling (short sleeps)
+constexpr int kLoopCtasPerSm = 3;
 
 struct CgLoopArgs {
     DevMap A, AT;
@@ -750,8 +759,9 @@ __device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        __threadfence();
-        atomicAdd(bar, 1u);
+        // release: the CTA's writes (ordered before this by the barrier above)
+        // become visible to every CTA that acquires the counter
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
         unsigned int v = 0;
         for (long n = 0;; n++) {
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
@@ -761,9 +771,8 @@ __device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target
                 ok = 0;
                 break;
             }
-            __nanosleep(64);
+            if (n > 64) __nanosleep(32);
         }
-        __threadfence();
     }
     __syncthreads();
     return ok != 0;
@@ -797,7 +806,7 @@ __device__ __forceinline__ void loop_reduce(const double* part, int n, int B, do
 }
 
 template <int CH>
-__global__ void __launch_bounds__(kThreads) cg_loop_kernel(const CgLoopArgs L) {
+__global__ void __launch_bounds__(kThreads, kLoopCtasPerSm) cg_loop_kernel(const CgLoopArgs L) {
     __shared__ double bookA[kBookSize], bookAT[kBookSize];
     __shared__ CgScalars sc[kLoopMaxB];
     __shared__ int sact[kLoopMaxB];
@@ -1085,15 +1094,16 @@ int cg_loop_grid(int device) {
     std::lock_guard<std::mutex> lk(mu);
     auto it = grid.find(device);
     if (it != grid.end()) return it->second;
-    int sms = 0, coop = 0, occ2 = 0, occ4 = 0;
+    int sms = 0, coop = 0, occ1 = 0, occ2 = 0, occ4 = 0;
     int g = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, cg_loop_kernel<1>, kThreads, 0) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, cg_loop_kernel<2>, kThreads, 0) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ4, cg_loop_kernel<4>, kThreads, 0) == cudaSuccess) {
-        // two CTAs per SM at most: more barrier arrivals cost more than the
-        // extra CTAs gain on these sizes
-        const int per_sm = std::min(2, std::min(occ2, occ4));
+        // three CTAs per SM (the launch bound of every form): the phases are
+        // latency-bound gathers that want the warps
+        const int per_sm = std::min(kLoopCtasPerSm, std::min(occ1, std::min(occ2, occ4)));
         if (per_sm >= 1) g = sms * per_sm;
     }
     cudaGetLastError();
@@ -1108,10 +1118,12 @@ cudaError_t launch_cg_loop(const DevMap& A, const DevMap& AT, int B, int64_t nc,
                            unsigned int* bar, int* err, int* n_active, int* iters, int cap, int grid,
                            cudaStream_t s) {
     CgLoopArgs L;
-    const int ch = B <= 2 ? 2 : 4;
+    // one instance per thread for a single instance (fewer registers); the
+    // unit layout is the 2-instance one, which has one chunk for B <= 2
+    const int ch = B == 1 ? 1 : (B <= 2 ? 2 : 4);
     L.A = A;
     L.AT = AT;
-    L.A.variant = L.AT.variant = (ch == 2 ? 0 : 1);  // the unit layout of ell_unit<ch, false>
+    L.A.variant = L.AT.variant = (ch <= 2 ? 0 : 1);
     L.blA = map_blocks(L.A, B);
     L.blAT = map_blocks(L.AT, B);
     L.B = B;
@@ -1130,7 +1142,8 @@ cudaError_t launch_cg_loop(const DevMap& A, const DevMap& AT, int B, int64_t nc,
     L.iters = iters;
     L.cap = cap;
     void* args[] = {&L};
-    const void* fn = ch == 2 ? (const void*)cg_loop_kernel<2> : (const void*)cg_loop_kernel<4>;
+    const void* fn = ch == 1 ? (const void*)cg_loop_kernel<1>
+                             : (ch == 2 ? (const void*)cg_loop_kernel<2> : (const void*)cg_loop_kernel<4>);
     const cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, s);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     return e;

@@ -222,6 +222,7 @@ struct TcPlan {
     int n_full = 0, n_sym = 0;
     const TcSplit* split = nullptr;
     int nsplit = 0;
+    int max_nk = 0;  // largest np / 32 of the tasks: the split runs one CTA per (row block, K chunk)
     uint32_t* wa = nullptr;
     uint32_t* wb = nullptr;
 };

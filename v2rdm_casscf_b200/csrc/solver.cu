@@ -1463,6 +1463,7 @@ class GroupRun {
         tc_plan_.n_sym = (int)ts.size();
         tc_plan_.split = tc_split_.p;
         tc_plan_.nsplit = (int)sp.size();
+        for (const auto& u : sp) tc_plan_.max_nk = std::max(tc_plan_.max_nk, hlarge_[u.task].np / 32);
         tc_plan_.wa = tcwa_.p;
         tc_plan_.wb = tcwb_.p;
         nstiles_ = (int)st.size();
@@ -2369,6 +2370,7 @@ struct BlockGemmPlan {
             tc.n_full = (int)tiles.size();
             tc.split = ds.p;
             tc.nsplit = (int)split.size();
+            for (const auto& t : tasks) tc.max_nk = std::max(tc.max_nk, t.np / 32);
             tc.wa = wa.p;
             tc.wb = wb.p;
         }

@@ -158,7 +158,10 @@ __global__ void __launch_bounds__(256) tc_split_kernel(const BlockTask* __restri
     const int np = t.np, nk = np / kTcK;
     const double* src = S + t.woff;
     const double* d = dvec ? dvec + t.doff : nullptr;
-    for (int kc = 0; kc < nk; kc++) {
+    // one K chunk per CTA on a 2-D grid (blockIdx.y); all chunks on a 1-D grid
+    const int kc0 = gridDim.y > 1 ? (int)blockIdx.y : 0;
+    const int kc1 = gridDim.y > 1 ? (int)blockIdx.y + 1 : nk;
+    for (int kc = kc0; kc < kc1 && kc < nk; kc++) {
         const int k0 = kc * kTcK;
         if (rowmajor) {
             // a warp reads 32 consecutive K of one row
@@ -339,8 +342,9 @@ void launch_tc_gemm(const TcPlan& p, bool sym, const double* A, bool transA, con
     set_tc_smem_attr();
     // op(A)(m, k): row-major when not transposed; op(B)^T(n, k) = op(B)(k, n):
     // row-major storage of B^T when B is transposed
-    tc_split_kernel<<<p.nsplit, 256, 0, s>>>(p.tasks, p.split, A, !transA, nullptr, p.wa, bmask);
-    tc_split_kernel<<<p.nsplit, 256, 0, s>>>(p.tasks, p.split, Bm, transB, dvec, p.wb, bmask);
+    const dim3 sg(p.nsplit, p.max_nk > 0 ? p.max_nk : 1);
+    tc_split_kernel<<<sg, 256, 0, s>>>(p.tasks, p.split, A, !transA, nullptr, p.wa, bmask);
+    tc_split_kernel<<<sg, 256, 0, s>>>(p.tasks, p.split, Bm, transB, dvec, p.wb, bmask);
     tc_gemm_kernel<<<ntiles, kTcThreads, kTcSmem, s>>>(p.tasks, sym ? p.tiles_sym : p.tiles_full, p.wa, p.wb, C,
                                                        bmask);
     g_kernel_launches.fetch_add(3, std::memory_order_relaxed);

@@ -671,19 +671,6 @@ __global__ void lam_from_diag_kernel(const BlockTask* __restrict__ tasks, const 
 constexpr double kHard = 0.1;
 constexpr double kFroMax = 0.2;
 
-// Residual coupling |s_ij - lambda_j g_ij| below which a pair is left as it is
-// (orthogonality term only): the rounding floor, or, with an absolute
-// tolerance for the block (the adaptive projection), the block's tolerance
-// over n.  The PSD projection is non-expansive, ||P+(W) - P+(diag W)||_F <=
-// ||offdiag W||_F, so couplings below this change x and z by at most the
-// tolerance in all, however small the pair's eigenvalue gap: a first-order
-// step num / gap, which a small gap makes large, is not needed for them.
-__device__ __forceinline__ double pair_floor(const BlockTask& t, int task, const double* __restrict__ scale,
-                                             const double* __restrict__ abs_tol) {
-    const double f = 1e-15 * scale[task];
-    return abs_tol ? fmax(f, abs_tol[task] / (double)t.n) : f;
-}
-
 __global__ void oa_lambda_kernel(const BlockTask* __restrict__ tasks, const double* __restrict__ S,
                                  const double* __restrict__ G, const int* __restrict__ bmask,
                                  double* __restrict__ lam, double* __restrict__ scale, int* __restrict__ restart) {
@@ -724,8 +711,7 @@ __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const doubl
                                 const double* __restrict__ G, const double* __restrict__ lam,
                                 const double* __restrict__ scale, const int* __restrict__ bmask,
                                 int* __restrict__ partner, int* __restrict__ hard,
-                                unsigned long long* __restrict__ gdev, int* __restrict__ restart,
-                                const double* __restrict__ abs_tol) {
+                                unsigned long long* __restrict__ gdev, int* __restrict__ restart) {
     __shared__ double sr[256];
     __shared__ int sj[256];
     __shared__ double sg[256];
@@ -738,7 +724,7 @@ __global__ void oa_pairs_kernel(const BlockTask* __restrict__ tasks, const doubl
     int bj = -1;
     double gd = 0.0;  // max_j |G_ij - delta_ij| of this row: how far V is from orthonormal
     if (i < t.n) {
-        const double negligible = pair_floor(t, task, scale, abs_tol);
+        const double negligible = 1e-15 * scale[task];
         const double li = lam[t.doff + i];
         for (int j = threadIdx.x; j < t.n; j += blockDim.x) {
             const int64_t w = t.woff + (int64_t)i * t.np + j;
@@ -788,14 +774,14 @@ __global__ void oa_update_kernel(const BlockTask* __restrict__ tasks, const doub
                                  const double* __restrict__ scale, const int* __restrict__ partner,
                                  const int* __restrict__ bmask, double* __restrict__ M,
                                  unsigned long long* __restrict__ emax, int* __restrict__ hard,
-                                 double* __restrict__ erow, const double* __restrict__ abs_tol) {
+                                 double* __restrict__ erow) {
     __shared__ double red[33];
     const int task = blockIdx.y;
     if (bmask && !bmask[task]) return;
     const BlockTask t = tasks[task];
     const int i = blockIdx.x;
     if (i >= t.np) return;
-    const double negligible = pair_floor(t, task, scale, abs_tol);
+    const double negligible = 1e-15 * scale[task];
     const double li = lam[t.doff + i];
     const int pi = (i < t.n) ? partner[t.doff + i] : -1;
     double emx = 0.0, esq = 0.0;
@@ -1110,15 +1096,15 @@ void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, 
 void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
                        const int* bmask, double* lam, double* scale, int* partner, double* M,
                        unsigned long long* emax, int* hard, double* erow, int* restart, unsigned long long* gdev,
-                       const double* abs_tol, cudaStream_t s) {
+                       cudaStream_t s) {
     if (ntasks == 0) return;
     oa_lambda_kernel<<<ntasks, 256, 0, s>>>(tasks, S, G, bmask, lam, scale, restart);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     oa_pairs_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, bmask, partner, hard, gdev,
-                                                          restart, abs_tol);
+                                                          restart);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     oa_update_kernel<<<dim3(max_np, ntasks), 256, 0, s>>>(tasks, S, G, lam, scale, partner, bmask, M, emax,
-                                                           hard, erow, abs_tol);
+                                                           hard, erow);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     oa_fro_kernel<<<ntasks, 256, 0, s>>>(tasks, erow, bmask, hard);
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);

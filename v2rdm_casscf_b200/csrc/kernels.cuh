@@ -276,12 +276,10 @@ void launch_lam_from_diag(const BlockTask* tasks, int ntasks, const double* Ww, 
 // ||E||_F > 0.2 are marked hard.  erow holds one double per padded row.
 // gdev[t] (optional) gets max |G_ij - delta_ij| of the block (as the bits of a
 // non-negative double): the distance of V from orthonormal.
-// abs_tol (optional, one per block): pairs whose residual coupling is below
-// abs_tol / n are left unrotated (orthogonality term only).
 void launch_oa_analyze(const BlockTask* tasks, int ntasks, int max_np, const double* S, const double* G,
                        const int* bmask, double* lam, double* scale, int* partner, double* M,
                        unsigned long long* emax, int* hard, double* erow, int* restart, unsigned long long* gdev,
-                       const double* abs_tol, cudaStream_t s);
+                       cudaStream_t s);
 void launch_oa_masks(int ntasks, const unsigned long long* emax, const int* hard, const double* tol,
                      const double* abs_tol, const double* scale, int* ref, int* upd, int* jac, int* n_ref,
                      cudaStream_t s);

@@ -499,7 +499,7 @@ class GroupRun {
             CK(cudaMemsetAsync(emax_.p, 0, nlarge_ * sizeof(unsigned long long), s_));
             CK(cudaMemsetAsync(hard_.p, 0, nlarge_ * sizeof(int), s_));
             launch_oa_analyze(large_d_.p, nlarge_, max_np_, W_.p, G_.p, bref_.p, lam_.p, scale_.p, partner_.p,
-                              M_.p, emax_.p, hard_.p, erow_.p, restart_.p, gdev_.p, atol_.p, s_);
+                              M_.p, emax_.p, hard_.p, erow_.p, restart_.p, gdev_.p, s_);
             launch_oa_masks(nlarge_, emax_.p, hard_.p, otol_.p, atol_.p, scale_.p, bref_.p, bupd_.p, bjac_.p,
                             nact_.p + 2, s_);
             gemm_full(V_.p, false, M_.p, false, nullptr, Tm_.p, bupd_.p);

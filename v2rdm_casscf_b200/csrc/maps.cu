@@ -96,15 +96,6 @@ struct Epi {
     const double* add;
     const double* dotv;
     double* out;
-    // Persistent CG only (COH), the p update p <- beta p + r of the previous
-    // iteration folded into this one, for the instances with pend[b] set:
-    // gathers of p read beta p + r (gr: r), and the row epilogue writes the
-    // updated p of its own row to pw before using it in the dot (pr: r).
-    const double* gr = nullptr;
-    double* pw = nullptr;
-    const double* pr = nullptr;
-    const double* beta = nullptr;
-    const int* pend = nullptr;
 };
 // COH: the vectors are written by other CTAs of the same (persistent) launch,
 // so they are loaded through L2 (ld.global.cg), never from a stale L1 line.
@@ -119,12 +110,7 @@ __device__ __forceinline__ double epilogue(const Epi& e, int64_t r, int B, int b
     else
         e.out[t] = s;
     if (!e.dotv) return 0.0;
-    double pv = COH ? __ldcg(e.dotv + t) : e.dotv[t];
-    if (COH && e.pw && e.pend[b]) {
-        pv = e.beta[b] * pv + __ldcg(e.pr + t);
-        e.pw[t] = pv;
-    }
-    return pv * s;
+    return (COH ? __ldcg(e.dotv + t) : e.dotv[t]) * s;
 }
 
 // Bucketed-ELL part.  One lane per row (slot index i of its bucket) and a
@@ -177,17 +163,7 @@ __device__ __forceinline__ void ell_rows(const DevMap& M, int bi, int64_t tile0,
             for (int k = 0; k < KB; k++) {
                 if (c[k] < 0) continue;
                 const double* g = in + (int64_t)c[k] * B + b0;
-                if (COH && e.gr) {
-                    // gathered p with the pending update beta p + r
-                    const double* gr = e.gr + (int64_t)c[k] * B + b0;
-#pragma unroll
-                    for (int j = 0; j < CH; j++)
-                        if (j < cnt) {
-                            double pv = __ldcg(g + j);
-                            if (e.pend[b0 + j]) pv = e.beta[b0 + j] * pv + __ldcg(gr + j);
-                            acc[j] += v[k] * pv;
-                        }
-                } else if (VEC) {
+                if (VEC) {
 #pragma unroll
                     for (int j = 0; j < CH; j += 2)
                         if (j < cnt) {
@@ -239,10 +215,8 @@ __device__ __forceinline__ void long_row(const DevMap& M, int B, const double* _
     double s = 0.0;
     if (threadIdx.x < lanes * B)
         for (int k = k0 + l; k < k1; k += lanes) {
-            const int64_t gi = (int64_t)M.long_col[k] * B + b;
-            double pv = COH ? __ldcg(in + gi) : in[gi];
-            if (COH && e.gr && e.pend[b]) pv = e.beta[b] * pv + __ldcg(e.gr + gi);
-            s += M.long_val[k] * pv;
+            const double* g = in + (int64_t)M.long_col[k] * B + b;
+            s += M.long_val[k] * (COH ? __ldcg(g) : *g);
         }
     shl[threadIdx.x] = s;
     __syncthreads();
@@ -836,9 +810,8 @@ __global__ void __launch_bounds__(kThreads, kLoopCtasPerSm) cg_loop_kernel(const
     __shared__ double bookA[kBookSize], bookAT[kBookSize];
     __shared__ CgScalars sc[kLoopMaxB];
     __shared__ int sact[kLoopMaxB];
-    __shared__ double spap[kLoopMaxB], srn[kLoopMaxB], sbeta[kLoopMaxB];
-    __shared__ int spend[kLoopMaxB];
-    __shared__ int s_any, s_pend;
+    __shared__ double spap[kLoopMaxB], srn[kLoopMaxB];
+    __shared__ int s_any;
     const int B = L.B;
     if (threadIdx.x < kBookSize) {
         if (L.A.book) bookA[threadIdx.x] = L.A.book[threadIdx.x];
@@ -847,8 +820,6 @@ __global__ void __launch_bounds__(kThreads, kLoopCtasPerSm) cg_loop_kernel(const
     if ((int)threadIdx.x < B) {
         sc[threadIdx.x] = L.cs[threadIdx.x];
         sact[threadIdx.x] = sc[threadIdx.x].active;
-        spend[threadIdx.x] = 0;  // p = r at the start: no update pending
-        sbeta[threadIdx.x] = 0.0;
     }
     __syncthreads();
     const unsigned int G = gridDim.x;
@@ -856,38 +827,23 @@ __global__ void __launch_bounds__(kThreads, kLoopCtasPerSm) cg_loop_kernel(const
     const int unitsAT = L.blAT.start[L.AT.nb] * L.blAT.nchunk + L.AT.nlong;
     const int unitsA = L.blA.start[L.A.nb] * L.blA.nchunk + L.A.nlong;
     const int slotsA = L.blA.start[L.A.nb] + L.A.nlong;  // partial slots of the A map
-    // The p update of an iteration (p = beta p + r, cg_solver.cc:173-176) is
-    // folded into the next: its A^T phase gathers beta p + r, and its A phase
-    // writes the updated p of each row before using it in p.Ap.  Three grid
-    // barriers per iteration instead of four, and no pass of its own.
-    Epi eAT{nullptr, nullptr, nullptr, nullptr, L.atp};
-    eAT.beta = sbeta;
-    eAT.pend = spend;
-    Epi eA{nullptr, nullptr, nullptr, L.p, L.ap};
-    eA.pr = L.r;
-    eA.beta = sbeta;
-    eA.pend = spend;
+    const Epi eAT{nullptr, nullptr, nullptr, nullptr, L.atp};
+    const Epi eA{nullptr, nullptr, nullptr, L.p, L.ap};
     int it = 0;
     while (true) {
         if (threadIdx.x == 0) {
-            int a = 0, pd = 0;
-            for (int b = 0; b < B; b++) {
-                a |= sact[b];
-                pd |= spend[b];
-            }
+            int a = 0;
+            for (int b = 0; b < B; b++) a |= sact[b];
             s_any = a;
-            s_pend = pd;
         }
         __syncthreads();
         if (!s_any || it >= L.cap) break;
-        eAT.gr = s_pend ? L.r : nullptr;
-        eA.pw = s_pend ? L.p : nullptr;
-        // A^T p (with the pending update of p)
+        // A^T p
         for (int u = blockIdx.x; u < unitsAT; u += G)
             ell_unit<CH, false, true>(L.AT, L.blAT, B, L.p, eAT, sact, nullptr, bookAT, u);
         target += G;
         if (!grid_wait(L.bar, target, L.err)) return;
-        // Ap = A (A^T p), the updated p of each row, and the partials of p.Ap
+        // Ap = A (A^T p) and the partials of p.Ap
         for (int u = blockIdx.x; u < unitsA; u += G)
             ell_unit<CH, false, true>(L.A, L.blA, B, L.atp, eA, sact, L.part_dot, bookA, u);
         target += G;
@@ -921,11 +877,17 @@ __global__ void __launch_bounds__(kThreads, kLoopCtasPerSm) cg_loop_kernel(const
         if ((int)threadIdx.x < B) {
             cg_scalar_step(sc[threadIdx.x], spap[threadIdx.x], srn[threadIdx.x]);
             sact[threadIdx.x] = sc[threadIdx.x].active;
-            spend[threadIdx.x] = sc[threadIdx.x].do_p;
-            sbeta[threadIdx.x] = sc[threadIdx.x].beta;
+        }
+        __syncthreads();
+        // p = beta p + r where the instance continues (cg_solver.cc:173-176)
+        for (int64_t t = (int64_t)blockIdx.x * kThreads + threadIdx.x; t < L.nc * B; t += (int64_t)G * kThreads) {
+            const int b = (int)(t % B);
+            if (!sc[b].do_p) continue;
+            L.p[t] = sc[b].beta * __ldcg(L.p + t) + __ldcg(L.r + t);
         }
         it++;
-        __syncthreads();  // the scalars of every instance before the loop head reads them
+        target += G;
+        if (!grid_wait(L.bar, target, L.err)) return;
     }
     if (blockIdx.x == 0) {
         if ((int)threadIdx.x < B) L.cs[threadIdx.x] = sc[threadIdx.x];

@@ -2,7 +2,7 @@
 
 Golden fixtures come from the reference's own code (tests/golden/make_golden.py);
 when the compiled oracle is present it is also run on fresh seeds.
-Tolerances: the maps are FP64 gathers, within 1e-12 relative (north-star bar);
+Tolerances: the maps are FP64 gathers, within 1e-12 relative;
 the projection within 1e-10 relative to the block norms (eigensolvers differ);
 total energies within 1e-6 Eh of the reference at the same convergence
 thresholds.

@@ -66,7 +66,7 @@ __device__ double block_sum(double v, double* red) {
 
 // Parallel cyclic Jacobi on the symmetric N x N matrix A (shared memory,
 // leading dimension kLd), round-robin ordering.  A pair (p,q) is rotated when
-// |a_pq| > rot_eps * sqrt(|a_pp a_qq|) and above an absolute floor of
+// |a_pq| > rot_eps * sqrt(|a_pp a_qq|) (tested squared) and above an absolute floor of
 // 1e-17 ||A||_F; the method stops when a sweep would rotate no pair (the
 // classical threshold criterion, which a relative off-norm test near the
 // rounding floor would never reach) or after max_sweeps.  That test runs on
@@ -112,10 +112,14 @@ __device__ void jacobi_smem(double* A, double* V, int N, int max_sweeps, double 
                 if (q < N) {
                     const double apq = A[p * kLd + q];
                     const double app = A[p * kLd + p], aqq = A[q * kLd + q];
-                    if (fabs(apq) > floor_abs && fabs(apq) > rot_eps * sqrt(fabs(app) * fabs(aqq))) {
-                        const double tau = (aqq - app) / (2.0 * apq);
-                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                        c = 1.0 / sqrt(1.0 + t * t);
+                    if (fabs(apq) > floor_abs && apq * apq > rot_eps * rot_eps * fabs(app * aqq)) {
+                        // the angle to FP32 accuracy (an inexact angle leaves a
+                        // residual of ~1e-7 |a_pq| that the next sweep removes);
+                        // c, s exactly orthogonal in FP64 for that angle
+                        const float tau = (float)((aqq - app) / 2.0) / (float)apq;
+                        const float tf = copysignf(1.0f, tau) / (fabsf(tau) + sqrtf(fmaf(tau, tau, 1.0f)));
+                        const double t = (double)tf;
+                        c = rsqrt(1.0 + t * t);
                         s = t * c;
                     }
                 }

@@ -100,3 +100,33 @@ def test_timed_products_leave_the_same_result(v2g):
             off += np_ * np_
             assert np.abs(got - ref).max() <= (1e-5 if tc else 1e-12) * np.abs(ref).max()
 
+
+@pytest.mark.parametrize("ta,tb,use_d", [(False, False, False), (True, False, True), (False, True, False),
+                                         (True, True, True)])
+def test_fp64_small_grid_split_k_matches_numpy(v2g, ta, tb, use_d):
+    """Blocks of one instance's size (30 tiles of 64 x 64): the FP64 product runs
+    as split-K clusters whose partial tiles are summed through distributed shared
+    memory; same 1e-12 bound as the other FP64 forms."""
+    import torch
+
+    dims = [100, 64, 130, 200]
+    rng = np.random.default_rng(21 + 2 * ta + tb)
+    A = _blocks(rng, dims, lambda r, n: r.standard_normal((n, n)))
+    B = _blocks(rng, dims, lambda r, n: r.standard_normal((n, n)))
+    D = [np.concatenate([rng.uniform(-1, 2, n), np.zeros((n + 63) // 64 * 64 - n)]) for n in dims]
+    dev = torch.device("cuda:0")
+    dA = torch.from_numpy(_flat(A)).to(dev)
+    dB = torch.from_numpy(_flat(B)).to(dev)
+    dD = torch.from_numpy(np.concatenate(D)).to(dev)
+    for rep in range(2):
+        dC = torch.full_like(dA, float("nan"))
+        v2g.block_gemm_device(dims, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), trans_a=ta, trans_b=tb,
+                              d_d=dD.data_ptr() if use_d else None, tensor_cores=False)
+        C, off = dC.cpu().numpy(), 0
+        for a, b, d in zip(A, B, D):
+            np_ = a.shape[0]
+            ref = (a.T if ta else a) @ (np.diag(d) if use_d else np.eye(np_)) @ (b.T if tb else b)
+            got = C[off:off + np_ * np_].reshape(np_, np_)
+            off += np_ * np_
+            assert np.isfinite(got).all()
+            assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()

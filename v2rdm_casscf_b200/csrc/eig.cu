@@ -15,6 +15,8 @@
 //     z = mu x - U come from one batched GEMM.
 // Jacobi's rotations need no ordering of eigenvalues and are robust for the
 // clustered and exactly degenerate spectra these blocks have.
+#include <cooperative_groups.h>
+
 #include <cfloat>
 
 #include <mutex>
@@ -414,6 +416,88 @@ __global__ void __launch_bounds__((64 / R) * (64 / R)) gemm_kernel(const BlockTa
     for (int i = 0; i < R; i++)
 #pragma unroll
         for (int j = 0; j < R; j++) cc[(int64_t)(i0 + ty + S * i) * np + j0 + tx + S * j] = acc[i][j];
+}
+
+// Split-K form for the smallest grids (one instance's few blocks): a cluster
+// of kSplitK CTAs per 64 x 64 tile, CTA r of the cluster summing k in
+// [r np / kSplitK, (r + 1) np / kSplitK) as gemm_kernel<4> does; the partial
+// tiles meet in rank 0's registers through distributed shared memory, added
+// in rank order (a fixed order: no atomics, no second launch).  kSplitK times
+// the CTAs of gemm_kernel<4>, each with a quarter of the FMA chain.
+constexpr int kSplitK = 4;
+__global__ void __cluster_dims__(kSplitK, 1, 1) __launch_bounds__(256)
+    gemm_splitk_kernel(const BlockTask* __restrict__ tasks, const GemmTile* __restrict__ tiles,
+                       const double* __restrict__ A, int transA, const double* __restrict__ Bm, int transB,
+                       const double* __restrict__ dvec, double* __restrict__ C, const int* __restrict__ bmask) {
+    namespace cg = cooperative_groups;
+    constexpr int R = 4, S = 16, NT = 256, U = 1024 / NT;
+    // the two operand buffers, and after the K loop the CTA's partial tile
+    // (64 rows of kGemmLd: the same 4,160 doubles)
+    __shared__ double sm[2 * 2 * kGemmBK * kGemmLd];
+    auto As = reinterpret_cast<double (*)[kGemmBK][kGemmLd]>(sm);
+    auto Bs = reinterpret_cast<double (*)[kGemmBK][kGemmLd]>(sm + 2 * kGemmBK * kGemmLd);
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const GemmTile tl = tiles[blockIdx.x / kSplitK];
+    if (bmask && !bmask[tl.task]) return;  // every CTA of the cluster: the same tile
+    const BlockTask t = tasks[tl.task];
+    const int np = t.np;
+    const double* a = A + t.woff;
+    const double* bb = Bm + t.woff;
+    const double* d = dvec ? dvec + t.doff : nullptr;
+    const int tx = threadIdx.x % S, ty = threadIdx.x / S;
+    const int i0 = tl.ti * 64, j0 = tl.tj * 64;
+    const int kq = np / kSplitK, kb = rank * kq, ke = kb + kq;  // np is a multiple of 64
+    double acc[R][R];
+#pragma unroll
+    for (int i = 0; i < R; i++)
+#pragma unroll
+        for (int j = 0; j < R; j++) acc[i][j] = 0.0;
+    double ra[U], rb[U];
+    gemm_load_chunk<NT>(a, bb, np, i0, j0, kb, transA, transB, ra, rb);
+    gemm_store_chunk<NT>(As[0], Bs[0], transA, transB, ra, rb, d, kb);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = kb; k0 < ke; k0 += kGemmBK) {
+        const bool more = k0 + kGemmBK < ke;
+        if (more) gemm_load_chunk<NT>(a, bb, np, i0, j0, k0 + kGemmBK, transA, transB, ra, rb);
+#pragma unroll
+        for (int kk = 0; kk < kGemmBK; kk++) {
+            double av[R], bv[R];
+#pragma unroll
+            for (int i = 0; i < R; i++) av[i] = As[buf][kk][ty + S * i];
+#pragma unroll
+            for (int j = 0; j < R; j++) bv[j] = Bs[buf][kk][tx + S * j];
+#pragma unroll
+            for (int i = 0; i < R; i++)
+#pragma unroll
+                for (int j = 0; j < R; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
+        if (more) {
+            gemm_store_chunk<NT>(As[buf ^ 1], Bs[buf ^ 1], transA, transB, ra, rb, d, k0 + kGemmBK);
+            __syncthreads();
+            buf ^= 1;
+        }
+    }
+    __syncthreads();  // the operand buffers become the partial tile
+#pragma unroll
+    for (int i = 0; i < R; i++)
+#pragma unroll
+        for (int j = 0; j < R; j++) sm[(ty + S * i) * kGemmLd + tx + S * j] = acc[i][j];
+    cl.sync();
+    if (rank == 0) {
+        double* cc = C + t.woff;
+#pragma unroll
+        for (int i = 0; i < R; i++)
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                const int o = (ty + S * i) * kGemmLd + tx + S * j;
+                double v = 0.0;
+                for (int r = 0; r < kSplitK; r++) v += cl.map_shared_rank(sm, r)[o];
+                cc[(int64_t)(i0 + ty + S * i) * np + j0 + tx + S * j] = v;
+            }
+    }
+    cl.sync();  // the partial tiles stay alive until rank 0 has read them
 }
 
 // Global index of local row a (0..63) of pair (I, J): first 32 rows are column
@@ -1046,8 +1130,11 @@ void launch_gemm(const BlockTask* tasks, const GemmTile* tiles, int ntiles, cons
                  const double* Bm, bool transB, const double* dvec, double* C, const int* bmask, cudaStream_t s) {
     if (ntiles == 0) return;
     // below two tiles per SM (148 SMs) the 256-thread form hides the latency
-    // the 64-thread form cannot
-    if (ntiles < 2 * 148)
+    // the 64-thread form cannot; below half a tile per SM, the split-K
+    // clusters also spread each tile's K over four CTAs
+    if (ntiles * kSplitK <= 2 * 148)
+        gemm_splitk_kernel<<<ntiles * kSplitK, 256, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
+    else if (ntiles < 2 * 148)
         gemm_kernel<4><<<ntiles, 256, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);
     else
         gemm_kernel<8><<<ntiles, 64, 0, s>>>(tasks, tiles, A, transA, Bm, transB, dvec, C, bmask);

@@ -571,12 +571,6 @@ class GroupRun {
         launch_lam_from_diag(large_d_.p, nlarge_, W_.p, bjac_.p, lam_.p, s_);
     }
 
-    void apply_A(const double* d_in, double* d_out) {
-        launch_spmv(mA_, B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
-    }
-    void apply_AT(const double* d_in, double* d_out) {
-        launch_spmv(mAT_, B_, d_in, d_out, nullptr, nullptr, nullptr, nullptr, s_);
-    }
     cudaStream_t stream() const { return s_; }
     DevBuf<double>& xbuf() { return x_; }
     DevBuf<double>& ybuf() { return y_; }
